@@ -1,0 +1,235 @@
+// Library context, error state and logging.
+#include "internal.h"
+
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+namespace {
+
+thread_local int g_last_error = BML_B200_OK;
+int g_verbose = 1;
+
+B200Context g_ctx;
+bool g_ctx_ready = false;
+bool g_ctx_failed = false;
+std::mutex g_ctx_mutex;
+
+} // namespace
+
+void b200_set_error(int status, const char *fmt, ...)
+{
+    g_last_error = status;
+    if (!g_verbose)
+        return;
+    va_list ap;
+    va_start(ap, fmt);
+    fprintf(stderr, "[bml_b200 error %d: %s] ", status, bml_b200_error_string(status));
+    vfprintf(stderr, fmt, ap);
+    fprintf(stderr, "\n");
+    va_end(ap);
+}
+
+int b200_get_error() { return g_last_error; }
+
+bool b200_cuda_ok(cudaError_t err, const char *what, const char *file, int line)
+{
+    if (err == cudaSuccess)
+        return true;
+    b200_set_error(BML_B200_ERR_CUDA, "%s failed at %s:%d: %s", what, file, line,
+                   cudaGetErrorString(err));
+    return false;
+}
+
+B200Context *b200_ctx()
+{
+    if (g_ctx_ready)
+        return &g_ctx;
+    std::lock_guard<std::mutex> lock(g_ctx_mutex);
+    if (g_ctx_ready)
+        return &g_ctx;
+    if (g_ctx_failed)
+    {
+        b200_set_error(BML_B200_ERR_NO_DEVICE, "no usable CUDA device");
+        return nullptr;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+    {
+        g_ctx_failed = true;
+        b200_set_error(BML_B200_ERR_NO_DEVICE, "no usable CUDA device (%s)",
+                       e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+        return nullptr;
+    }
+    memset(&g_ctx, 0, sizeof(g_ctx));
+    if (!CUDA_OK(cudaGetDevice(&g_ctx.device)))
+        return nullptr;
+    cudaDeviceProp prop;
+    if (!CUDA_OK(cudaGetDeviceProperties(&prop, g_ctx.device)))
+        return nullptr;
+    if (prop.major < 10)
+    {
+        g_ctx_failed = true;
+        b200_set_error(BML_B200_ERR_NO_DEVICE,
+                       "device %d (%s, sm_%d%d) is not an sm_100 part; the kernels are built for sm_100a only",
+                       g_ctx.device, prop.name, prop.major, prop.minor);
+        return nullptr;
+    }
+    g_ctx.sm_count = prop.multiProcessorCount;
+    g_ctx.smem_optin = prop.sharedMemPerBlockOptin;
+    if (!CUDA_OK(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking)))
+        return nullptr;
+    if (!CUDA_OK(cudaMallocHost(&g_ctx.pinned, 65536)))
+        return nullptr;
+    if (!CUDA_OK(cudaMalloc(&g_ctx.d_small, 65536)))
+        return nullptr;
+    g_ctx_ready = true;
+    return &g_ctx;
+}
+
+void *b200_scratch(size_t bytes)
+{
+    B200Context *c = b200_ctx();
+    if (!c)
+        return nullptr;
+    if (bytes <= c->scratch_bytes)
+        return c->scratch;
+    // Grow geometrically; the old arena may still be in use by queued kernels,
+    // so drain the stream before releasing it.
+    if (!CUDA_OK(cudaStreamSynchronize(c->stream)))
+        return nullptr;
+    if (c->scratch)
+        cudaFree(c->scratch);
+    c->scratch = nullptr;
+    c->scratch_bytes = 0;
+    size_t want = bytes + bytes / 4 + (1 << 20);
+    if (cudaMalloc(&c->scratch, want) != cudaSuccess)
+    {
+        cudaGetLastError();
+        b200_set_error(BML_B200_ERR_ALLOC, "device scratch of %zu bytes", want);
+        c->scratch = nullptr;
+        return nullptr;
+    }
+    c->scratch_bytes = want;
+    return c->scratch;
+}
+
+bool b200_sync()
+{
+    B200Context *c = b200_ctx();
+    if (!c)
+        return false;
+    return CUDA_OK(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: status and housekeeping
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int bml_b200_last_error(void) { return g_last_error; }
+
+void bml_b200_clear_error(void) { g_last_error = BML_B200_OK; }
+
+void bml_b200_set_verbose(int on) { g_verbose = on; }
+
+const char *bml_b200_error_string(int status)
+{
+    switch (status)
+    {
+    case BML_B200_OK: return "ok";
+    case BML_B200_ERR_NO_DEVICE: return "no usable CUDA device";
+    case BML_B200_ERR_CUDA: return "CUDA runtime error";
+    case BML_B200_ERR_INVALID: return "invalid argument";
+    case BML_B200_ERR_UNSUPPORTED: return "unsupported matrix type or precision";
+    case BML_B200_ERR_ROW_OVERFLOW: return "Number of non-zeroes per row > M, Increase M";
+    case BML_B200_ERR_ALLOC: return "allocation failed";
+    case BML_B200_ERR_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+    }
+}
+
+int bml_b200_synchronize(void) { return b200_sync() ? BML_B200_OK : b200_get_error(); }
+
+int bml_b200_device_info(int *sm_count, int *device)
+{
+    B200Context *c = b200_ctx();
+    if (!c)
+        return b200_get_error();
+    if (sm_count)
+        *sm_count = c->sm_count;
+    if (device)
+        *device = c->device;
+    return BML_B200_OK;
+}
+
+void bml_init(void) { (void) b200_ctx(); }
+
+void bml_shutdown(void)
+{
+    std::lock_guard<std::mutex> lock(g_ctx_mutex);
+    if (!g_ctx_ready)
+        return;
+    cudaStreamSynchronize(g_ctx.stream);
+    if (g_ctx.scratch)
+        cudaFree(g_ctx.scratch);
+    if (g_ctx.d_small)
+        cudaFree(g_ctx.d_small);
+    if (g_ctx.pinned)
+        cudaFreeHost(g_ctx.pinned);
+    cudaStreamDestroy(g_ctx.stream);
+    memset(&g_ctx, 0, sizeof(g_ctx));
+    g_ctx_ready = false;
+}
+
+// Logging with the reference's level names; an ERROR is reported and recorded
+// but never terminates the process (the reference exits, bml_logger.c:111-115).
+static void b200_vlog(bml_log_level_t level, const char *file, int line,
+                      const char *format, va_list ap)
+{
+    if (level == BML_LOG_DEBUG)
+        return;
+    FILE *out = level >= BML_LOG_WARNING ? stderr : stdout;
+    if (level == BML_LOG_ERROR)
+        g_last_error = BML_B200_ERR_INVALID;
+    if (file)
+        fprintf(out, "[%s:%d] ", file, line);
+    if (level == BML_LOG_WARNING)
+        fprintf(out, "WARNING ");
+    if (level == BML_LOG_ERROR)
+        fprintf(out, "ERROR ");
+    vfprintf(out, format, ap);
+    fflush(out);
+}
+
+void bml_log(bml_log_level_t log_level, char *format, ...)
+{
+    va_list ap;
+    va_start(ap, format);
+    b200_vlog(log_level, nullptr, 0, format, ap);
+    va_end(ap);
+}
+
+void bml_log_location(bml_log_level_t log_level, char *filename, int linenumber,
+                      char *format, ...)
+{
+    va_list ap;
+    va_start(ap, format);
+    b200_vlog(log_level, filename, linenumber, format, ap);
+    va_end(ap);
+}
+
+char *bml_version(void)
+{
+    static char v[] = "2.4.0-b200";
+    return v;
+}
+
+void bml_print_version(void)
+{
+    printf("bml version %s (B200 sm_100a ELLPACK/ELLBLOCK path)\n", bml_version());
+}
+
+} // extern "C"

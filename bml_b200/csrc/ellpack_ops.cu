@@ -1,0 +1,996 @@
+// ELLPACK-R bandwidth-bound operations around the product: add, add_identity,
+// scale, threshold, trace, trace_mult, transpose, copy, Gershgorin bounds.
+// Each kernel reproduces the reference loop's arithmetic and output order.
+#include "device_util.cuh"
+
+#include <cfloat>
+#include <cstring>
+
+using namespace b200;
+
+// ---------------------------------------------------------------------------
+// Reductions shared by several operations.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) b200_sum_rows_kernel(const double *a, const double *b,
+                                                            int n, double *out)
+{
+    __shared__ double sa[1024], sb[1024];
+    const int t = threadIdx.x;
+    const int per = b200_ceil_div(n, 1024);
+    double xa = 0.0, xb = 0.0;
+    for (int r = t * per; r < min(n, (t + 1) * per); ++r)
+    {
+        if (a)
+            xa += a[r];
+        if (b)
+            xb += b[r];
+    }
+    sa[t] = xa;
+    sb[t] = xb;
+    __syncthreads();
+    for (int s = 512; s; s >>= 1)
+    {
+        if (t < s)
+        {
+            sa[t] += sa[t + s];
+            sb[t] += sb[t + s];
+        }
+        __syncthreads();
+    }
+    if (t == 0)
+    {
+        out[0] = sa[0];
+        out[1] = sb[0];
+    }
+}
+
+__global__ void __launch_bounds__(1024) b200_maxmin_rows_kernel(const double *hi, const double *lo,
+                                                               int n, double init_max,
+                                                               double init_min, double *out)
+{
+    __shared__ double smax[1024], smin[1024];
+    const int t = threadIdx.x;
+    double mx = init_max, mn = init_min;
+    for (int r = t; r < n; r += 1024)
+    {
+        mx = fmax(mx, hi[r]);
+        mn = fmin(mn, lo[r]);
+    }
+    smax[t] = mx;
+    smin[t] = mn;
+    __syncthreads();
+    for (int s = 512; s; s >>= 1)
+    {
+        if (t < s)
+        {
+            smax[t] = fmax(smax[t], smax[t + s]);
+            smin[t] = fmin(smin[t], smin[t + s]);
+        }
+        __syncthreads();
+    }
+    if (t == 0)
+    {
+        out[0] = smax[0];
+        out[1] = smin[0];
+    }
+}
+
+namespace {
+
+inline int rows_grid(B200Context *c, int N, int rows_per_block)
+{
+    return max(1, min(b200_ceil_div(N, rows_per_block), c->sm_count * 16));
+}
+
+// ---------------------------------------------------------------------------
+// add: A <- alpha*A + beta*B, threshold without diagonal exemption.
+// Reference: ellpack/bml_add_ellpack_typed.c:50-216.  Per row: A's columns in
+// A's order (x = 0 + alpha*a), then B's (x += beta*b; new columns appended in
+// B's order); kept when |x| > threshold.  A term is skipped entirely when its
+// scalar is 0.  One team of W warps per row; A's row is staged in shared
+// memory with a hash from column to position, so the row is rewritten in
+// place only after it has been read.
+// Shared memory per team: keys[TS] pos[TS] xa[ldA](T) ka[ldA] newpos[ldB] cnt.
+// ---------------------------------------------------------------------------
+template <typename T, int W>
+__global__ void __launch_bounds__(W * 32) add_kernel(T *Av, int *Ai, int *An, int lda, int Ma,
+                                                   const T *Bv, const int *Bi, const int *Bn,
+                                                   int ldb, int N, double alpha, double beta,
+                                                   double thr, int logts, int *overflow)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int TS = 1 << logts;
+    const unsigned mask = TS - 1;
+    T *xa = reinterpret_cast<T *>(smem);
+    int *ka = reinterpret_cast<int *>(xa + lda);
+    int *keys = ka + lda;
+    int *pos = keys + TS;
+    int *newb = pos + TS;   // B positions of new columns, in B order
+    int *cnt = newb + ldb;  // [2][W]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+    const T thr_t = (T) thr;
+    const bool use_a = alpha > 0.0 || alpha < 0.0;
+    const bool use_b = beta > 0.0 || beta < 0.0;
+
+    for (int i = blockIdx.x; i < N; i += gridDim.x)
+    {
+        for (int s = tid; s < TS; s += W * 32)
+            keys[s] = B200_EMPTY_KEY;
+        __syncthreads();
+        const int na = use_a ? An[i] : 0;
+        const int nb = use_b ? Bn[i] : 0;
+        // stage A's row: x = 0 + alpha*a
+        for (int p = tid; p < na; p += W * 32)
+        {
+            const int k = Ai[(size_t) i * lda + p];
+            ka[p] = k;
+            xa[p] = axpy_d(T(0), alpha, Av[(size_t) i * lda + p]);
+            hash_put(keys, pos, mask, k, p);
+        }
+        __syncthreads();
+        // B's contributions: existing columns update xa, new ones are listed
+        // in B order (warp-contiguous chunks + cross-warp prefix).
+        int nnew = 0;
+        for (int c0 = 0; c0 < nb; c0 += W * 32)
+        {
+            const int q = c0 + warp * 32 + lane;
+            bool isnew = false;
+            if (q < nb)
+            {
+                const int k = Bi[(size_t) i * ldb + q];
+                const int p = hash_get(keys, pos, mask, k);
+                if (p >= 0)
+                    xa[p] = axpy_d(xa[p], beta, Bv[(size_t) i * ldb + q]);
+                else
+                    isnew = true;
+            }
+            const unsigned bal = __ballot_sync(FULL, isnew);
+            if (lane == 0)
+                cnt[((c0 / (W * 32)) & 1) * W + warp] = __popc(bal);
+            __syncthreads();
+            int pre = 0, tot = 0;
+            for (int w = 0; w < W; ++w)
+            {
+                const int cw = cnt[((c0 / (W * 32)) & 1) * W + w];
+                pre += w < warp ? cw : 0;
+                tot += cw;
+            }
+            if (isnew)
+                newb[nnew + pre + __popc(bal & lanemask_lt())] = q;
+            nnew += tot;
+        }
+        __syncthreads();
+        // compaction: A's entries then the new B entries
+        const int total = na + nnew;
+        int ll = 0;
+        int round = 0;
+        for (int c0 = 0; c0 < total; c0 += W * 32, ++round)
+        {
+            const int q = c0 + warp * 32 + lane;
+            T x = T(0);
+            int k = 0;
+            if (q < na)
+            {
+                x = xa[q];
+                k = ka[q];
+            }
+            else if (q < total)
+            {
+                const int bq = newb[q - na];
+                k = Bi[(size_t) i * ldb + bq];
+                x = axpy_d(T(0), beta, Bv[(size_t) i * ldb + bq]);
+            }
+            const bool keep = q < total && fabs(x) > thr_t;
+            const unsigned bal = __ballot_sync(FULL, keep);
+            if (lane == 0)
+                cnt[(round & 1) * W + warp] = __popc(bal);
+            __syncthreads();
+            int pre = 0, tot = 0;
+            for (int w = 0; w < W; ++w)
+            {
+                const int cw = cnt[(round & 1) * W + w];
+                pre += w < warp ? cw : 0;
+                tot += cw;
+            }
+            const int p = ll + pre + __popc(bal & lanemask_lt());
+            if (keep && p < Ma)
+            {
+                Av[(size_t) i * lda + p] = x;
+                Ai[(size_t) i * lda + p] = k;
+            }
+            ll += tot;
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            An[i] = min(ll, Ma);
+            if (ll > Ma)
+                atomicExch(overflow, 1);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// add_identity: A <- A + beta*I, then threshold.  Reference:
+// ellpack/bml_add_ellpack_typed.c:420-549.  The last diagonal entry of the row
+// gets x + beta (or (beta, i) is appended when the row has none); entries are
+// kept when |x| > threshold, in row order.  One warp per row, in place.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void add_identity_kernel(T *Av, int *Ai, int *An, int ld, int M, int N, double beta,
+                                    double thr, int *overflow)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const T thr_t = (T) thr;
+    const bool use_b = beta > 0.0 || beta < 0.0;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        T *v = Av + (size_t) i * ld;
+        int *ix = Ai + (size_t) i * ld;
+        int diag = -1;
+        for (int p = lane; p < n; p += 32)
+            if (ix[p] == i)
+                diag = p;
+        for (int o = 16; o; o >>= 1)
+            diag = max(diag, __shfl_xor_sync(FULL, diag, o));
+        const int total = n + ((use_b && diag < 0) ? 1 : 0);
+        int ll = 0;
+        for (int c0 = 0; c0 < total; c0 += 32)
+        {
+            const int q = c0 + lane;
+            T x = T(0);
+            int k = 0;
+            if (q < n)
+            {
+                x = v[q];
+                k = ix[q];
+                if (use_b && q == diag)
+                    x = (T) __dadd_rn((double) x, beta);
+            }
+            else if (q < total)
+            {
+                x = (T) beta;
+                k = i;
+            }
+            const bool keep = q < total && fabs(x) > thr_t;
+            const unsigned bal = __ballot_sync(FULL, keep);
+            const int p = ll + __popc(bal & lanemask_lt());
+            if (keep && p < M)
+            {
+                v[p] = x;
+                ix[p] = k;
+            }
+            ll += __popc(bal);
+        }
+        if (lane == 0)
+        {
+            An[i] = min(ll, M);
+            if (ll > M)
+                atomicExch(overflow, 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// threshold: stable in-place compaction keeping |v| > threshold (no diagonal
+// exemption).  Reference: ellpack/bml_threshold_ellpack_typed.c:88-133 (in
+// place) and :28-78 (into a new matrix).  One warp per row.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void threshold_kernel(const T *Av, const int *Ai, const int *An, int lda, T *Bv,
+                                 int *Bi, int *Bn, int ldb, int N, double thr)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const T thr_t = (T) thr;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        int ll = 0;
+        for (int c0 = 0; c0 < n; c0 += 32)
+        {
+            const int q = c0 + lane;
+            T x = T(0);
+            int k = 0;
+            if (q < n)
+            {
+                x = Av[(size_t) i * lda + q];
+                k = Ai[(size_t) i * lda + q];
+            }
+            const bool keep = q < n && fabs(x) > thr_t;
+            const unsigned bal = __ballot_sync(FULL, keep);
+            const int p = ll + __popc(bal & lanemask_lt());
+            if (keep)
+            {
+                Bv[(size_t) i * ldb + p] = x;
+                Bi[(size_t) i * ldb + p] = k;
+            }
+            ll += __popc(bal);
+        }
+        if (lane == 0)
+            Bn[i] = ll;
+    }
+}
+
+// scale: B = s*A over the stored entries (the reference scales the padded
+// N*M array with BLAS ?scal, bml_scale_ellpack_typed.c:85,119; entries past
+// nnz are never read).  One warp per row.
+template <typename T>
+__global__ void scale_kernel(const T *Av, const int *Ai, const int *An, int lda, T *Bv, int *Bi,
+                             int *Bn, int ldb, int N, T s, int copy_structure)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        for (int p = lane; p < n; p += 32)
+        {
+            Bv[(size_t) i * ldb + p] = mul_rn(s, Av[(size_t) i * lda + p]);
+            if (copy_structure)
+                Bi[(size_t) i * ldb + p] = Ai[(size_t) i * lda + p];
+        }
+        if (copy_structure && lane == 0)
+            Bn[i] = n;
+    }
+}
+
+// copy: B <- A row by row (reference ellpack/bml_copy_ellpack_typed.c:86-148).
+template <typename T>
+__global__ void copy_kernel(const T *Av, const int *Ai, const int *An, int lda, T *Bv, int *Bi,
+                            int *Bn, int ldb, int Mb, int N, int *overflow)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        const int m = min(n, Mb);
+        for (int p = lane; p < m; p += 32)
+        {
+            Bv[(size_t) i * ldb + p] = Av[(size_t) i * lda + p];
+            Bi[(size_t) i * ldb + p] = Ai[(size_t) i * lda + p];
+        }
+        if (lane == 0)
+        {
+            Bn[i] = m;
+            if (n > Mb)
+                atomicExch(overflow, 1);
+        }
+    }
+}
+
+// trace: value of the first diagonal entry of each row (reference
+// ellpack/bml_trace_ellpack_typed.c:74-88, `break` at the first match).
+template <typename T>
+__global__ void diag_kernel(const T *Av, const int *Ai, const int *An, int ld, int N, double *d)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        int first = n;
+        for (int c0 = 0; c0 < n && first == n; c0 += 32)
+        {
+            const int q = c0 + lane;
+            const unsigned bal = __ballot_sync(FULL, q < n && Ai[(size_t) i * ld + q] == i);
+            if (bal)
+                first = c0 + __ffs(bal) - 1;
+        }
+        if (lane == 0)
+            d[i] = first < n ? (double) Av[(size_t) i * ld + first] : 0.0;
+    }
+}
+
+// trace_mult: sum over row i and the columns c of A's row of A[i,c]*B[i,c]
+// (the reference's bml_getVector_ellpack reads B's row i at A's columns,
+// ellpack/bml_trace_ellpack_typed.c:145-158 with
+// ellpack/bml_submatrix_ellpack_typed.c:380-406; a column absent from B's row
+// contributes 0).  Per-row partial sums in FP64.  One warp per row, B's row in
+// a shared-memory hash of 2^logts slots per warp.
+template <typename T>
+__global__ void trace_mult_kernel(const T *Av, const int *Ai, const int *An, int lda,
+                                  const T *Bv, const int *Bi, const int *Bn, int ldb, int N,
+                                  int logts, double *part)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int TS = 1 << logts;
+    const unsigned mask = TS - 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *keys = reinterpret_cast<int *>(smem) + (size_t) warp * 2 * TS;
+    int *pos = keys + TS;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        for (int s = lane; s < TS; s += 32)
+            keys[s] = B200_EMPTY_KEY;
+        __syncwarp();
+        const int nb = Bn[i];
+        // the first occurrence of a column in B's row wins, as in the reference
+        for (int p = nb - 1 - lane; p >= 0; p -= 32)
+            ;
+        for (int c0 = 0; c0 < nb; c0 += 32)
+        {
+            const int p = c0 + lane;
+            if (p < nb)
+                hash_put(keys, pos, mask, Bi[(size_t) i * ldb + p], p);
+            __syncwarp();
+        }
+        __syncwarp();
+        double s = 0.0;
+        T acc = T(0);
+        const int na = An[i];
+        for (int p = lane; p < na; p += 32)
+        {
+            const int q = hash_get(keys, pos, mask, Ai[(size_t) i * lda + p]);
+            if (q >= 0)
+                s += (double) mul_rn(Av[(size_t) i * lda + p], Bv[(size_t) i * ldb + q]);
+        }
+        (void) acc;
+        for (int o = 16; o; o >>= 1)
+            s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0)
+            part[i] = s;
+        __syncwarp();
+    }
+}
+
+// Gershgorin per row (reference ellpack/bml_normalize_ellpack_typed.c:82-175):
+// radius = sum of |a| over off-diagonal entries, accumulated as
+// `radius += (double) |a|` into a variable of the matrix precision; dvalue =
+// the last diagonal entry; hi = dvalue + radius, lo = dvalue - radius in the
+// matrix precision.
+template <typename T>
+__global__ void gershgorin_kernel(const T *Av, const int *Ai, const int *An, int ld, int N,
+                                  double *hi, double *lo)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        // The sum runs in row order, so one lane walks the row; the row is
+        // read in 32-wide chunks so the loads stay coalesced.
+        T radius = T(0), dvalue = T(0);
+        for (int c0 = 0; c0 < n; c0 += 32)
+        {
+            const int q = c0 + lane;
+            T v = T(0);
+            int k = -1;
+            if (q < n)
+            {
+                v = Av[(size_t) i * ld + q];
+                k = Ai[(size_t) i * ld + q];
+            }
+            const int m = min(32, n - c0);
+            for (int t = 0; t < m; ++t)
+            {
+                const T vt = __shfl_sync(FULL, v, t);
+                const int kt = __shfl_sync(FULL, k, t);
+                if (kt == i)
+                    dvalue = vt;
+                else
+                    radius = (T) __dadd_rn((double) radius, (double) fabs(vt));
+            }
+        }
+        if (lane == 0)
+        {
+            hi[i] = (double) add_rn(dvalue, radius);
+            lo[i] = (double) add_rn(dvalue, (T) -radius);
+        }
+    }
+}
+
+// transpose, step 1: count entries per column and scatter (row, value) into
+// the column's output row at an atomically reserved position.
+template <typename T>
+__global__ void transpose_scatter_kernel(const T *Av, const int *Ai, const int *An, int lda,
+                                         int N, T *Bv, int *Bi, int *Bn, int ldb, int Mb,
+                                         int *overflow)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        for (int p = lane; p < n; p += 32)
+        {
+            const int j = Ai[(size_t) i * lda + p];
+            const int slot = atomicAdd(&Bn[j], 1);
+            if (slot < Mb)
+            {
+                Bi[(size_t) j * ldb + slot] = i;
+                Bv[(size_t) j * ldb + slot] = Av[(size_t) i * lda + p];
+            }
+            else
+                atomicExch(overflow, 1);
+        }
+    }
+}
+
+// transpose, step 2: sort every output row by source row (the serial order of
+// the reference's bml_transpose_new_ellpack, bml_transpose_ellpack_typed.c:
+// 76-96, whose OpenMP version is otherwise nondeterministic).  One block per
+// row, bitonic sort of (row, value) pairs in shared memory.
+template <typename T>
+__global__ void row_sort_kernel(T *Bv, int *Bi, int *Bn, int ldb, int Mb, int N, int pow2)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    T *sv = reinterpret_cast<T *>(smem);
+    int *sk = reinterpret_cast<int *>(sv + pow2);
+    for (int j = blockIdx.x; j < N; j += gridDim.x)
+    {
+        const int n = min(Bn[j], Mb);
+        if (n <= 1)
+        {
+            if (threadIdx.x == 0)
+                Bn[j] = n;
+            continue;
+        }
+        int p2 = 1;
+        while (p2 < n)
+            p2 <<= 1;
+        for (int t = threadIdx.x; t < p2; t += blockDim.x)
+        {
+            sk[t] = t < n ? Bi[(size_t) j * ldb + t] : 0x7fffffff;
+            sv[t] = t < n ? Bv[(size_t) j * ldb + t] : T(0);
+        }
+        __syncthreads();
+        for (int k = 2; k <= p2; k <<= 1)
+            for (int s = k >> 1; s > 0; s >>= 1)
+            {
+                for (int t = threadIdx.x; t < p2; t += blockDim.x)
+                {
+                    const int u = t ^ s;
+                    if (u > t)
+                    {
+                        const bool up = (t & k) == 0;
+                        const int a = sk[t], b = sk[u];
+                        if ((a > b) == up)
+                        {
+                            sk[t] = b;
+                            sk[u] = a;
+                            const T tv = sv[t];
+                            sv[t] = sv[u];
+                            sv[u] = tv;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        for (int t = threadIdx.x; t < n; t += blockDim.x)
+        {
+            Bi[(size_t) j * ldb + t] = sk[t];
+            Bv[(size_t) j * ldb + t] = sv[t];
+        }
+        if (threadIdx.x == 0)
+            Bn[j] = n;
+        __syncthreads();
+    }
+}
+
+bool read_flag(B200Context *c, int *dflag, int *out)
+{
+    int *pin = reinterpret_cast<int *>(static_cast<unsigned char *>(c->pinned) + 2048);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream)) ||
+        !b200_sync())
+        return false;
+    *out = *pin;
+    return true;
+}
+
+int *zeroed_flag(B200Context *c)
+{
+    int *f = reinterpret_cast<int *>(static_cast<unsigned char *>(c->d_small) + 2048);
+    if (!CUDA_OK(cudaMemsetAsync(f, 0, sizeof(int), c->stream)))
+        return nullptr;
+    return f;
+}
+
+bool check_pair(const bml_matrix_ellpack_t *A, const bml_matrix_ellpack_t *B, const char *op)
+{
+    if (!A || !B)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "%s: NULL matrix", op);
+        return false;
+    }
+    if (A->N != B->N || A->matrix_precision != B->matrix_precision)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "%s: matrices differ in size or precision", op);
+        return false;
+    }
+    return true;
+}
+
+} // namespace
+
+bool ell_add(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double alpha, double beta,
+             double threshold)
+{
+    if (!check_pair(A, B, "add"))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A) || !ell_to_device(B))
+        return false;
+    if (A == B)
+    {
+        // x = 0 + alpha*a, then x + beta*a: same arithmetic through a copy.
+        bml_matrix_ellpack_t *T0 = ell_alloc(A->matrix_precision, A->N, A->M, A->distribution_mode, false);
+        if (!T0)
+            return false;
+        bool ok = ell_copy(A, T0) && ell_add(A, T0, alpha, beta, threshold);
+        ell_free(T0);
+        return ok;
+    }
+    int *ovf = zeroed_flag(c);
+    if (!ovf)
+        return false;
+    const int need = 2 * (A->M + B->M);
+    int logts = 5;
+    while ((1 << logts) < need)
+        ++logts;
+    const size_t sz = prec_size(A->matrix_precision);
+    const size_t smem = (size_t) A->ld * (sz + 4) + ((size_t) 2 << logts) * 4 + (size_t) B->ld * 4 +
+                        2 * 8 * 4 + 64;
+    if (smem > c->smem_optin)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "add: rows of width %d/%d exceed shared memory",
+                       A->M, B->M);
+        return false;
+    }
+    const int grid = min(A->N, c->sm_count * 8);
+    if (A->matrix_precision == double_real)
+    {
+        auto k = add_kernel<double, 8>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 256, smem, c->stream>>>(static_cast<double *>(A->d_value), A->d_index, A->d_nnz,
+                                          A->ld, A->M, static_cast<const double *>(B->d_value),
+                                          B->d_index, B->d_nnz, B->ld, A->N, alpha, beta,
+                                          threshold, logts, ovf);
+    }
+    else
+    {
+        auto k = add_kernel<float, 8>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 256, smem, c->stream>>>(static_cast<float *>(A->d_value), A->d_index, A->d_nnz,
+                                          A->ld, A->M, static_cast<const float *>(B->d_value),
+                                          B->d_index, B->d_nnz, B->ld, A->N, alpha, beta,
+                                          threshold, logts, ovf);
+    }
+    if (!LAUNCH_OK("add_kernel"))
+        return false;
+    ell_mark_device(A);
+    int hov = 0;
+    if (!read_flag(c, ovf, &hov))
+        return false;
+    if (hov)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "add: a row of the sum has more than M=%d entries",
+                       A->M);
+        return false;
+    }
+    return true;
+}
+
+bool ell_add_identity(bml_matrix_ellpack_t *A, double beta, double threshold)
+{
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A))
+        return false;
+    int *ovf = zeroed_flag(c);
+    if (!ovf)
+        return false;
+    const int grid = rows_grid(c, A->N, 8);
+    if (A->matrix_precision == double_real)
+        add_identity_kernel<double><<<grid, 256, 0, c->stream>>>(
+            static_cast<double *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->M, A->N, beta,
+            threshold, ovf);
+    else
+        add_identity_kernel<float><<<grid, 256, 0, c->stream>>>(
+            static_cast<float *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->M, A->N, beta,
+            threshold, ovf);
+    if (!LAUNCH_OK("add_identity_kernel"))
+        return false;
+    ell_mark_device(A);
+    int hov = 0;
+    if (!read_flag(c, ovf, &hov))
+        return false;
+    if (hov)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "add_identity: a row needs more than M=%d entries",
+                       A->M);
+        return false;
+    }
+    return true;
+}
+
+bool ell_scale(const void *scale, bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B)
+{
+    if (!check_pair(A, B, "scale"))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A) || (B != A && !ell_to_device(B)))
+        return false;
+    if (B != A && B->M < A->M)
+    {
+        long long tot;
+        int maxrow = 0;
+        if (!ell_nnz_total(A, &tot, &maxrow))
+            return false;
+        if (maxrow > B->M)
+        {
+            b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "scale: output M=%d < row width %d", B->M,
+                           maxrow);
+            return false;
+        }
+    }
+    const int grid = rows_grid(c, A->N, 8);
+    const int copy = B != A;
+    if (A->matrix_precision == double_real)
+        scale_kernel<double><<<grid, 256, 0, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<double *>(B->d_value), B->d_index, B->d_nnz, B->ld, A->N,
+            *static_cast<const double *>(scale), copy);
+    else
+        scale_kernel<float><<<grid, 256, 0, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<float *>(B->d_value), B->d_index, B->d_nnz, B->ld, A->N,
+            *static_cast<const float *>(scale), copy);
+    if (!LAUNCH_OK("scale_kernel"))
+        return false;
+    ell_mark_device(B);
+    return true;
+}
+
+bool ell_threshold_new(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double threshold)
+{
+    if (!check_pair(A, B, "threshold"))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A) || !ell_to_device(B))
+        return false;
+    const int grid = rows_grid(c, A->N, 8);
+    if (A->matrix_precision == double_real)
+        threshold_kernel<double><<<grid, 256, 0, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<double *>(B->d_value), B->d_index, B->d_nnz, B->ld, A->N, threshold);
+    else
+        threshold_kernel<float><<<grid, 256, 0, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<float *>(B->d_value), B->d_index, B->d_nnz, B->ld, A->N, threshold);
+    if (!LAUNCH_OK("threshold_kernel"))
+        return false;
+    ell_mark_device(B);
+    return true;
+}
+
+bool ell_threshold(bml_matrix_ellpack_t *A, double threshold)
+{
+    // Stable in-place compaction: every write lands at or before the position
+    // being read within the same warp chunk, so aliasing A with B is safe.
+    return ell_threshold_new(A, A, threshold);
+}
+
+bool ell_copy(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B)
+{
+    if (!check_pair(A, B, "copy"))
+        return false;
+    if (A == B)
+        return true;
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A))
+        return false;
+    if (B->mirror == MIRROR_HOST_NEWER)
+        B->mirror = MIRROR_SYNCED; // overwritten entirely below
+    int *ovf = zeroed_flag(c);
+    if (!ovf)
+        return false;
+    const int grid = rows_grid(c, A->N, 8);
+    if (A->matrix_precision == double_real)
+        copy_kernel<double><<<grid, 256, 0, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<double *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, A->N, ovf);
+    else
+        copy_kernel<float><<<grid, 256, 0, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<float *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, A->N, ovf);
+    if (!LAUNCH_OK("copy_kernel"))
+        return false;
+    ell_mark_device(B);
+    if (B->M >= A->M)
+        return true;
+    int hov = 0;
+    if (!read_flag(c, ovf, &hov))
+        return false;
+    if (hov)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "copy: a row of A is wider than B's M=%d", B->M);
+        return false;
+    }
+    return true;
+}
+
+bool ell_trace(bml_matrix_ellpack_t *A, double *trace)
+{
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A))
+        return false;
+    double *d = static_cast<double *>(b200_scratch((size_t) A->N * sizeof(double)));
+    if (!d)
+        return false;
+    const int grid = rows_grid(c, A->N, 8);
+    if (A->matrix_precision == double_real)
+        diag_kernel<double><<<grid, 256, 0, c->stream>>>(static_cast<const double *>(A->d_value),
+                                                         A->d_index, A->d_nnz, A->ld, A->N, d);
+    else
+        diag_kernel<float><<<grid, 256, 0, c->stream>>>(static_cast<const float *>(A->d_value),
+                                                        A->d_index, A->d_nnz, A->ld, A->N, d);
+    double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
+    b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(d, nullptr, A->N, out);
+    if (!LAUNCH_OK("trace kernels"))
+        return false;
+    double *pin = reinterpret_cast<double *>(static_cast<unsigned char *>(c->pinned) + 3072);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream)) ||
+        !b200_sync())
+        return false;
+    *trace = pin[0];
+    return true;
+}
+
+bool ell_trace_mult(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *trace)
+{
+    if (!check_pair(A, B, "trace_mult"))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A) || !ell_to_device(B))
+        return false;
+    double *part = static_cast<double *>(b200_scratch((size_t) A->N * sizeof(double)));
+    if (!part)
+        return false;
+    int logts = 5;
+    while ((1 << logts) < 2 * B->M)
+        ++logts;
+    int warps_per_block = 4;
+    size_t smem = (size_t) warps_per_block * 2 * (1 << logts) * sizeof(int);
+    while (smem > c->smem_optin && warps_per_block > 1)
+    {
+        warps_per_block >>= 1;
+        smem >>= 1;
+    }
+    if (smem > c->smem_optin)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "trace_mult: B rows of width %d too wide", B->M);
+        return false;
+    }
+    const int grid = min(b200_ceil_div(A->N, warps_per_block), c->sm_count * 16);
+    if (A->matrix_precision == double_real)
+    {
+        auto k = trace_mult_kernel<double>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 32 * warps_per_block, smem, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<const double *>(B->d_value), B->d_index, B->d_nnz, B->ld, A->N, logts, part);
+    }
+    else
+    {
+        auto k = trace_mult_kernel<float>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 32 * warps_per_block, smem, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<const float *>(B->d_value), B->d_index, B->d_nnz, B->ld, A->N, logts, part);
+    }
+    double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
+    b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(part, nullptr, A->N, out);
+    if (!LAUNCH_OK("trace_mult kernels"))
+        return false;
+    double *pin = reinterpret_cast<double *>(static_cast<unsigned char *>(c->pinned) + 3072);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream)) ||
+        !b200_sync())
+        return false;
+    *trace = pin[0];
+    return true;
+}
+
+bool ell_transpose_new(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B)
+{
+    if (!check_pair(A, B, "transpose"))
+        return false;
+    if (A == B)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "transpose: output aliases input");
+        return false;
+    }
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A))
+        return false;
+    if (B->mirror == MIRROR_HOST_NEWER)
+        B->mirror = MIRROR_SYNCED;
+    int *ovf = zeroed_flag(c);
+    if (!ovf || !CUDA_OK(cudaMemsetAsync(B->d_nnz, 0, (size_t) B->N * sizeof(int), c->stream)))
+        return false;
+    const int grid = rows_grid(c, A->N, 8);
+    int pow2 = 1;
+    while (pow2 < B->M)
+        pow2 <<= 1;
+    const size_t sz = prec_size(A->matrix_precision);
+    const size_t smem = (size_t) pow2 * (sz + 4);
+    if (smem > c->smem_optin)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "transpose: M=%d too wide for the row sort", B->M);
+        return false;
+    }
+    const int sgrid = min(B->N, c->sm_count * 8);
+    if (A->matrix_precision == double_real)
+    {
+        transpose_scatter_kernel<double><<<grid, 256, 0, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->N,
+            static_cast<double *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, ovf);
+        auto k = row_sort_kernel<double>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<sgrid, 256, smem, c->stream>>>(static_cast<double *>(B->d_value), B->d_index, B->d_nnz,
+                                           B->ld, B->M, B->N, pow2);
+    }
+    else
+    {
+        transpose_scatter_kernel<float><<<grid, 256, 0, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->N,
+            static_cast<float *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, ovf);
+        auto k = row_sort_kernel<float>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<sgrid, 256, smem, c->stream>>>(static_cast<float *>(B->d_value), B->d_index, B->d_nnz,
+                                           B->ld, B->M, B->N, pow2);
+    }
+    if (!LAUNCH_OK("transpose kernels"))
+        return false;
+    ell_mark_device(B);
+    int hov = 0;
+    if (!read_flag(c, ovf, &hov))
+        return false;
+    if (hov)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "transpose: a column of A has more than M=%d entries",
+                       B->M);
+        return false;
+    }
+    return true;
+}
+
+bool ell_gershgorin(bml_matrix_ellpack_t *A, double *bounds)
+{
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A))
+        return false;
+    double *hi = static_cast<double *>(b200_scratch((size_t) 2 * A->N * sizeof(double)));
+    if (!hi)
+        return false;
+    double *lo = hi + A->N;
+    const int grid = rows_grid(c, A->N, 8);
+    if (A->matrix_precision == double_real)
+        gershgorin_kernel<double><<<grid, 256, 0, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->N, hi, lo);
+    else
+        gershgorin_kernel<float><<<grid, 256, 0, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->N, hi, lo);
+    double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
+    // emax starts at DBL_MIN and emin at DBL_MAX, as in the reference (:88-89).
+    b200_maxmin_rows_kernel<<<1, 1024, 0, c->stream>>>(hi, lo, A->N, DBL_MIN, DBL_MAX, out);
+    if (!LAUNCH_OK("gershgorin kernels"))
+        return false;
+    double *pin = reinterpret_cast<double *>(static_cast<unsigned char *>(c->pinned) + 3072);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream)) ||
+        !b200_sync())
+        return false;
+    bounds[0] = pin[1]; // emin
+    bounds[1] = pin[0]; // emax
+    return true;
+}

@@ -1,0 +1,316 @@
+/*
+ * bml_b200.h -- public C ABI of libbml_b200.so, a B200 (sm_100a) implementation
+ * of bml's thresholded sparse matrix path (ELLPACK-R and ELLBLOCK) that links in
+ * place of the reference libbml for that path.
+ *
+ * Every function below that carries a bml_ name has the reference's name,
+ * signature, argument meaning and ownership rules; the citation beside each one
+ * is the reference declaration it replaces (paths relative to the bml tree,
+ * src/C-interface/).  Matrices live in device memory; every computing call runs
+ * hand-written CUDA kernels on the current device and returns when its result is
+ * complete.  There is no CPU fallback: without a usable GPU a call fails.
+ *
+ * Errors.  The reference logs, prints a backtrace and exit()s on any error
+ * (bml_logger.c:92-116).  This library never exits or traps: it prints the same
+ * kind of message to stderr, records a status that bml_b200_last_error() returns,
+ * and leaves its outputs in a defined state (see each call).  Row overflow
+ * (a result row wider than the output's M) is detected before anything is
+ * written past M; the reference writes into the next row first
+ * (ellpack/bml_multiply_ellpack_typed.c:301-330).
+ *
+ * Types and precisions.  ELLPACK and ELLBLOCK matrices in single_real and
+ * double_real are supported.  Other types and precisions set
+ * BML_B200_ERR_UNSUPPORTED and return NULL/0.
+ */
+#ifndef BML_B200_H
+#define BML_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BML_B200_API __attribute__((visibility("default")))
+#else
+#define BML_B200_API
+#endif
+
+/* ---- types: same enumerators, same order, same struct layouts as the
+ * reference (bml_types.h:7-129), so callers compiled against bml.h link
+ * unchanged. ---------------------------------------------------------------- */
+typedef enum
+{
+    type_uninitialized,
+    dense,
+    ellpack,
+    ellblock,
+    csr,
+    distributed2d
+} bml_matrix_type_t;
+
+typedef enum
+{
+    precision_uninitialized,
+    single_real,
+    double_real,
+    single_complex,
+    double_complex
+} bml_matrix_precision_t;
+
+typedef enum
+{
+    dense_row_major,
+    dense_column_major
+} bml_dense_order_t;
+
+typedef void bml_vector_t;
+typedef void bml_matrix_t;
+
+typedef struct
+{
+    int N_rows;
+    int N_cols;
+    int N_nz_max;
+    int *bsizes;
+    int NB;
+} bml_matrix_dimension_t;
+
+typedef enum
+{
+    sequential,
+    distributed,
+    graph_distributed
+} bml_distribution_mode_t;
+
+struct bml_domain_t
+{
+    int totalProcs;
+    int totalRows;
+    int totalCols;
+    int globalRowMin;
+    int globalRowMax;
+    int globalRowExtent;
+    int maxLocalExtent;
+    int minLocalExtent;
+    int *localRowMin;
+    int *localRowMax;
+    int *localRowExtent;
+    int *localElements;
+    int *localDispl;
+};
+typedef struct bml_domain_t bml_domain_t;
+
+typedef enum
+{
+    BML_LOG_DEBUG,
+    BML_LOG_INFO,
+    BML_LOG_WARNING,
+    BML_LOG_ERROR
+} bml_log_level_t;
+
+/* ---- allocation (bml_allocate.h) ---------------------------------------- */
+BML_B200_API void *bml_allocate_memory(size_t s);                 /* bml_allocate.h:13 */
+BML_B200_API void *bml_noinit_allocate_memory(size_t s);          /* bml_allocate.h:16 */
+BML_B200_API void bml_free_memory(void *ptr);                     /* bml_allocate.h:23 */
+BML_B200_API void bml_free_ptr(void **ptr);                       /* bml_allocate.h:26 */
+BML_B200_API int bml_allocated(bml_matrix_t *A);                  /* bml_allocate.h:10 */
+BML_B200_API void bml_deallocate(bml_matrix_t **A);               /* bml_allocate.h:29 */
+BML_B200_API void bml_deallocate_domain(bml_domain_t *D);         /* bml_allocate.h:32 */
+BML_B200_API void bml_clear(bml_matrix_t *A);                     /* bml_allocate.h:35 */
+BML_B200_API bml_matrix_t *bml_noinit_matrix(bml_matrix_type_t matrix_type,
+    bml_matrix_precision_t matrix_precision, int N, int M,
+    bml_distribution_mode_t distrib_mode);                        /* bml_allocate.h:44 */
+BML_B200_API bml_matrix_t *bml_zero_matrix(bml_matrix_type_t matrix_type,
+    bml_matrix_precision_t matrix_precision, int N, int M,
+    bml_distribution_mode_t distrib_mode);                        /* bml_allocate.h:51 */
+BML_B200_API bml_matrix_t *bml_random_matrix(bml_matrix_type_t matrix_type,
+    bml_matrix_precision_t matrix_precision, int N, int M,
+    bml_distribution_mode_t distrib_mode);                        /* bml_allocate.h:58 */
+BML_B200_API bml_matrix_t *bml_banded_matrix(bml_matrix_type_t matrix_type,
+    bml_matrix_precision_t matrix_precision, int N, int M,
+    bml_distribution_mode_t distrib_mode);                        /* bml_allocate.h:65 */
+BML_B200_API bml_matrix_t *bml_identity_matrix(bml_matrix_type_t matrix_type,
+    bml_matrix_precision_t matrix_precision, int N, int M,
+    bml_distribution_mode_t distrib_mode);                        /* bml_allocate.h:72 */
+BML_B200_API bml_domain_t *bml_default_domain(int N, int M,
+    bml_distribution_mode_t distrib_mode);                        /* bml_allocate.h:79 */
+
+/* ---- introspection (bml_introspection.h) -------------------------------- */
+BML_B200_API bml_matrix_type_t bml_get_type(bml_matrix_t *A);               /* :8  */
+BML_B200_API bml_matrix_type_t bml_get_deep_type(bml_matrix_t *A);          /* :11 */
+BML_B200_API bml_matrix_precision_t bml_get_precision(bml_matrix_t *A);     /* :14 */
+BML_B200_API int bml_get_N(bml_matrix_t *A);                                /* :17 */
+BML_B200_API int bml_get_M(bml_matrix_t *A);                                /* :20 */
+BML_B200_API int bml_get_NB(bml_matrix_t *A);                               /* :23 */
+BML_B200_API int bml_get_row_bandwidth(bml_matrix_t *A, int i);             /* :26 */
+BML_B200_API int bml_get_bandwidth(bml_matrix_t *A);                        /* :30 */
+BML_B200_API double bml_get_sparsity(bml_matrix_t *A, double threshold);    /* :33 */
+BML_B200_API bml_distribution_mode_t bml_get_distribution_mode(bml_matrix_t *A); /* :37 */
+
+/* ---- copy / convert / import / export / elements ------------------------ */
+BML_B200_API bml_matrix_t *bml_copy_new(bml_matrix_t *A);                   /* bml_copy.h:8  */
+BML_B200_API void bml_copy(bml_matrix_t *A, bml_matrix_t *B);               /* bml_copy.h:11 */
+BML_B200_API bml_matrix_t *bml_convert(bml_matrix_t *A, bml_matrix_type_t matrix_type,
+    bml_matrix_precision_t matrix_precision, int M,
+    bml_distribution_mode_t distrib_mode);                                  /* bml_convert.h:8 */
+BML_B200_API bml_matrix_t *bml_import_from_dense(bml_matrix_type_t matrix_type,
+    bml_matrix_precision_t matrix_precision, bml_dense_order_t order, int N, int M,
+    void *A, double threshold, bml_distribution_mode_t distrib_mode);      /* bml_import.h:8 */
+BML_B200_API void *bml_export_to_dense(bml_matrix_t *A, bml_dense_order_t order); /* bml_export.h:8 */
+BML_B200_API void *bml_get_element(bml_matrix_t *A, int i, int j);          /* bml_getters.h:8  */
+BML_B200_API void *bml_get_row(bml_matrix_t *A, int i);                     /* bml_getters.h:13 */
+BML_B200_API void *bml_get_diagonal(bml_matrix_t *A);                       /* bml_getters.h:17 */
+BML_B200_API void bml_set_element_new(bml_matrix_t *A, int i, int j, void *value); /* bml_setters.h:8  */
+BML_B200_API void bml_set_element(bml_matrix_t *A, int i, int j, void *value);     /* bml_setters.h:14 */
+BML_B200_API void bml_set_row(bml_matrix_t *A, int i, void *row, double threshold); /* bml_setters.h:20 */
+BML_B200_API void bml_set_diagonal(bml_matrix_t *A, void *diagonal, double threshold); /* bml_setters.h:26 */
+
+/* ---- the thresholded sparse path ---------------------------------------- */
+/* C <- alpha*A*B + beta*C, thresholded (bml_multiply.h:9; bml_multiply.c:27-59). */
+BML_B200_API void bml_multiply(bml_matrix_t *A, bml_matrix_t *B, bml_matrix_t *C,
+    double alpha, double beta, double threshold);
+/* X2 <- X*X thresholded; returns malloc'd double[2] = {tr X, tr X2}, released
+ * with bml_free_memory() (bml_multiply.h:18; bml_multiply.c:71-101). */
+BML_B200_API void *bml_multiply_x2(bml_matrix_t *X, bml_matrix_t *X2, double threshold);
+/* C <- A*B thresholded, diagonal kept (bml_multiply.h:24; bml_multiply.c:114-144). */
+BML_B200_API void bml_multiply_AB(bml_matrix_t *A, bml_matrix_t *B, bml_matrix_t *C,
+    double threshold);
+/* As bml_multiply_AB, doubling the threshold until every row fits in C's M
+ * (bml_multiply.h:31; ellpack/bml_multiply_ellpack_typed.c:566-707). */
+BML_B200_API void bml_multiply_adjust_AB(bml_matrix_t *A, bml_matrix_t *B,
+    bml_matrix_t *C, double threshold);
+/* A <- alpha*A + beta*B thresholded (bml_add.h:8; bml_add.c:26-57). */
+BML_B200_API void bml_add(bml_matrix_t *A, bml_matrix_t *B, double alpha, double beta,
+    double threshold);
+/* A <- A + beta*I (bml_add.h:22); A <- alpha*A + beta*I (bml_add.h:27). */
+BML_B200_API void bml_add_identity(bml_matrix_t *A, double beta, double threshold);
+BML_B200_API void bml_scale_add_identity(bml_matrix_t *A, double alpha, double beta,
+    double threshold);
+/* In-place and copying threshold (bml_threshold.h:8-12; bml_threshold.c:30-89). */
+BML_B200_API bml_matrix_t *bml_threshold_new(bml_matrix_t *A, double threshold);
+BML_B200_API void bml_threshold(bml_matrix_t *A, double threshold);
+/* tr A and tr(A*B) (bml_trace.h:9-13; bml_trace.c:20-88). */
+BML_B200_API double bml_trace(bml_matrix_t *A);
+BML_B200_API double bml_trace_mult(bml_matrix_t *A, bml_matrix_t *B);
+/* Transpose (bml_transpose.h:9-12; bml_transpose.c:21-85). */
+BML_B200_API bml_matrix_t *bml_transpose_new(bml_matrix_t *A);
+BML_B200_API void bml_transpose(bml_matrix_t *A);
+/* Scaling (bml_scale.h:8-17). scale_factor points to a value of A's precision. */
+BML_B200_API bml_matrix_t *bml_scale_new(void *scale_factor, bml_matrix_t *A);
+BML_B200_API void bml_scale(void *scale_factor, bml_matrix_t *A, bml_matrix_t *B);
+BML_B200_API void bml_scale_inplace(void *scale_factor, bml_matrix_t *A);
+/* Gershgorin bounds -> malloc'd double[2] = {emin, emax}; normalisation to
+ * (emax*I - A)/(emax - emin) (bml_normalize.h:9-15). */
+BML_B200_API void *bml_gershgorin(bml_matrix_t *A);
+BML_B200_API void bml_normalize(bml_matrix_t *A, double mineval, double maxeval);
+
+/* ---- ELLBLOCK block partition (ellblock/bml_allocate_ellblock.h:199-210) -- */
+BML_B200_API void bml_set_block_sizes(int *bsize, int nb, int mb);
+BML_B200_API int *bml_get_block_sizes(int N, int M);
+BML_B200_API int bml_get_nb(void);
+BML_B200_API int bml_get_mb(void);
+
+/* Forget the process-wide block partition so that another can be set (the
+ * reference allows one per process; no counterpart there). */
+BML_B200_API void bml_b200_reset_block_sizes(void);
+
+/* ---- init / shutdown / logging / printing -------------------------------- */
+BML_B200_API void bml_init(void);                                  /* bml_init.h:12 (non-MPI form) */
+BML_B200_API void bml_shutdown(void);                              /* bml_shutdown.h:8 */
+BML_B200_API void bml_log(bml_log_level_t log_level, char *format, ...);  /* bml_logger.h:24 */
+BML_B200_API void bml_log_location(bml_log_level_t log_level, char *filename,
+    int linenumber, char *format, ...);                            /* bml_logger.h:29 */
+BML_B200_API char *bml_version(void);                              /* bml_logger.h:36 */
+BML_B200_API void bml_print_version(void);                         /* bml_logger.h:39 */
+BML_B200_API void bml_print_dense_matrix(int N, bml_matrix_precision_t matrix_precision,
+    bml_dense_order_t order, void *A, int i_l, int i_u, int j_l, int j_u); /* bml_utilities.h:9 */
+BML_B200_API void bml_print_bml_matrix(bml_matrix_t *A, int i_l, int i_u, int j_l,
+    int j_u);                                                      /* bml_utilities.h:31 */
+BML_B200_API void bml_read_bml_matrix(bml_matrix_t *A, char *filename);   /* bml_utilities.h:38 */
+BML_B200_API void bml_write_bml_matrix(bml_matrix_t *A, char *filename);  /* bml_utilities.h:42 */
+BML_B200_API int bml_sqrtint(const int x);                         /* bml_utilities.h:46 */
+
+/* ======================================================================== *
+ * B200 extensions.  None of these exists in the reference; they give callers
+ * status codes, raw-array transfer and the SP2 solver that consumers of the
+ * reference write themselves.
+ * ======================================================================== */
+enum
+{
+    BML_B200_OK = 0,
+    BML_B200_ERR_NO_DEVICE = 1,    /* no CUDA device, or the kernels do not load */
+    BML_B200_ERR_CUDA = 2,         /* a CUDA call failed */
+    BML_B200_ERR_INVALID = 3,      /* bad argument (NULL, size mismatch, index out of range) */
+    BML_B200_ERR_UNSUPPORTED = 4,  /* matrix type or precision outside this library */
+    BML_B200_ERR_ROW_OVERFLOW = 5, /* a result row needs more than M entries */
+    BML_B200_ERR_ALLOC = 6,        /* device or host allocation failed */
+    BML_B200_ERR_TIMEOUT = 7       /* a bounded device-side wait ran out */
+};
+
+/* Status of the most recent failing call on this thread (0 if none since the
+ * last clear), its text, and a reset. */
+BML_B200_API int bml_b200_last_error(void);
+BML_B200_API const char *bml_b200_error_string(int status);
+BML_B200_API void bml_b200_clear_error(void);
+/* Suppress (0) or enable (1, default) the stderr message printed on error. */
+BML_B200_API void bml_b200_set_verbose(int on);
+
+/* Status-returning X^2: same semantics as bml_multiply_x2, traces written to
+ * trace[0..1].  On ROW_OVERFLOW each overflowing row keeps its first M entries
+ * (in the reference's first-touch order) and the traces are still exact. */
+BML_B200_API int bml_b200_multiply_x2(bml_matrix_t *X, bml_matrix_t *X2,
+    double threshold, double *trace);
+/* Largest row width that the last X^2 / multiply on this thread needed before
+ * truncation to M (lets a caller size M exactly after ROW_OVERFLOW). */
+BML_B200_API int bml_b200_last_required_M(void);
+
+/* Raw ELLPACK transfer between the device matrix and caller host arrays laid
+ * out like the reference (row-major value[N*M], index[N*M], nnz[N]). */
+BML_B200_API int bml_b200_ellpack_upload(bml_matrix_t *A, const void *value,
+    const int *index, const int *nnz);
+BML_B200_API int bml_b200_ellpack_download(bml_matrix_t *A, void *value, int *index,
+    int *nnz);
+/* Device pointers and row stride (elements) of an ELLPACK matrix. */
+BML_B200_API int bml_b200_ellpack_device_arrays(bml_matrix_t *A, void **d_value,
+    int **d_index, int **d_nnz, int *ld);
+/* Number of non-zeros of a matrix (sum of nnz), computed on the device. */
+BML_B200_API long long bml_b200_nnz(bml_matrix_t *A);
+/* Wait for all work this library queued. */
+BML_B200_API int bml_b200_synchronize(void);
+/* Device properties this library uses: SM count, device ordinal. */
+BML_B200_API int bml_b200_device_info(int *sm_count, int *device);
+
+/* SP2 density-matrix purification (Niklasson, PRB 66, 155115 (2002)), the
+ * consumer loop around bml_multiply_x2 that PROGRESS/LATTE write on top of bml:
+ *   X0 = (emax I - H)/(emax - emin) with Gershgorin bounds of H;
+ *   repeat: X2 = X*X (thresholded), t = tr X, t2 = tr X2;
+ *           X <- X2        if |t2 - occ| <= |2t - t2 - occ|,
+ *           X <- 2X - X2   otherwise (thresholded add);
+ *   stop when |t - t2| < tol, when the idempotency error |t - t2| has not
+ *   decreased for `stall` iterations (stall <= 0 disables), or at maxiter.
+ * H is not modified.  D receives the final X and must have H's type and
+ * precision (its M bounds every iterate; overflow stops the solve with
+ * ROW_OVERFLOW).  info (may be NULL) receives: [0] iterations run, [1] stop
+ * rule (1 tol, 2 stall, 3 maxiter, 4 error), [2] tr D, [3] last |t - t2|,
+ * [4] max row width seen, [5] seconds spent in X^2 calls. */
+BML_B200_API int bml_b200_sp2(bml_matrix_t *H, bml_matrix_t *D, double threshold,
+    double occupation, int maxiter, double tol, int stall, double *info);
+
+/* Synthetic Hamiltonians (host arrays in the reference ELLPACK layout), seeded
+ * splitmix64 + Box-Muller, symmetric.  Used to give the oracle and this
+ * library byte-identical inputs.
+ *   kind 1: 1-D chain, H_ii ~ U[-1,1], H_ij = u exp(-|i-j|/4), 0<|i-j|<=16.
+ *   kind 2: L^3 cubic lattice (x fastest), neighbours with |r| <= radius,
+ *           H_ij = -exp(-d)(1 + 0.1 g), H_ii ~ N(0,1); first N sites kept.
+ * Returns the number of rows written, or -1 if a row needs more than M. */
+BML_B200_API int bml_b200_gen_chain(int N, int M, unsigned long long seed,
+    double *value, int *index, int *nnz);
+BML_B200_API int bml_b200_gen_lattice(int L, int radius, int N, int M,
+    unsigned long long seed, double *value, int *index, int *nnz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BML_B200_H */
