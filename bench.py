@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark: SP2 density-matrix purification on the ELLPACK N=64000 lattice
+Hamiltonian (40^3 sites, neighbours within radius 3, threshold 1e-5,
+occupation N/2), FP64, through libbml_b200's C ABI.
+
+One step = one SP2 run from H: Gershgorin bounds, X0 = (emax I - H)/(emax -
+emin), then SP2_ITERS iterations of X^2 (thresholded, traces) and the branch
+update X <- X^2 or X <- 2X - X^2.  The full solve of this Hamiltonian fills in
+to a dense 64000^2 matrix (the system is metallic at half filling: its density
+matrix decays too slowly for the threshold to keep rows sparse), so the timed
+solve is the first SP2_ITERS iterations, in which rows grow from 123 to ~1500
+entries; the stop rule |tr X - tr X^2| < 1e-8 is not reached within them.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) each rank runs an independent replica on its own GPU
+(the path does not shard across GPUs here); rank 0 prints one JSON line with
+the slowest rank's time.  `value` is seconds per SP2 run for the whole job
+(device time of K steps on every rank / (N*K) runs).  `e2e` is the same
+metric through the C ABI with host buffers: H uploaded from host arrays and
+the density matrix downloaded every step.  --impl reference runs the reference
+bml CPU library (built from its sources into oracle/_ref) on the host cores
+with the same inputs and loop.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L, RADIUS, SEED = 40, 3, 0
+N = L ** 3
+M_H = 256          # stored width of H (interior rows hold 123)
+M_X = 2048         # stored width of the iterates (iteration 5 needs 1792)
+THRESHOLD = 1e-5
+OCC = N / 2.0
+SP2_ITERS = 4
+METRIC = "s per SP2 solve & X² HBM GB/s, ELLPACK N=64K: FP64 vs mixed at ≤1e-6 err"
+WORKLOAD = ("SP2 on the 40^3 lattice Hamiltonian (N=64000, radius 3, M=%d, thr 1e-5, occ N/2, FP64), "
+            "first %d iterations from X0 (the full solve fills in to dense)" % (M_X, SP2_ITERS))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def inputs():
+    import bml_b200 as B
+    return B.gen_lattice(L, RADIUS, N, M_H, SEED)
+
+
+# ---------------------------------------------------------------------------
+# libbml_b200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args, rank, world, local):
+    import numpy as np
+    import bml_b200 as B
+    B.check(B.lib.bml_b200_set_device(local))
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        pg = dist
+    v, ix, nz = inputs()
+    H = B.Ellpack.from_arrays(v, ix, nz, N, M_H)
+    D = B.Ellpack(N, M_X)
+    info = (C.c_double * 6)()
+    dv = np.zeros(N * M_X)
+    dix = np.zeros(N * M_X, np.int32)
+    dnz = np.zeros(N, np.int32)
+    # pinned host buffers for the end-to-end leg
+    import torch
+    h_v = torch.from_numpy(v).pin_memory().numpy()
+    h_ix = torch.from_numpy(ix).pin_memory().numpy()
+    h_nz = torch.from_numpy(nz).pin_memory().numpy()
+    o_v = torch.empty(N * M_X, dtype=torch.float64).pin_memory().numpy()
+    o_ix = torch.empty(N * M_X, dtype=torch.int32).pin_memory().numpy()
+    o_nz = torch.empty(N, dtype=torch.int32).pin_memory().numpy()
+
+    def step():
+        st = B.lib.bml_b200_sp2(H.h, D.h, THRESHOLD, OCC, SP2_ITERS, 1e-8, 0, info)
+        B.check(st)
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step()
+    B.check(B.lib.bml_b200_synchronize())
+    # X^2 roofline inputs from the last warm-up run
+    x2_seconds_per_run = info[5]
+    widths = info[4]
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = B.lib.bml_b200_launch_count()
+    B.check(B.lib.bml_b200_event_record(0))
+    for _ in range(args.steps):
+        step()
+    B.check(B.lib.bml_b200_event_record(1))
+    ms = B.event_ms(0, 1)
+    launches = B.lib.bml_b200_launch_count() - launches0
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(ms)
+    sec_per_step = ms / 1e3 / args.steps
+    value = sec_per_step / world  # whole job: world replicas run concurrently
+
+    # end-to-end through the C ABI with host buffers
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 3))):
+        B.check(B.lib.bml_b200_ellpack_upload(H.h, h_v.ctypes.data_as(C.c_void_p),
+                                             h_ix.ctypes.data_as(C.POINTER(C.c_int)),
+                                             h_nz.ctypes.data_as(C.POINTER(C.c_int))))
+        step()
+        B.check(B.lib.bml_b200_ellpack_download(D.h, o_v.ctypes.data_as(C.c_void_p),
+                                               o_ix.ctypes.data_as(C.POINTER(C.c_int)),
+                                               o_nz.ctypes.data_as(C.POINTER(C.c_int))))
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e = (time.perf_counter() - t0) / e2e_steps
+    e2e = max_over_ranks(e2e) / world
+
+    # per-X^2 roofline: one X^2 on the iterate of iteration SP2_ITERS-1
+    rl = x2_roofline(B, H, info)
+    res = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded splitmix64 lattice Hamiltonian, generated on the host)",
+        "config": {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
+                   "sp2_iterations": SP2_ITERS, "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (iterates ~0.8-1.3 GB)"},
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(v.nbytes + ix.nbytes + nz.nbytes),
+                "d2h_bytes_per_step": int(o_v.nbytes + o_ix.nbytes + o_nz.nbytes)},
+        "gpu_launches": int(launches),
+        "roofline": rl,
+        "clocks": clk,
+        "sp2": {"iterations": info[0], "trace": info[2], "idempotency": info[3], "max_row_width": widths,
+                "x2_seconds_per_run": x2_seconds_per_run},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res["cpu_baseline"] = cpu_baseline()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return res if rank == 0 else None
+
+
+def x2_roofline(B, H, info):
+    """Algorithmic bytes of one X^2 on the last SP2 iterate over its device
+    time (CUDA events on the library stream)."""
+    import numpy as np
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs")
+    src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    # rebuild the iterate entering iteration SP2_ITERS-1
+    X = B.Ellpack(N, M_X)
+    info2 = (C.c_double * 6)()
+    B.check(B.lib.bml_b200_sp2(H.h, X.h, THRESHOLD, OCC, SP2_ITERS - 1, 1e-8, 0, info2))
+    X2 = B.Ellpack(N, M_X)
+    tr = (C.c_double * 2)()
+    B.check(B.lib.bml_b200_multiply_x2(X.h, X2.h, THRESHOLD, tr))  # warm
+    reps = 3
+    B.check(B.lib.bml_b200_event_record(2))
+    for _ in range(reps):
+        B.check(B.lib.bml_b200_multiply_x2(X.h, X2.h, THRESHOLD, tr))
+    B.check(B.lib.bml_b200_event_record(3))
+    t = B.event_ms(2, 3) / 1e3 / reps
+    nnz_x = B.lib.bml_b200_nnz(X.h)
+    nnz_x2 = B.lib.bml_b200_nnz(X2.h)
+    xv, xix, xnz = X.download()
+    # product terms P = sum_i sum_{j in row i} nnz_j
+    P = 0
+    rows = xix.reshape(N, M_X)
+    for i in range(0, N, 4096):
+        blk = rows[i:i + 4096]
+        mask = np.arange(M_X)[None, :] < xnz[i:i + 4096, None]
+        P += int(xnz[blk[mask]].astype(np.int64).sum())
+    bytes_alg = 12 * nnz_x + 12 * nnz_x2 + 8 * N
+    achieved = bytes_alg / t / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_source": src, "traffic": None,
+            "kernel": "one ELLPACK X^2 call (tier kernels together) on the SP2 iterate of iteration %d"
+                      % (SP2_ITERS - 1),
+            "x2_seconds": t, "nnz_x": int(nnz_x), "nnz_x2": int(nnz_x2), "products": P,
+            "fp64_gflops": 2.0 * P / t / 1e9, "products_per_s": P / t,
+            "gathered_gbs": 12.0 * P / t / 1e9}
+
+
+# ---------------------------------------------------------------------------
+# reference (CPU) arm and the CPU baseline
+# ---------------------------------------------------------------------------
+def _omp_env():
+    ncpu = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncpu))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    os.environ.setdefault("OMP_STACKSIZE", "64M")
+    return int(os.environ["OMP_NUM_THREADS"])
+
+
+def ref_sp2(O, H, D, X2, iters):
+    """The SP2 loop of bml_b200_sp2, on the reference library."""
+    lib = O.ref()
+    lib.bml_copy(H, D)
+    b = lib.bml_gershgorin(H)
+    bb = (C.c_double * 2).from_address(b)
+    emin, emax = bb[0], bb[1]
+    lib.bml_free_memory(b)
+    lib.bml_normalize(D, emin, emax)
+    for _ in range(iters):
+        tr = O.ref_x2(D, X2, THRESHOLD)
+        if abs(tr[1] - OCC) <= abs(2 * tr[0] - tr[1] - OCC):
+            lib.bml_copy(X2, D)
+        else:
+            lib.bml_add(D, X2, 2.0, -1.0, THRESHOLD)
+    return tr
+
+
+def _ref_setup():
+    threads = _omp_env()
+    from oracle import oracle as O
+    if not O.available():
+        raise RuntimeError("oracle/_ref is not built")
+    import numpy as np
+    v, ix, nz = inputs()
+    # the reference copies whole padded rows: H and the iterates share M
+    pad = lambda a: np.pad(a.reshape(N, M_H), ((0, 0), (0, M_X - M_H))).reshape(-1)
+    H = O.ref_ellpack(pad(v), pad(ix), nz, N, M_X)
+    D = O.ref().bml_zero_matrix(2, 2, N, M_X, 0)
+    X2 = O.ref().bml_zero_matrix(2, 2, N, M_X, 0)
+    return O, H, D, X2, threads
+
+
+def cpu_baseline():
+    O, H, D, X2, threads = _ref_setup()
+    t0 = time.perf_counter()
+    ref_sp2(O, H, D, X2, SP2_ITERS)
+    dt = time.perf_counter() - t0
+    return {"value": dt, "unit": "s", "cores": threads, "kind": "reference",
+            "sample": "one full step (SP2 from H, %d iterations) on the reference bml ELLPACK "
+                      "OpenMP CPU path, built -O3 -std=c99 -fopenmp from its sources" % SP2_ITERS}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    O, H, D, X2, threads = _ref_setup()
+    warm = max(0, min(args.warmup, 1))
+    steps = max(1, min(args.steps, 2))
+    for _ in range(warm):
+        ref_sp2(O, H, D, X2, SP2_ITERS)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref_sp2(O, H, D, X2, SP2_ITERS)
+    dt = (time.perf_counter() - t0) / steps
+    sample = ("%d timed step(s) after %d warm-up, each a full SP2 run from H (%d iterations), reference "
+              "bml ELLPACK OpenMP CPU path on %d threads" % (steps, warm, SP2_ITERS, threads))
+    return {"impl": "reference", "metric": METRIC, "value": dt, "unit": "s", "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": dt * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded splitmix64 lattice Hamiltonian)",
+            "config": {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
+                       "sp2_iterations": SP2_ITERS},
+            "cpu_baseline": {"value": dt, "unit": "s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": dt, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_b200(args, rank, world, local)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

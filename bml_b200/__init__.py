@@ -108,6 +108,11 @@ _PROTOS = {
     "bml_b200_gen_chain": (_i, [_i, _i, C.c_ulonglong, _dp, _ip, _ip]),
     "bml_b200_gen_lattice": (_i, [_i, _i, _i, _i, C.c_ulonglong, _dp, _ip, _ip]),
     "bml_b200_reset_block_sizes": (None, []),
+    "bml_b200_last_tier_counts": (_i, [_ip, _i]),
+    "bml_b200_set_device": (_i, [_i]),
+    "bml_b200_launch_count": (C.c_ulonglong, []),
+    "bml_b200_event_record": (_i, [_i]),
+    "bml_b200_event_elapsed": (_i, [_i, _i, C.POINTER(C.c_float)]),
 }
 
 for _name, (_res, _args) in _PROTOS.items():
@@ -231,6 +236,18 @@ def multiply_x2(X, X2, threshold):
     tr = (C.c_double * 2)()
     st = lib.bml_b200_multiply_x2(X.h, X2.h, threshold, tr)
     return st, (tr[0], tr[1])
+
+
+def last_tier_counts():
+    out = (C.c_int * 8)()
+    n = lib.bml_b200_last_tier_counts(out, 8)
+    return list(out[:n])
+
+
+def event_ms(a, b):
+    ms = C.c_float()
+    check(lib.bml_b200_event_elapsed(a, b, C.byref(ms)))
+    return ms.value
 
 
 def device_info():

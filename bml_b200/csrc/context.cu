@@ -10,6 +10,10 @@ namespace {
 
 thread_local int g_last_error = BML_B200_OK;
 int g_verbose = 1;
+int g_requested_device = -1;
+unsigned long long g_launches = 0;
+cudaEvent_t g_events[64];
+bool g_events_ready = false;
 
 B200Context g_ctx;
 bool g_ctx_ready = false;
@@ -17,6 +21,8 @@ bool g_ctx_failed = false;
 std::mutex g_ctx_mutex;
 
 } // namespace
+
+void b200_count_launch() { ++g_launches; }
 
 void b200_set_error(int status, const char *fmt, ...)
 {
@@ -37,6 +43,8 @@ bool b200_cuda_ok(cudaError_t err, const char *what, const char *file, int line)
 {
     if (err == cudaSuccess)
         return true;
+    if (g_ctx_failed)
+        return false;
     b200_set_error(BML_B200_ERR_CUDA, "%s failed at %s:%d: %s", what, file, line,
                    cudaGetErrorString(err));
     return false;
@@ -64,6 +72,8 @@ B200Context *b200_ctx()
         return nullptr;
     }
     memset(&g_ctx, 0, sizeof(g_ctx));
+    if (g_requested_device >= 0 && !CUDA_OK(cudaSetDevice(g_requested_device)))
+        return nullptr;
     if (!CUDA_OK(cudaGetDevice(&g_ctx.device)))
         return nullptr;
     cudaDeviceProp prop;
@@ -166,6 +176,47 @@ int bml_b200_device_info(int *sm_count, int *device)
 }
 
 void bml_init(void) { (void) b200_ctx(); }
+
+int bml_b200_set_device(int device)
+{
+    if (g_ctx_ready && g_ctx.device != device)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "set_device(%d) after the library started on device %d",
+                       device, g_ctx.device);
+        return BML_B200_ERR_INVALID;
+    }
+    g_requested_device = device;
+    return BML_B200_OK;
+}
+
+unsigned long long bml_b200_launch_count(void) { return g_launches; }
+
+int bml_b200_event_record(int slot)
+{
+    B200Context *c = b200_ctx();
+    if (!c)
+        return b200_get_error();
+    if (slot < 0 || slot >= 64)
+        return BML_B200_ERR_INVALID;
+    if (!g_events_ready)
+    {
+        for (int e = 0; e < 64; ++e)
+            if (!CUDA_OK(cudaEventCreate(&g_events[e])))
+                return b200_get_error();
+        g_events_ready = true;
+    }
+    return CUDA_OK(cudaEventRecord(g_events[slot], c->stream)) ? BML_B200_OK : b200_get_error();
+}
+
+int bml_b200_event_elapsed(int a, int b, float *ms)
+{
+    if (!g_events_ready || a < 0 || b < 0 || a >= 64 || b >= 64 || !ms)
+        return BML_B200_ERR_INVALID;
+    if (!CUDA_OK(cudaEventSynchronize(g_events[b])) ||
+        !CUDA_OK(cudaEventElapsedTime(ms, g_events[a], g_events[b])))
+        return b200_get_error();
+    return BML_B200_OK;
+}
 
 void bml_shutdown(void)
 {

@@ -7,53 +7,38 @@
 // then the touched columns are visited in first-touch order and kept when
 // k == i or |x| > threshold (typed.h:73, strict), and tr A / tr C are summed.
 //
-// B200 design.  A team of W warps owns one output row.  The team walks jp in
-// order; within one jp every k is distinct, so the lanes update their
-// accumulator slots without races, and a team barrier between consecutive
-// jp keeps every x[k] summed in exactly the reference order.  Products and
-// sums use __dmul_rn/__dadd_rn (no FMA contraction), matching the reference
-// build (-std=c99, no -mfma), so each call is bit-identical to the reference
-// on the same input.  New keys of a jp are appended to an order list with a
-// warp ballot + popcount prefix (and a cross-warp prefix for W > 1), which
-// rebuilds the reference's first-touch output order without sorting.
+// B200 design.  A team of warps owns one output row and walks jp in order.
+// Within one jp every k is distinct, so the lanes update their accumulator
+// slots without races; a barrier between consecutive units of work keeps every
+// x[k] summed in exactly the reference order.  Products and sums use
+// __dmul_rn/__dadd_rn (no FMA contraction), matching the reference build
+// (-std=c99, no -mfma), so each call is bit-identical to the reference on the
+// same input.  New keys are appended to an order list with a warp ballot +
+// popcount prefix (plus a cross-warp prefix), which rebuilds the reference's
+// first-touch output order without sorting.
 //
-// Three tiers, chosen per row by a planning kernel:
-//   tier A  one warp per row, 1024-slot shared-memory hash (rows whose
-//           product count already bounds their width by 640);
-//   tier B  8 warps per row, 8192-slot shared-memory hash (optimistic: a row
-//           whose distinct columns exceed 5/8 of the table is handed on);
-//   tier C  8 warps per row, dense accumulator over all N columns in global
-//           memory (any width; the reference's own x[N]/ix[N]/jx[N] scheme).
-// All tiers are persistent grids that pull rows from device-side lists, so a
+// Rows of B are staged into shared memory by TMA bulk copies
+// (cp.async.bulk, completion on an mbarrier), STAGES units ahead of the team,
+// so the gather latency overlaps the hash work of the preceding units.
+//
+// Tiers, chosen per row by a planning kernel from a bound or an estimate of
+// the row's distinct columns (the previous call's counts, when the matrix
+// size matches), each handing rows that outgrow it to the next:
+//   A   1 warp per row, 1024-slot hash, direct loads (4 rows per block);
+//   B1  4 warps, 2048-slot hash, TMA staging;
+//   B2  4 warps, 4096-slot hash, TMA staging;
+//   B3  16 warps, 8192-slot hash, TMA staging;
+//   C   8 warps, dense accumulator over all columns in global memory (the
+//       reference's own x[N]/ix[N]/jx[N] scheme; any width).
+// All tiers are persistent grids pulling rows from device-side lists, so a
 // multiply needs no host round trip until the traces are read back.
-#include "internal.h"
+#include "device_util.cuh"
+
+#include <cstring>
+
+using namespace b200;
 
 namespace {
-
-constexpr unsigned FULL = 0xffffffffu;
-
-template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
-template <> __device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
-template <> __device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
-template <typename T> __device__ __forceinline__ T add_rn(T a, T b);
-template <> __device__ __forceinline__ double add_rn<double>(double a, double b) { return __dadd_rn(a, b); }
-template <> __device__ __forceinline__ float add_rn<float>(float a, float b) { return __fadd_rn(a, b); }
-
-__device__ __forceinline__ unsigned lanemask_lt()
-{
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-// Barrier over the W warps of one team.  Team t uses named barrier t+1.
-template <int W> __device__ __forceinline__ void team_sync(int team)
-{
-    if (W == 1)
-        __syncwarp();
-    else
-        asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "r"(W * 32) : "memory");
-}
 
 // Flags shared by all tiers of one multiply call (device memory).
 struct MulFlags
@@ -61,7 +46,7 @@ struct MulFlags
     int overflow;     // some row needed more than Mc entries
     int max_width;    // largest pre-truncation output width
     int bad_input;    // an input column index or nnz out of range
-    int pad;
+    int timeout;      // a bounded wait on a bulk copy ran out
 };
 
 struct MulArgs
@@ -74,20 +59,32 @@ struct MulArgs
     double *dC;       // per-row C diagonal value (nullable)
     MulFlags *flags;
     int check_pre;    // A*B: also report rows whose pre-threshold width > Mc
+    const int *hint;  // previous distinct-column counts per row (nullable)
+    int *hint_out;    // distinct-column counts of this call
 };
 
-// Row lists and cursors for the three tiers.
+// Tiers: A (warp, 1024 slots), B1 (2048), B2 (4096), B3 (8192), C (dense).
+constexpr int NTIERS = 5;
+__constant__ int TIER_CAP[NTIERS] = {640, 1280, 2560, 5120, 0x7fffffff};
+
 struct TierLists
 {
-    int count[3];
-    int cursor[3];
+    int count[NTIERS];
+    int cursor[NTIERS];
+};
+
+struct TeamMisc
+{
+    double diag;
+    int row;
+    int pad;
 };
 
 // -------------------------------------------------------------------------
-// Planning: product-count bound per row, input validation, tier assignment.
+// Planning: product-count bound per row, input validation, tier choice.
 // One warp per row.
 // -------------------------------------------------------------------------
-__global__ void plan_kernel(MulArgs g, int capA, TierLists *tl, int *listA, int *listB)
+__global__ void plan_kernel(MulArgs g, int ncols, int skip_mid, TierLists *tl, int *lists)
 {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -119,18 +116,28 @@ __global__ void plan_kernel(MulArgs g, int capA, TierLists *tl, int *listA, int 
         if (lane == 0)
         {
             if (bad)
+            {
                 atomicExch(&g.flags->bad_input, 1);
-            else if (P <= capA)
-                listA[atomicAdd(&tl->count[0], 1)] = i;
-            else
-                listB[atomicAdd(&tl->count[1], 1)] = i;
+                continue;
+            }
+            long long est = P < ncols ? P : ncols;
+            if (g.hint)
+            {
+                const long long h = (long long) g.hint[i] + g.hint[i] / 4 + 16;
+                if (h < est)
+                    est = h;
+            }
+            int t = 0;
+            while (t < NTIERS - 1 && est > TIER_CAP[t])
+                ++t;
+            if (skip_mid && t > 0)
+                t = NTIERS - 1;
+            lists[(size_t) t * g.NA + atomicAdd(&tl->count[t], 1)] = i;
         }
     }
 }
 
-// Column indices of B inside the kernels are validated by the plan kernel
-// (which checks every index of A and the nnz of every referenced B row); B's
-// own column indices are checked here when they are used.
+// B's own column indices are checked where they are used (plan checks A's).
 __global__ void validate_cols_kernel(const int *Bi, const int *Bn, int ldb, int NB, int ncols,
                                      MulFlags *flags)
 {
@@ -150,25 +157,6 @@ __global__ void validate_cols_kernel(const int *Bi, const int *Bn, int ldb, int 
         if (__any_sync(FULL, bad) && lane == 0)
             atomicExch(&flags->bad_input, 1);
     }
-}
-
-// -------------------------------------------------------------------------
-// Shared-memory hash tiers (A and B).
-// Per-team shared memory: vals[TS] | keys[TS] | order[TS] | stage[W][smax] |
-//                         cnt[2][W] | misc
-// -------------------------------------------------------------------------
-template <typename T> struct TeamMisc
-{
-    T diag;
-    int row;
-    int pad;
-};
-
-template <typename T, int W, int LOGTS>
-__host__ __device__ constexpr size_t team_smem_bytes(int smax)
-{
-    return (size_t(1) << LOGTS) * (sizeof(T) + 2 * sizeof(int)) +
-           (W > 1 ? size_t(W) * smax * sizeof(int) : 0) + 2 * W * sizeof(int) + 32;
 }
 
 template <int LOGTS>
@@ -206,29 +194,51 @@ __device__ __forceinline__ int probe_insert(int *keys, int k, bool &inserted)
     return -1;
 }
 
-template <typename T, int W, int LOGTS>
-__global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArgs g, int smax,
-                                                       const int *rows, TierLists *tl, int tier,
-                                                       int *next_rows)
+// Common row epilogue: write the row's results and bookkeeping.
+template <typename T>
+__device__ __forceinline__ void finish_row(const MulArgs &g, int i, int ll, int distinct, T dA,
+                                           double diag)
 {
-    constexpr int TS = 1 << LOGTS;
-    constexpr int CAP = TS * 5 / 8;
-    extern __shared__ __align__(16) unsigned char smem[];
+    g.Cn[i] = min(ll, g.Mc);
+    atomicMax(&g.flags->max_width, ll);
+    if (ll > g.Mc || (g.check_pre && distinct > g.Mc))
+        atomicExch(&g.flags->overflow, 1);
+    if (g.dA)
+        g.dA[i] = (double) dA;
+    if (g.dC)
+        g.dC[i] = diag;
+    if (g.hint_out)
+        g.hint_out[i] = distinct;
+}
 
+// -------------------------------------------------------------------------
+// Tier A: one warp per row, 1024-slot table, direct (L1-cached) loads.
+// Shared memory per warp: vals[TS] | keys[TS] | order[TS] (ushort)
+// -------------------------------------------------------------------------
+constexpr int A_LOGTS = 10;
+constexpr int A_WARPS = 4;
+
+template <typename T> constexpr size_t tierA_warp_bytes()
+{
+    return (size_t(1) << A_LOGTS) * (sizeof(T) + sizeof(int) + sizeof(unsigned short));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * A_WARPS, 4) tierA_kernel(MulArgs g, const int *rows,
+                                                            TierLists *tl, int next_tier,
+                                                            int *next_rows)
+{
+    constexpr int TS = 1 << A_LOGTS;
+    extern __shared__ __align__(128) unsigned char smem[];
     if (g.flags->bad_input)
         return;
-    const int nrows = tl->count[tier];
-
+    const int CAP = TIER_CAP[0];
+    const int nrows = tl->count[0];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int team = warp / W, wt = warp % W, tid = wt * 32 + lane;
-    unsigned char *base = smem + (size_t) team * team_smem_bytes<T, W, LOGTS>(smax);
+    unsigned char *base = smem + (size_t) warp * tierA_warp_bytes<T>();
     T *vals = reinterpret_cast<T *>(base);
     int *keys = reinterpret_cast<int *>(vals + TS);
-    int *order = keys + TS;
-    int *stage = order + TS + (W > 1 ? wt * smax : 0);
-    int *cnt = order + TS + (W > 1 ? W * smax : 0);
-    TeamMisc<T> *misc = reinterpret_cast<TeamMisc<T> *>(cnt + 2 * W);
-
+    unsigned short *order = reinterpret_cast<unsigned short *>(keys + TS);
     const T *Av = static_cast<const T *>(g.Av);
     const T *Bv = static_cast<const T *>(g.Bv);
     T *Cv = static_cast<T *>(g.Cv);
@@ -236,40 +246,25 @@ __global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArg
 
     for (;;)
     {
-        int pos;
-        if (W == 1)
-        {
-            if (lane == 0)
-                pos = atomicAdd(&tl->cursor[tier], 1);
-            pos = __shfl_sync(FULL, pos, 0);
-        }
-        else
-        {
-            if (tid == 0)
-                misc->row = atomicAdd(&tl->cursor[tier], 1);
-            team_sync<W>(team);
-            pos = misc->row;
-        }
+        int pos = 0;
+        if (lane == 0)
+            pos = atomicAdd(&tl->cursor[0], 1);
+        pos = __shfl_sync(FULL, pos, 0);
         if (pos >= nrows)
             break;
         const int i = rows[pos];
-
-        for (int s = tid; s < TS; s += W * 32)
+        for (int s = lane; s < TS; s += 32)
         {
             keys[s] = B200_EMPTY_KEY;
             vals[s] = T(0);
         }
-        if (tid == 0)
-            misc->diag = T(0);
-        team_sync<W>(team);
-
+        __syncwarp();
         const int ni = g.An[i];
         const T *arow = Av + (size_t) i * g.lda;
         const int *airow = g.Ai + (size_t) i * g.lda;
         int distinct = 0;
         T dA = T(0);
         bool aborted = false;
-
         for (int jp0 = 0; jp0 < ni && !aborted; jp0 += 32)
         {
             const int q = jp0 + lane;
@@ -282,9 +277,8 @@ __global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArg
                 nj_l = g.Bn[aj];
             }
             const int cnt_here = min(32, ni - jp0);
-            for (int t = 0; t < cnt_here; ++t)
+            for (int t = 0; t < cnt_here && !aborted; ++t)
             {
-                const int jp = jp0 + t;
                 const T a = __shfl_sync(FULL, av, t);
                 const int j = __shfl_sync(FULL, aj, t);
                 const int nj = __shfl_sync(FULL, nj_l, t);
@@ -292,13 +286,278 @@ __global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArg
                     dA = add_rn(dA, a);
                 const T *brow = Bv + (size_t) j * g.ldb;
                 const int *birow = g.Bi + (size_t) j * g.ldb;
-                int k0 = 0, k1 = nj;
-                if (W > 1)
+                for (int kb = 0; kb < nj; kb += 32)
                 {
-                    const int S = b200_round_up(b200_ceil_div(nj, W), 32);
-                    k0 = min(wt * S, nj);
-                    k1 = min(k0 + S, nj);
+                    const int kp = kb + lane;
+                    bool ins = false;
+                    int slot = -1;
+                    if (kp < nj)
+                    {
+                        const int k = birow[kp];
+                        const T p = mul_rn(a, brow[kp]);
+                        slot = probe_insert<A_LOGTS>(keys, k, ins);
+                        if (slot >= 0)
+                            vals[slot] = add_rn(vals[slot], p);
+                    }
+                    const unsigned bal = __ballot_sync(FULL, ins);
+                    if (ins)
+                        order[distinct + __popc(bal & lanemask_lt())] = (unsigned short) slot;
+                    distinct += __popc(bal);
+                    if (__any_sync(FULL, kp < nj && slot < 0) || distinct > CAP)
+                    {
+                        aborted = true;
+                        break;
+                    }
                 }
+                __syncwarp();
+            }
+        }
+        if (aborted)
+        {
+            if (lane == 0)
+                next_rows[atomicAdd(&tl->count[next_tier], 1)] = i;
+            __syncwarp();
+            continue;
+        }
+        int ll = 0;
+        double diag = 0.0;
+        for (int c0 = 0; c0 < distinct; c0 += 32)
+        {
+            const int q = c0 + lane;
+            bool keep = false;
+            int k = 0;
+            T x = T(0);
+            if (q < distinct)
+            {
+                const int s = order[q];
+                k = keys[s];
+                x = vals[s];
+                keep = (k == i) || fabs(x) > thr;
+            }
+            const unsigned dbal = __ballot_sync(FULL, q < distinct && k == i);
+            if (dbal)
+                diag = (double) __shfl_sync(FULL, x, __ffs(dbal) - 1);
+            const unsigned bal = __ballot_sync(FULL, keep);
+            const int p = ll + __popc(bal & lanemask_lt());
+            if (keep && p < g.Mc)
+            {
+                Cv[(size_t) i * g.ldc + p] = x;
+                g.Ci[(size_t) i * g.ldc + p] = k;
+            }
+            ll += __popc(bal);
+        }
+        if (lane == 0)
+            finish_row<T>(g, i, ll, distinct, dA, diag);
+        __syncwarp();
+    }
+}
+
+// -------------------------------------------------------------------------
+// Tiers B1-B3: a team of W warps per row (one team per block), rows of B
+// staged by TMA bulk copies in units of at most CHUNK entries.
+// Shared memory: mbar[STAGES] | sv[STAGES][CHUNK] | sk[STAGES][CHUNK] |
+//                vals[TS] | keys[TS] | order[TS] (ushort) |
+//                stg[W][SPW] (ushort) | cnt[2][W] | misc
+// -------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return (unsigned) __cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `parity` of `bar`, giving up after ~2 s (a bulk copy that
+// never lands); on timeout the caller's flag is raised and false returned.
+__device__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *timeout_flag)
+{
+    if (mbar_try_wait(bar, parity))
+        return true;
+    const unsigned long long t0 = global_ns();
+    for (;;)
+    {
+        if (mbar_try_wait(bar, parity))
+            return true;
+        if (global_ns() - t0 > 2000000000ull)
+        {
+            atomicExch(timeout_flag, 1);
+            return false;
+        }
+    }
+}
+
+template <typename T, int W, int LOGTS, int STAGES, int CHUNK> struct TeamCfg
+{
+    static constexpr int TS = 1 << LOGTS;
+    static constexpr int NT = W * 32;
+    static constexpr int SPW = ((CHUNK + W - 1) / W + 31) / 32 * 32; // staging per warp
+    static constexpr size_t off_sv = 128;
+    static constexpr size_t off_sk = off_sv + size_t(STAGES) * CHUNK * sizeof(T);
+    static constexpr size_t off_vals = off_sk + size_t(STAGES) * CHUNK * sizeof(int);
+    static constexpr size_t off_keys = off_vals + size_t(TS) * sizeof(T);
+    static constexpr size_t off_order = off_keys + size_t(TS) * sizeof(int);
+    static constexpr size_t off_stg = off_order + size_t(TS) * sizeof(unsigned short);
+    static constexpr size_t off_cnt =
+        (off_stg + size_t(W) * SPW * sizeof(unsigned short) + 15) / 16 * 16;
+    static constexpr size_t off_misc = off_cnt + 2 * W * sizeof(int);
+    static constexpr size_t bytes = off_misc + sizeof(TeamMisc) + 16;
+};
+
+template <typename T, int W, int LOGTS, int STAGES, int CHUNK, int MINB>
+__global__ void __launch_bounds__(W * 32, MINB) team_kernel(MulArgs g, const int *rows, TierLists *tl,
+                                                           int tier, int *next_rows)
+{
+    using Cfg = TeamCfg<T, W, LOGTS, STAGES, CHUNK>;
+    constexpr int TS = Cfg::TS, NT = Cfg::NT, SPW = Cfg::SPW;
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (g.flags->bad_input)
+        return;
+    const int CAP = TIER_CAP[tier];
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);
+    T *sv = reinterpret_cast<T *>(smem + Cfg::off_sv);
+    int *sk = reinterpret_cast<int *>(smem + Cfg::off_sk);
+    T *vals = reinterpret_cast<T *>(smem + Cfg::off_vals);
+    int *keys = reinterpret_cast<int *>(smem + Cfg::off_keys);
+    unsigned short *order = reinterpret_cast<unsigned short *>(smem + Cfg::off_order);
+    int *cnt = reinterpret_cast<int *>(smem + Cfg::off_cnt);
+    TeamMisc *misc = reinterpret_cast<TeamMisc *>(smem + Cfg::off_misc);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned short *stg = reinterpret_cast<unsigned short *>(smem + Cfg::off_stg) + warp * SPW;
+
+    const int nrows = tl->count[tier];
+    const T *Av = static_cast<const T *>(g.Av);
+    const T *Bv = static_cast<const T *>(g.Bv);
+    T *Cv = static_cast<T *>(g.Cv);
+    const T thr = (T) g.thr;
+    int *tflag = &g.flags->timeout;
+
+    if (tid == 0)
+    {
+        for (int s = 0; s < STAGES; ++s)
+            mbar_init(&mbar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    unsigned ucount = 0; // units consumed by this block (uniform)
+    for (;;)
+    {
+        if (tid == 0)
+            misc->row = atomicAdd(&tl->cursor[tier], 1);
+        __syncthreads();
+        const int pos = misc->row;
+        if (pos >= nrows || *reinterpret_cast<volatile int *>(tflag))
+            break;
+        const int i = rows[pos];
+        for (int s = tid; s < TS; s += NT)
+        {
+            keys[s] = B200_EMPTY_KEY;
+            vals[s] = T(0);
+        }
+        if (tid == 0)
+            misc->diag = 0.0;
+        __syncthreads();
+
+        const int ni = g.An[i];
+        const T *arow = Av + (size_t) i * g.lda;
+        const int *airow = g.Ai + (size_t) i * g.lda;
+
+        // Producer position (tracked by every thread, issued by thread 0):
+        // the next unit to copy is chunk pc of the B row named at position pj.
+        int pj = 0, pc = 0, pnj = 0;
+        auto prod_skip = [&]() {
+            while (pj < ni)
+            {
+                pnj = g.Bn[airow[pj]];
+                if (pc * CHUNK < pnj)
+                    return;
+                ++pj;
+                pc = 0;
+            }
+        };
+        auto issue = [&](unsigned slot_u) {
+            const int s = slot_u % STAGES;
+            const int j = airow[pj];
+            const int off = pc * CHUNK;
+            const int n = min(CHUNK, pnj - off);
+            const unsigned bv = (unsigned) ((n * sizeof(T) + 15) & ~size_t(15));
+            const unsigned bk = (unsigned) ((n * sizeof(int) + 15) & ~size_t(15));
+            if (tid == 0)
+            {
+                mbar_expect_tx(&mbar[s], bv + bk);
+                bulk_g2s(sv + (size_t) s * CHUNK, Bv + (size_t) j * g.ldb + off, bv, &mbar[s]);
+                bulk_g2s(sk + (size_t) s * CHUNK, g.Bi + (size_t) j * g.ldb + off, bk, &mbar[s]);
+            }
+            ++pc;
+        };
+        prod_skip();
+        unsigned issued = 0;
+        while (issued < STAGES && pj < ni)
+        {
+            issue(ucount + issued);
+            ++issued;
+            prod_skip();
+        }
+
+        int distinct = 0;
+        T dA = T(0);
+        bool aborted = false;
+        unsigned consumed = 0;
+        for (int jp = 0; jp < ni && !aborted; ++jp)
+        {
+            const T a = arow[jp];
+            const int j = airow[jp];
+            const int nj = g.Bn[j];
+            if (j == i)
+                dA = add_rn(dA, a);
+            for (int off = 0; off < nj; off += CHUNK)
+            {
+                const unsigned u = ucount + consumed;
+                const int s = u % STAGES;
+                const int n = min(CHUNK, nj - off);
+                mbar_wait_bounded(&mbar[s], (u / STAGES) & 1, tflag);
+                const T *uv = sv + (size_t) s * CHUNK;
+                const int *uk = sk + (size_t) s * CHUNK;
+                const int S = b200_round_up(b200_ceil_div(n, W), 32);
+                const int k0 = min(warp * S, n), k1 = min(k0 + S, n);
                 int local = 0;
                 bool fail = false;
                 for (int kb = k0; kb < k1; kb += 32)
@@ -308,8 +567,8 @@ __global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArg
                     int slot = -1;
                     if (kp < k1)
                     {
-                        const int k = birow[kp];
-                        const T p = mul_rn(a, brow[kp]);
+                        const int k = uk[kp];
+                        const T p = mul_rn(a, uv[kp]);
                         slot = probe_insert<LOGTS>(keys, k, ins);
                         if (slot >= 0)
                             vals[slot] = add_rn(vals[slot], p);
@@ -317,79 +576,65 @@ __global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArg
                             fail = true;
                     }
                     const unsigned bal = __ballot_sync(FULL, ins);
-                    if (W == 1)
-                    {
-                        if (ins)
-                            order[distinct + local + __popc(bal & lanemask_lt())] = slot;
-                    }
-                    else if (ins)
-                    {
-                        stage[local + __popc(bal & lanemask_lt())] = slot;
-                    }
+                    if (ins)
+                        stg[local + __popc(bal & lanemask_lt())] = (unsigned short) slot;
                     local += __popc(bal);
-                    fail = __any_sync(FULL, fail);
-                    if (fail || (W == 1 && distinct + local > CAP))
-                    {
-                        fail = true;
-                        break;
-                    }
                 }
-                if (W == 1)
-                {
-                    __syncwarp();
-                    distinct += local;
-                    if (fail)
-                        aborted = true;
-                }
-                else
-                {
-                    // A failed probe is signalled as a negative count, so that
-                    // every warp of the team reads the same decision after the
-                    // barrier (the counts are double-buffered by jp parity).
-                    if (lane == 0)
-                        cnt[(jp & 1) * W + wt] = fail ? -1 : local;
-                    team_sync<W>(team);
-                    int pre = 0, tot = 0;
-                    bool any_fail = false;
+                fail = __any_sync(FULL, fail);
+                if (lane == 0)
+                    cnt[(u & 1) * W + warp] = fail ? -1 : local;
+                __syncthreads();
+                ++consumed;
+                int pre = 0, tot = 0;
+                bool any_fail = false;
 #pragma unroll
-                    for (int w = 0; w < W; ++w)
-                    {
-                        const int c = cnt[(jp & 1) * W + w];
-                        any_fail |= c < 0;
-                        pre += (w < wt) ? c : 0;
-                        tot += c;
-                    }
-                    if (!any_fail && distinct + tot <= TS)
-                        for (int s = lane; s < local; s += 32)
-                            order[distinct + pre + s] = stage[s];
-                    __syncwarp();
-                    distinct += tot;
-                    if (any_fail || distinct > CAP)
-                        aborted = true;
+                for (int w = 0; w < W; ++w)
+                {
+                    const int cw = cnt[(u & 1) * W + w];
+                    any_fail |= cw < 0;
+                    pre += (w < warp) ? cw : 0;
+                    tot += cw;
                 }
-                if (aborted)
+                if (!any_fail && distinct + tot <= TS)
+                    for (int q = lane; q < local; q += 32)
+                        order[distinct + pre + q] = stg[q];
+                __syncwarp();
+                distinct += tot;
+                if (any_fail || distinct > CAP)
+                {
+                    aborted = true;
                     break;
+                }
+                // the stage just consumed is free: refill it
+                if (pj < ni)
+                {
+                    issue(ucount + issued);
+                    ++issued;
+                    prod_skip();
+                }
             }
         }
-
+        // Drain copies still in flight for this row (only after an abort).
+        while (consumed < issued)
+        {
+            const unsigned u = ucount + consumed;
+            mbar_wait_bounded(&mbar[u % STAGES], (u / STAGES) & 1, tflag);
+            ++consumed;
+        }
+        ucount += consumed;
+        __syncthreads();
         if (aborted)
         {
             if (tid == 0)
                 next_rows[atomicAdd(&tl->count[tier + 1], 1)] = i;
-            team_sync<W>(team);
             continue;
         }
 
         // Compaction in first-touch order: keep k == i or |x| > threshold.
-        // The barrier separates the last jp's reads of cnt from the rounds'.
-        team_sync<W>(team);
-        if (g.check_pre && distinct > g.Mc && tid == 0)
-            atomicExch(&g.flags->overflow, 1);
-        int ll = 0;
-        int round = 0;
-        for (int c0 = 0; c0 < distinct; c0 += W * 32, ++round)
+        int ll = 0, round = 0;
+        for (int c0 = 0; c0 < distinct; c0 += NT, ++round)
         {
-            const int q = c0 + wt * 32 + lane;
+            const int q = c0 + warp * 32 + lane;
             bool keep = false;
             int k = 0;
             T x = T(0);
@@ -401,26 +646,22 @@ __global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArg
                 if (k == i)
                 {
                     keep = true;
-                    misc->diag = x;
+                    misc->diag = (double) x;
                 }
                 else
                     keep = fabs(x) > thr;
             }
             const unsigned bal = __ballot_sync(FULL, keep);
-            int pre = 0, tot = __popc(bal);
-            if (W > 1)
-            {
-                if (lane == 0)
-                    cnt[(round & 1) * W + wt] = tot;
-                team_sync<W>(team);
-                tot = 0;
+            if (lane == 0)
+                cnt[(round & 1) * W + warp] = __popc(bal);
+            __syncthreads();
+            int pre = 0, tot = 0;
 #pragma unroll
-                for (int w = 0; w < W; ++w)
-                {
-                    const int c = cnt[(round & 1) * W + w];
-                    pre += (w < wt) ? c : 0;
-                    tot += c;
-                }
+            for (int w = 0; w < W; ++w)
+            {
+                const int cw = cnt[(round & 1) * W + w];
+                pre += (w < warp) ? cw : 0;
+                tot += cw;
             }
             const int p = ll + pre + __popc(bal & lanemask_lt());
             if (keep && p < g.Mc)
@@ -430,43 +671,35 @@ __global__ void __launch_bounds__(W == 1 ? 128 : W * 32) hash_tier_kernel(MulArg
             }
             ll += tot;
         }
-        team_sync<W>(team);
+        __syncthreads();
         if (tid == 0)
-        {
-            g.Cn[i] = min(ll, g.Mc);
-            atomicMax(&g.flags->max_width, ll);
-            if (ll > g.Mc)
-                atomicExch(&g.flags->overflow, 1);
-            if (g.dA)
-                g.dA[i] = (double) dA;
-            if (g.dC)
-                g.dC[i] = (double) misc->diag;
-        }
-        team_sync<W>(team);
+            finish_row<T>(g, i, ll, distinct, dA, misc->diag);
     }
 }
 
 // -------------------------------------------------------------------------
 // Tier C: dense accumulator over all columns, in global memory, one slab per
-// CTA: acc[ncols] (T), mark[ncols] (int, row+1 while the column is live),
+// block: acc[ncols] (T), mark[ncols] (int, row+1 while the column is live),
 // order[ncols] (int, column ids in first-touch order).  Marks are cleared
 // column by column at the end of each row, as the reference clears ix[].
 // -------------------------------------------------------------------------
+constexpr int C_W = 8;
+
 template <typename T>
-__global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, int ncols,
+__global__ void __launch_bounds__(256, 4) dense_tier_kernel(MulArgs g, int smax, int ncols,
                                                         const int *rows, TierLists *tl,
                                                         unsigned char *slabs)
 {
-    constexpr int W = 8;
-    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int W = C_W;
+    extern __shared__ __align__(128) unsigned char smem[];
     if (g.flags->bad_input)
         return;
-    const int nrows = tl->count[2];
+    const int nrows = tl->count[NTIERS - 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wt = warp;
     const int tid = threadIdx.x;
     int *stage = reinterpret_cast<int *>(smem) + wt * smax;
     int *cnt = reinterpret_cast<int *>(smem) + W * smax;
-    TeamMisc<T> *misc = reinterpret_cast<TeamMisc<T> *>(cnt + 2 * W);
+    TeamMisc *misc = reinterpret_cast<TeamMisc *>(cnt + 2 * W);
 
     const size_t slab_bytes = (size_t) ncols * (sizeof(T) + 2 * sizeof(int));
     unsigned char *slab = slabs + (size_t) blockIdx.x * slab_bytes;
@@ -483,7 +716,7 @@ __global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, in
     for (;;)
     {
         if (tid == 0)
-            misc->row = atomicAdd(&tl->cursor[2], 1);
+            misc->row = atomicAdd(&tl->cursor[NTIERS - 1], 1);
         __syncthreads();
         const int pos = misc->row;
         if (pos >= nrows)
@@ -491,19 +724,20 @@ __global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, in
         const int i = rows[pos];
         if (!marks_clear)
         {
-            // The slab is shared scratch: clear this CTA's marks once.
+            // The slab is shared scratch: clear this block's marks once.
             for (int s = tid; s < ncols; s += 256)
-                __stcg(&mark[s], 0);
+                mark[s] = 0;
             __syncthreads();
             marks_clear = true;
         }
         if (tid == 0)
-            misc->diag = T(0);
+            misc->diag = 0.0;
         const int ni = g.An[i];
         const T *arow = Av + (size_t) i * g.lda;
         const int *airow = g.Ai + (size_t) i * g.lda;
         int distinct = 0;
         T dA = T(0);
+        int step = 0;
         for (int jp0 = 0; jp0 < ni; jp0 += 32)
         {
             const int q = jp0 + lane;
@@ -516,9 +750,8 @@ __global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, in
                 nj_l = g.Bn[aj];
             }
             const int cnt_here = min(32, ni - jp0);
-            for (int t = 0; t < cnt_here; ++t)
+            for (int t = 0; t < cnt_here; ++t, ++step)
             {
-                const int jp = jp0 + t;
                 const T a = __shfl_sync(FULL, av, t);
                 const int j = __shfl_sync(FULL, aj, t);
                 const int nj = __shfl_sync(FULL, nj_l, t);
@@ -538,14 +771,14 @@ __global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, in
                     {
                         k = birow[kp];
                         const T p = mul_rn(a, brow[kp]);
-                        if (__ldcg(&mark[k]) != i + 1)
+                        if (mark[k] != i + 1)
                         {
-                            __stcg(&mark[k], i + 1);
-                            __stcg(&acc[k], add_rn(T(0), p));
+                            mark[k] = i + 1;
+                            acc[k] = add_rn(T(0), p);
                             ins = true;
                         }
                         else
-                            __stcg(&acc[k], add_rn(__ldcg(&acc[k]), p));
+                            acc[k] = add_rn(acc[k], p);
                     }
                     const unsigned bal = __ballot_sync(FULL, ins);
                     if (ins)
@@ -553,25 +786,23 @@ __global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, in
                     local += __popc(bal);
                 }
                 if (lane == 0)
-                    cnt[(jp & 1) * W + wt] = local;
+                    cnt[(step & 1) * W + wt] = local;
                 __syncthreads();
                 int pre = 0, tot = 0;
 #pragma unroll
                 for (int w = 0; w < W; ++w)
                 {
-                    const int c = cnt[(jp & 1) * W + w];
+                    const int c = cnt[(step & 1) * W + w];
                     pre += (w < wt) ? c : 0;
                     tot += c;
                 }
                 for (int s = lane; s < local; s += 32)
-                    __stcg(&order[distinct + pre + s], stage[s]);
+                    order[distinct + pre + s] = stage[s];
                 __syncwarp();
                 distinct += tot;
             }
         }
         __syncthreads();
-        if (g.check_pre && distinct > g.Mc && tid == 0)
-            atomicExch(&g.flags->overflow, 1);
         int ll = 0, round = 0;
         for (int c0 = 0; c0 < distinct; c0 += W * 32, ++round)
         {
@@ -581,13 +812,13 @@ __global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, in
             T x = T(0);
             if (q < distinct)
             {
-                k = __ldcg(&order[q]);
-                x = __ldcg(&acc[k]);
-                __stcg(&mark[k], 0);
+                k = order[q];
+                x = acc[k];
+                mark[k] = 0;
                 if (k == i)
                 {
                     keep = true;
-                    misc->diag = x;
+                    misc->diag = (double) x;
                 }
                 else
                     keep = fabs(x) > thr;
@@ -614,58 +845,40 @@ __global__ void __launch_bounds__(256) dense_tier_kernel(MulArgs g, int smax, in
         }
         __syncthreads();
         if (tid == 0)
-        {
-            g.Cn[i] = min(ll, g.Mc);
-            atomicMax(&g.flags->max_width, ll);
-            if (ll > g.Mc)
-                atomicExch(&g.flags->overflow, 1);
-            if (g.dA)
-                g.dA[i] = (double) dA;
-            if (g.dC)
-                g.dC[i] = (double) misc->diag;
-        }
+            finish_row<T>(g, i, ll, distinct, dA, misc->diag);
         __syncthreads();
     }
 }
 
-// Sum of per-row diagonal values (two arrays) in FP64, fixed order: each
-// thread sums a contiguous stripe, then a tree over threads.  One block.
-__global__ void __launch_bounds__(1024) trace_pair_kernel(const double *a, const double *b, int n,
-                                                         double *out)
+// Team tier configurations: (W, LOGTS, STAGES, CHUNK, min blocks per SM)
+#define B1_CFG 4, 11, 3, 256, 4
+#define B2_CFG 4, 12, 3, 256, 3
+#define B3_CFG 16, 13, 3, 512, 1
+
+template <typename T, int W, int LOGTS, int STAGES, int CHUNK, int MINB>
+bool launch_team(B200Context *c, const MulArgs &g, const int *rows, TierLists *tl, int tier,
+                 int *next_rows)
 {
-    __shared__ double sa[1024], sb[1024];
-    const int t = threadIdx.x;
-    const int per = b200_ceil_div(n, 1024);
-    double xa = 0.0, xb = 0.0;
-    for (int r = t * per; r < min(n, (t + 1) * per); ++r)
-    {
-        if (a)
-            xa += a[r];
-        if (b)
-            xb += b[r];
-    }
-    sa[t] = xa;
-    sb[t] = xb;
-    __syncthreads();
-    for (int s = 512; s; s >>= 1)
-    {
-        if (t < s)
-        {
-            sa[t] += sa[t + s];
-            sb[t] += sb[t + s];
-        }
-        __syncthreads();
-    }
-    if (t == 0)
-    {
-        out[0] = sa[0];
-        out[1] = sb[0];
-    }
+    using Cfg = TeamCfg<T, W, LOGTS, STAGES, CHUNK>;
+    auto k = team_kernel<T, W, LOGTS, STAGES, CHUNK, MINB>;
+    if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg::bytes)))
+        return false;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, W * 32, Cfg::bytes);
+    const int grid = c->sm_count * (occ > 0 ? occ : 1);
+    k<<<grid, W * 32, Cfg::bytes, c->stream>>>(g, rows, tl, tier, next_rows);
+    return LAUNCH_OK("team_kernel");
 }
 
-constexpr int TIER_A_LOGTS = 10; // 1024 slots, capacity 640
-constexpr int TIER_B_LOGTS = 13; // 8192 slots, capacity 5120
-constexpr int TIER_A_TEAMS = 4;  // one-warp teams per 128-thread block
+constexpr int C_BLOCKS_PER_SM = 4;
+
+// Distinct-column counts of the last multiply, reused as the next call's
+// tier estimate when the row count matches (SP2 multiplies the same-size
+// matrix over and over; a stale estimate only costs a retry in a larger tier).
+int *g_hint = nullptr;
+int g_hint_n = 0;
+bool g_hint_valid = false;
+int g_last_tiers[NTIERS] = {0};
 
 template <typename T>
 bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
@@ -674,32 +887,39 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     if (!c)
         return false;
     const int N = g.NA;
-    const int smaxB = b200_round_up(b200_ceil_div(g.ldb, 8), 32);
-    const size_t smemA = team_smem_bytes<T, 1, TIER_A_LOGTS>(0) * TIER_A_TEAMS;
-    const size_t smemB = team_smem_bytes<T, 8, TIER_B_LOGTS>(smaxB);
-    const size_t smemC = (size_t) 8 * smaxB * sizeof(int) + 2 * 8 * sizeof(int) + 32;
-    const bool tierB_ok = smemB <= c->smem_optin;
+    const int smaxC = b200_round_up(b200_ceil_div(g.ldb, C_W), 32);
+    const size_t smemA = tierA_warp_bytes<T>() * A_WARPS;
+    const size_t smemC = (size_t) C_W * smaxC * sizeof(int) + 2 * C_W * sizeof(int) + 32;
     if (smemC > c->smem_optin)
     {
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "row width %d too large for the multiply kernels", g.ldb);
         return false;
     }
-    const int gridC = c->sm_count;
+    const int gridC = c->sm_count * C_BLOCKS_PER_SM;
     const size_t slab_bytes = (size_t) ncols * (sizeof(T) + 2 * sizeof(int));
 
-    // scratch: lists A/B/C (N ints each), diag arrays (2N doubles), slabs
-    size_t off_lists = 0;
-    size_t off_diag = (size_t) 3 * N * sizeof(int);
-    off_diag = (off_diag + 255) & ~size_t(255);
-    size_t off_slabs = off_diag + (size_t) 2 * N * sizeof(double);
-    off_slabs = (off_slabs + 255) & ~size_t(255);
+    if (g_hint_n != N)
+    {
+        if (g_hint)
+            cudaFree(g_hint);
+        g_hint = nullptr;
+        g_hint_valid = false;
+        g_hint_n = 0;
+        if (!CUDA_OK(cudaMalloc(&g_hint, (size_t) N * sizeof(int))))
+            return false;
+        g_hint_n = N;
+    }
+    g.hint = g_hint_valid ? g_hint : nullptr;
+    g.hint_out = g_hint;
+
+    // scratch: NTIERS lists of N ints, diag arrays (2N doubles), dense slabs
+    size_t off_diag = ((size_t) NTIERS * N * sizeof(int) + 255) & ~size_t(255);
+    size_t off_slabs = (off_diag + (size_t) 2 * N * sizeof(double) + 255) & ~size_t(255);
     size_t total = off_slabs + (size_t) gridC * slab_bytes;
     unsigned char *scr = static_cast<unsigned char *>(b200_scratch(total));
     if (!scr)
         return false;
-    int *listA = reinterpret_cast<int *>(scr + off_lists);
-    int *listB = listA + N;
-    int *listC = listB + N;
+    int *lists = reinterpret_cast<int *>(scr);
     double *diagA = reinterpret_cast<double *>(scr + off_diag);
     double *diagC = diagA + N;
     unsigned char *slabs = scr + off_slabs;
@@ -725,64 +945,43 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
         g.dC = nullptr;
     }
 
-    const int plan_blocks = min(b200_ceil_div(N, 8), c->sm_count * 16);
-    validate_cols_kernel<<<min(b200_ceil_div(g.NB, 8), c->sm_count * 16), 256, 0, c->stream>>>(
-        g.Bi, g.Bn, g.ldb, g.NB, ncols, flags);
-    // When tier B cannot hold its staging area (very wide rows), the rows past
-    // tier A go straight to the dense tier: they are listed in listC under
-    // count[1], and count[1] is copied to count[2] after tier A.
-    int *listBC = tierB_ok ? listB : listC;
-    plan_kernel<<<max(plan_blocks, 1), 256, 0, c->stream>>>(g, 640, tl, listA, listBC);
+    const int vgrid = max(1, min(b200_ceil_div(g.NB, 8), c->sm_count * 16));
+    validate_cols_kernel<<<vgrid, 256, 0, c->stream>>>(g.Bi, g.Bn, g.ldb, g.NB, ncols, flags);
+    if (!LAUNCH_OK("validate_cols_kernel"))
+        return false;
+    const int pgrid = max(1, min(b200_ceil_div(N, 8), c->sm_count * 16));
+    // The team tiers keep order positions in 16 bits: tables of at most 8192.
+    plan_kernel<<<pgrid, 256, 0, c->stream>>>(g, ncols, 0, tl, lists);
     if (!LAUNCH_OK("plan_kernel"))
         return false;
 
-    if (!CUDA_OK(cudaFuncSetAttribute(hash_tier_kernel<T, 1, TIER_A_LOGTS>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemA)))
+    auto list = [&](int t) { return lists + (size_t) t * N; };
+    if (!CUDA_OK(cudaFuncSetAttribute(tierA_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) smemA)))
         return false;
     int occA = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occA, hash_tier_kernel<T, 1, TIER_A_LOGTS>,
-                                                  32 * TIER_A_TEAMS, smemA);
-    const int gridA = c->sm_count * max(occA, 1);
-    hash_tier_kernel<T, 1, TIER_A_LOGTS><<<gridA, 32 * TIER_A_TEAMS, smemA, c->stream>>>(
-        g, 0, listA, tl, 0, listBC);
-    if (!LAUNCH_OK("hash_tier_kernel<A>"))
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occA, tierA_kernel<T>, 32 * A_WARPS, smemA);
+    tierA_kernel<T><<<c->sm_count * max(occA, 1), 32 * A_WARPS, smemA, c->stream>>>(
+        g, list(0), tl, 1, list(1));
+    if (!LAUNCH_OK("tierA_kernel"))
         return false;
-
-    if (tierB_ok)
-    {
-        if (!CUDA_OK(cudaFuncSetAttribute(hash_tier_kernel<T, 8, TIER_B_LOGTS>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemB)))
-            return false;
-        int occB = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occB, hash_tier_kernel<T, 8, TIER_B_LOGTS>,
-                                                      256, smemB);
-        const int gridB = c->sm_count * max(occB, 1);
-        hash_tier_kernel<T, 8, TIER_B_LOGTS><<<gridB, 256, smemB, c->stream>>>(g, smaxB, listB, tl,
-                                                                               1, listC);
-        if (!LAUNCH_OK("hash_tier_kernel<B>"))
-            return false;
-    }
-    else
-    {
-        if (!CUDA_OK(cudaMemcpyAsync(&tl->count[2], &tl->count[1], sizeof(int),
-                                     cudaMemcpyDeviceToDevice, c->stream)))
-            return false;
-    }
-
+    if (!launch_team<T, B1_CFG>(c, g, list(1), tl, 1, list(2)) ||
+        !launch_team<T, B2_CFG>(c, g, list(2), tl, 2, list(3)) ||
+        !launch_team<T, B3_CFG>(c, g, list(3), tl, 3, list(4)))
+        return false;
     if (!CUDA_OK(cudaFuncSetAttribute(dense_tier_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
         return false;
-    dense_tier_kernel<T><<<gridC, 256, smemC, c->stream>>>(g, smaxB, ncols, listC, tl, slabs);
+    dense_tier_kernel<T><<<gridC, 256, smemC, c->stream>>>(g, smaxC, ncols, list(NTIERS - 1), tl, slabs);
     if (!LAUNCH_OK("dense_tier_kernel"))
         return false;
 
     if (trace)
     {
-        trace_pair_kernel<<<1, 1024, 0, c->stream>>>(diagA, diagC, N, dtrace);
-        if (!LAUNCH_OK("trace_pair_kernel"))
+        b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(diagA, diagC, N, dtrace);
+        if (!LAUNCH_OK("b200_sum_rows_kernel"))
             return false;
     }
-    // bring back flags (+ traces)
     unsigned char *pin = static_cast<unsigned char *>(c->pinned);
     if (!CUDA_OK(cudaMemcpyAsync(pin, small, 256, cudaMemcpyDeviceToHost, c->stream)))
         return false;
@@ -790,14 +989,23 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
         return false;
     const MulFlags *hf = reinterpret_cast<const MulFlags *>(pin + 64);
     const double *ht = reinterpret_cast<const double *>(pin + 128);
+    memcpy(g_last_tiers, reinterpret_cast<const TierLists *>(pin)->count, sizeof(g_last_tiers));
     if (required_M)
         *required_M = hf->max_width;
     if (hf->bad_input)
     {
+        g_hint_valid = false;
         b200_set_error(BML_B200_ERR_INVALID,
                        "multiply: a column index or row length of an input is out of range");
         return false;
     }
+    if (hf->timeout)
+    {
+        g_hint_valid = false;
+        b200_set_error(BML_B200_ERR_TIMEOUT, "multiply: a shared-memory bulk copy did not complete");
+        return false;
+    }
+    g_hint_valid = true;
     if (trace)
     {
         trace[0] = ht[0];
@@ -840,11 +1048,14 @@ bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matri
     }
     if (!ell_to_device(A) || (B != A && !ell_to_device(B)) || !ell_to_device(C))
         return false;
+    if (C->mirror == MIRROR_HOST_NEWER)
+        C->mirror = MIRROR_SYNCED;
     MulArgs g{};
     g.Av = A->d_value; g.Ai = A->d_index; g.An = A->d_nnz; g.lda = A->ld; g.NA = A->N;
     g.Bv = B->d_value; g.Bi = B->d_index; g.Bn = B->d_nnz; g.ldb = B->ld; g.NB = B->N;
     g.Cv = C->d_value; g.Ci = C->d_index; g.Cn = C->d_nnz; g.ldc = C->ld; g.Mc = C->M;
     g.thr = threshold;
+    g.check_pre = (A != B) ? 1 : 0;
     // Column indices of B address columns of the product: at most max(B->N, C->N).
     const int ncols = B->N > C->N ? B->N : C->N;
     bool ok = A->matrix_precision == double_real
@@ -853,4 +1064,13 @@ bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matri
     // C's device arrays now hold the product (also on ROW_OVERFLOW, truncated).
     ell_mark_device(C);
     return ok;
+}
+
+// Rows handled by each multiply tier in the last call on this process
+// (A, O1, O2, O3, C; a row handed on is counted in every tier it entered).
+extern "C" BML_B200_API int bml_b200_last_tier_counts(int *counts, int n)
+{
+    for (int t = 0; t < n && t < NTIERS; ++t)
+        counts[t] = g_last_tiers[t];
+    return NTIERS;
 }

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(W * 32) add_kernel(T *Av, int *Ai, int *An, in
                                                    int ldb, int N, double alpha, double beta,
                                                    double thr, int logts, int *overflow)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int TS = 1 << logts;
     const unsigned mask = TS - 1;
     T *xa = reinterpret_cast<T *>(smem);
@@ -397,7 +397,7 @@ __global__ void trace_mult_kernel(const T *Av, const int *Ai, const int *An, int
                                   const T *Bv, const int *Bi, const int *Bn, int ldb, int N,
                                   int logts, double *part)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int TS = 1 << logts;
     const unsigned mask = TS - 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -410,9 +410,6 @@ __global__ void trace_mult_kernel(const T *Av, const int *Ai, const int *An, int
             keys[s] = B200_EMPTY_KEY;
         __syncwarp();
         const int nb = Bn[i];
-        // the first occurrence of a column in B's row wins, as in the reference
-        for (int p = nb - 1 - lane; p >= 0; p -= 32)
-            ;
         for (int c0 = 0; c0 < nb; c0 += 32)
         {
             const int p = c0 + lane;
@@ -422,7 +419,6 @@ __global__ void trace_mult_kernel(const T *Av, const int *Ai, const int *An, int
         }
         __syncwarp();
         double s = 0.0;
-        T acc = T(0);
         const int na = An[i];
         for (int p = lane; p < na; p += 32)
         {
@@ -430,7 +426,6 @@ __global__ void trace_mult_kernel(const T *Av, const int *Ai, const int *An, int
             if (q >= 0)
                 s += (double) mul_rn(Av[(size_t) i * lda + p], Bv[(size_t) i * ldb + q]);
         }
-        (void) acc;
         for (int o = 16; o; o >>= 1)
             s += __shfl_xor_sync(FULL, s, o);
         if (lane == 0)
@@ -519,7 +514,7 @@ __global__ void transpose_scatter_kernel(const T *Av, const int *Ai, const int *
 template <typename T>
 __global__ void row_sort_kernel(T *Bv, int *Bi, int *Bn, int ldb, int Mb, int N, int pow2)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     T *sv = reinterpret_cast<T *>(smem);
     int *sk = reinterpret_cast<int *>(sv + pow2);
     for (int j = blockIdx.x; j < N; j += gridDim.x)
@@ -832,6 +827,7 @@ bool ell_trace(bml_matrix_ellpack_t *A, double *trace)
         diag_kernel<float><<<grid, 256, 0, c->stream>>>(static_cast<const float *>(A->d_value),
                                                         A->d_index, A->d_nnz, A->ld, A->N, d);
     double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
+    b200_count_launch(); // diag_kernel
     b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(d, nullptr, A->N, out);
     if (!LAUNCH_OK("trace kernels"))
         return false;
@@ -888,6 +884,7 @@ bool ell_trace_mult(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *tr
             static_cast<const float *>(B->d_value), B->d_index, B->d_nnz, B->ld, A->N, logts, part);
     }
     double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
+    b200_count_launch(); // trace_mult_kernel
     b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(part, nullptr, A->N, out);
     if (!LAUNCH_OK("trace_mult kernels"))
         return false;
@@ -950,6 +947,7 @@ bool ell_transpose_new(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B)
         k<<<sgrid, 256, smem, c->stream>>>(static_cast<float *>(B->d_value), B->d_index, B->d_nnz,
                                            B->ld, B->M, B->N, pow2);
     }
+    b200_count_launch(); // transpose_scatter_kernel
     if (!LAUNCH_OK("transpose kernels"))
         return false;
     ell_mark_device(B);
@@ -983,6 +981,7 @@ bool ell_gershgorin(bml_matrix_ellpack_t *A, double *bounds)
             static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->N, hi, lo);
     double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
     // emax starts at DBL_MIN and emin at DBL_MAX, as in the reference (:88-89).
+    b200_count_launch(); // gershgorin_kernel
     b200_maxmin_rows_kernel<<<1, 1024, 0, c->stream>>>(hi, lo, A->N, DBL_MIN, DBL_MAX, out);
     if (!LAUNCH_OK("gershgorin kernels"))
         return false;

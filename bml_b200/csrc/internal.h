@@ -81,7 +81,8 @@ int b200_get_error();
 // Evaluates a CUDA runtime call; on failure records ERR_CUDA and yields false.
 bool b200_cuda_ok(cudaError_t err, const char *what, const char *file, int line);
 #define CUDA_OK(call) b200_cuda_ok((call), #call, __FILE__, __LINE__)
-#define LAUNCH_OK(what) b200_cuda_ok(cudaGetLastError(), what, __FILE__, __LINE__)
+void b200_count_launch();
+#define LAUNCH_OK(what) (b200_count_launch(), b200_cuda_ok(cudaGetLastError(), what, __FILE__, __LINE__))
 
 // ---------------------------------------------------------------------------
 // Device context: one CUDA stream per process on the current device, a

@@ -266,6 +266,11 @@ BML_B200_API int bml_b200_multiply_x2(bml_matrix_t *X, bml_matrix_t *X2,
  * truncation to M (lets a caller size M exactly after ROW_OVERFLOW). */
 BML_B200_API int bml_b200_last_required_M(void);
 
+/* Diagnostics of the last ELLPACK multiply: rows per kernel tier (tier A:
+ * one warp and a 1024-slot table; O1-O3: sixteen warps and 2048/4096/8192
+ * slots; C: dense accumulator in device memory).  Returns the tier count. */
+BML_B200_API int bml_b200_last_tier_counts(int *counts, int n);
+
 /* Raw ELLPACK transfer between the device matrix and caller host arrays laid
  * out like the reference (row-major value[N*M], index[N*M], nnz[N]). */
 BML_B200_API int bml_b200_ellpack_upload(bml_matrix_t *A, const void *value,
@@ -279,6 +284,15 @@ BML_B200_API int bml_b200_ellpack_device_arrays(bml_matrix_t *A, void **d_value,
 BML_B200_API long long bml_b200_nnz(bml_matrix_t *A);
 /* Wait for all work this library queued. */
 BML_B200_API int bml_b200_synchronize(void);
+/* Select the CUDA device the library starts on (before its first call; one
+ * process per GPU).  Default: the thread's current device. */
+BML_B200_API int bml_b200_set_device(int device);
+/* Number of kernels this library has launched so far in this process. */
+BML_B200_API unsigned long long bml_b200_launch_count(void);
+/* CUDA events on the library's stream (slots 0..63), for timing its work on
+ * the device: record, then milliseconds between two recorded slots. */
+BML_B200_API int bml_b200_event_record(int slot);
+BML_B200_API int bml_b200_event_elapsed(int a, int b, float *ms);
 /* Device properties this library uses: SM count, device ordinal. */
 BML_B200_API int bml_b200_device_info(int *sm_count, int *device);
 
