@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="small case for ncu: 30^3 lattice, 3 SP2 iterations then one X^2")
     return ap.parse_args()
 
 
@@ -356,9 +358,31 @@ def run_reference(args, rank, world):
             "e2e": {"value": dt, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_profile_case():
+    """A case small enough for an ncu capture (about 3 GB on the device):
+    the 30^3 lattice (N=27000), three SP2 iterations, then one more X^2 whose
+    kernels are the ones to capture (skip the launches of the first three)."""
+    import bml_b200 as B
+    Lp = 30
+    Np = Lp ** 3
+    v, ix, nz = B.gen_lattice(Lp, RADIUS, Np, M_H, SEED)
+    H = B.Ellpack.from_arrays(v, ix, nz, Np, M_H)
+    D = B.Ellpack(Np, M_X)
+    info = (C.c_double * 6)()
+    B.check(B.lib.bml_b200_sp2(H.h, D.h, THRESHOLD, Np / 2.0, 3, 1e-8, 0, info))
+    X2 = B.Ellpack(Np, M_X)
+    tr = (C.c_double * 2)()
+    B.check(B.lib.bml_b200_multiply_x2(D.h, X2.h, THRESHOLD, tr))
+    print(json.dumps({"profile_case": "30^3 lattice, X^2 after 3 SP2 iterations", "trace": list(tr),
+                      "tiers": B.last_tier_counts(), "width": B.lib.bml_b200_last_required_M()}))
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.profile:
+        run_profile_case()
+        return
     if args.impl == "reference":
         res = run_reference(args, rank, world)
     else:

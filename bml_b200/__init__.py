@@ -12,7 +12,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libbml_b200.so")
+# BML_B200_LIB names another build of the same library (e.g. one compiled with
+# different tuning switches); by default the in-tree build is loaded.
+LIB_PATH = os.environ.get("BML_B200_LIB") or os.path.join(HERE, "libbml_b200.so")
 
 # enumerators of the reference's bml_types.h (same order)
 TYPE = {"dense": 1, "ellpack": 2, "ellblock": 3, "csr": 4}

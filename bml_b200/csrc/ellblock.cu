@@ -1,0 +1,1597 @@
+// ELLBLOCK (block ELLPACK) matrices: storage, host mirror, constructors,
+// element access, and the block-row kernels of the thresholded path.
+//
+// Device layout: one pool of NB*MB slots of maxbs*maxbs elements; block
+// (ib, jp) (the jp-th block of block row ib, column block indexb[ib*MB+jp])
+// is a row-major bsize[ib] x bsize[jb] array at slot ib*MB + jp.  The host
+// mirror uses the same slots, and ptr_value[ib*MB + jp] points at them for
+// jp < nnzb[ib] (the reference's per-block pointers, bml_types_ellblock.h:36).
+//
+// Every kernel works on whole block rows (one CTA per block row), follows the
+// reference loop's block order and element arithmetic, and keeps or drops
+// whole blocks by their max-norm as the reference does.
+#include "ellblock.h"
+#include "device_util.cuh"
+
+#include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+using namespace b200;
+
+extern "C" void bml_b200_reset_block_sizes(void);
+
+namespace {
+
+inline size_t eb_pool_elems(const bml_matrix_ellblock_t *A)
+{
+    return (size_t) A->NB * A->MB * A->slot_elems;
+}
+
+template <typename T> struct EbView
+{
+    T *pool;
+    int *indexb;
+    int *nnzb;
+    const int *bsize;
+    const int *boff;
+    int NB, MB;
+    long long slot;
+    __device__ T *blk(int ib, int jp) const { return pool + ((size_t) ib * MB + jp) * slot; }
+};
+
+template <typename T> EbView<T> view(bml_matrix_ellblock_t *A)
+{
+    return EbView<T>{static_cast<T *>(A->d_pool), A->d_indexb, A->d_nnzb, A->d_bsize, A->d_boff,
+                     A->NB, A->MB, A->slot_elems};
+}
+
+void host_pointers(bml_matrix_ellblock_t *A)
+{
+    const size_t sz = prec_size(A->matrix_precision);
+    for (int ib = 0; ib < A->NB; ib++)
+        for (int jp = 0; jp < A->MB; jp++)
+        {
+            const size_t ind = (size_t) ib * A->MB + jp;
+            A->ptr_value[ind] =
+                jp < A->nnzb[ib] ? static_cast<char *>(A->h_pool) + ind * A->slot_elems * sz : nullptr;
+        }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// storage
+// ---------------------------------------------------------------------------
+bml_matrix_ellblock_t *eb_alloc_blocks(bml_matrix_precision_t prec, int NB, int MB, int M,
+                                       const int *bsize, bml_distribution_mode_t mode)
+{
+    const size_t sz = prec_size(prec);
+    if (sz == 0)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "ELLBLOCK precision %d", (int) prec);
+        return nullptr;
+    }
+    if (NB <= 0 || MB <= 0 || !bsize)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK NB=%d MB=%d", NB, MB);
+        return nullptr;
+    }
+    B200Context *c = b200_ctx();
+    if (!c)
+        return nullptr;
+    auto *A = static_cast<bml_matrix_ellblock_t *>(calloc(1, sizeof(bml_matrix_ellblock_t)));
+    if (!A)
+        return nullptr;
+    A->matrix_type = ellblock;
+    A->matrix_precision = prec;
+    A->distribution_mode = mode;
+    A->NB = NB;
+    A->MB = MB;
+    A->M = M;
+    A->bsize = static_cast<int *>(malloc(sizeof(int) * NB));
+    memcpy(A->bsize, bsize, sizeof(int) * NB);
+    int N = 0, maxbs = 0;
+    std::vector<int> boff(NB + 1, 0);
+    for (int ib = 0; ib < NB; ib++)
+    {
+        boff[ib] = N;
+        N += bsize[ib];
+        maxbs = bsize[ib] > maxbs ? bsize[ib] : maxbs;
+    }
+    boff[NB] = N;
+    A->N = N;
+    A->maxbs = maxbs;
+    A->slot_elems = (long long) maxbs * maxbs;
+    A->indexb = static_cast<int *>(malloc(sizeof(int) * (size_t) NB * MB));
+    for (size_t q = 0; q < (size_t) NB * MB; q++)
+        A->indexb[q] = -1;
+    A->nnzb = static_cast<int *>(calloc(NB, sizeof(int)));
+    A->ptr_value = static_cast<void **>(calloc((size_t) NB * MB, sizeof(void *)));
+    A->h_pool = calloc(eb_pool_elems(A), sz);
+    A->domain = b200_default_domain(N, M, mode);
+    A->domain2 = b200_default_domain(N, M, mode);
+    bool ok = A->bsize && A->indexb && A->nnzb && A->ptr_value && A->h_pool;
+    if (ok)
+    {
+        cudaError_t e1 = cudaMalloc(&A->d_pool, eb_pool_elems(A) * sz);
+        cudaError_t e2 = cudaMalloc(reinterpret_cast<void **>(&A->d_indexb), sizeof(int) * (size_t) NB * MB);
+        cudaError_t e3 = cudaMalloc(reinterpret_cast<void **>(&A->d_nnzb), sizeof(int) * NB);
+        cudaError_t e4 = cudaMalloc(reinterpret_cast<void **>(&A->d_bsize), sizeof(int) * NB);
+        cudaError_t e5 = cudaMalloc(reinterpret_cast<void **>(&A->d_boff), sizeof(int) * (NB + 1));
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess ||
+            e5 != cudaSuccess)
+        {
+            cudaGetLastError();
+            b200_set_error(BML_B200_ERR_ALLOC, "ELLBLOCK device arrays NB=%d MB=%d maxbs=%d", NB, MB, maxbs);
+            ok = false;
+        }
+    }
+    ok = ok && CUDA_OK(cudaMemcpyAsync(A->d_bsize, bsize, sizeof(int) * NB, cudaMemcpyHostToDevice, c->stream)) &&
+         CUDA_OK(cudaMemcpyAsync(A->d_boff, boff.data(), sizeof(int) * (NB + 1), cudaMemcpyHostToDevice,
+                                 c->stream)) &&
+         CUDA_OK(cudaMemcpyAsync(A->d_indexb, A->indexb, sizeof(int) * (size_t) NB * MB,
+                                 cudaMemcpyHostToDevice, c->stream)) &&
+         CUDA_OK(cudaMemsetAsync(A->d_nnzb, 0, sizeof(int) * NB, c->stream)) &&
+         CUDA_OK(cudaMemsetAsync(A->d_pool, 0, eb_pool_elems(A) * sz, c->stream)) && b200_sync();
+    if (!ok)
+    {
+        eb_free(A);
+        return nullptr;
+    }
+    A->mirror = MIRROR_SYNCED;
+    // the first matrix defines the process-wide partition (reference
+    // bml_allocate_ellblock_typed.c:237-240)
+    if (bml_get_mb() == 0)
+        bml_set_block_sizes(A->bsize, NB, MB);
+    return A;
+}
+
+void eb_free(bml_matrix_ellblock_t *A)
+{
+    if (!A)
+        return;
+    B200Context *c = b200_ctx();
+    if (c)
+        cudaStreamSynchronize(c->stream);
+    cudaFree(A->d_pool);
+    cudaFree(A->d_indexb);
+    cudaFree(A->d_nnzb);
+    cudaFree(A->d_bsize);
+    cudaFree(A->d_boff);
+    free(A->h_pool);
+    free(A->ptr_value);
+    free(A->indexb);
+    free(A->nnzb);
+    free(A->bsize);
+    b200_free_domain(A->domain);
+    b200_free_domain(A->domain2);
+    free(A);
+}
+
+bool eb_to_device(bml_matrix_ellblock_t *A)
+{
+    if (A->mirror != MIRROR_HOST_NEWER)
+        return true;
+    B200Context *c = b200_ctx();
+    if (!c)
+        return false;
+    const size_t sz = prec_size(A->matrix_precision);
+    if (!CUDA_OK(cudaMemcpyAsync(A->d_pool, A->h_pool, eb_pool_elems(A) * sz, cudaMemcpyHostToDevice,
+                                 c->stream)) ||
+        !CUDA_OK(cudaMemcpyAsync(A->d_indexb, A->indexb, sizeof(int) * (size_t) A->NB * A->MB,
+                                 cudaMemcpyHostToDevice, c->stream)) ||
+        !CUDA_OK(cudaMemcpyAsync(A->d_nnzb, A->nnzb, sizeof(int) * A->NB, cudaMemcpyHostToDevice,
+                                 c->stream)) ||
+        !b200_sync())
+        return false;
+    A->mirror = MIRROR_SYNCED;
+    return true;
+}
+
+bool eb_to_host(bml_matrix_ellblock_t *A)
+{
+    if (A->mirror != MIRROR_DEVICE_NEWER)
+        return true;
+    B200Context *c = b200_ctx();
+    if (!c)
+        return false;
+    const size_t sz = prec_size(A->matrix_precision);
+    if (!CUDA_OK(cudaMemcpyAsync(A->h_pool, A->d_pool, eb_pool_elems(A) * sz, cudaMemcpyDeviceToHost,
+                                 c->stream)) ||
+        !CUDA_OK(cudaMemcpyAsync(A->indexb, A->d_indexb, sizeof(int) * (size_t) A->NB * A->MB,
+                                 cudaMemcpyDeviceToHost, c->stream)) ||
+        !CUDA_OK(cudaMemcpyAsync(A->nnzb, A->d_nnzb, sizeof(int) * A->NB, cudaMemcpyDeviceToHost,
+                                 c->stream)) ||
+        !b200_sync())
+        return false;
+    host_pointers(A);
+    A->mirror = MIRROR_SYNCED;
+    return true;
+}
+
+static void eb_mark_device(bml_matrix_ellblock_t *A) { A->mirror = MIRROR_DEVICE_NEWER; }
+static void eb_mark_host(bml_matrix_ellblock_t *A) { A->mirror = MIRROR_HOST_NEWER; }
+
+void eb_clear(bml_matrix_ellblock_t *A)
+{
+    B200Context *c = b200_ctx();
+    if (!c)
+        return;
+    if (CUDA_OK(cudaMemsetAsync(A->d_nnzb, 0, sizeof(int) * A->NB, c->stream)))
+    {
+        if (A->mirror == MIRROR_HOST_NEWER)
+            A->mirror = MIRROR_SYNCED;
+        eb_mark_device(A);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// constructors: filled on the host in the reference's order, then uploaded
+// (ellblock/bml_allocate_ellblock_typed.c:245-443)
+// ---------------------------------------------------------------------------
+template <typename T> static T *hblk(bml_matrix_ellblock_t *A, int ib, int jp)
+{
+    return static_cast<T *>(A->h_pool) + ((size_t) ib * A->MB + jp) * A->slot_elems;
+}
+
+template <typename T> static void eb_set_element_host(bml_matrix_ellblock_t *A, int i, int j, T v, bool append_new)
+{
+    (void) append_new;
+    int ib = 0, jb = 0, ii = i, jj = j;
+    while (ii >= A->bsize[ib])
+    {
+        ii -= A->bsize[ib];
+        ib++;
+    }
+    while (jj >= A->bsize[jb])
+    {
+        jj -= A->bsize[jb];
+        jb++;
+    }
+    for (int jp = 0; jp < A->nnzb[ib]; jp++)
+        if (A->indexb[(size_t) ib * A->MB + jp] == jb)
+        {
+            hblk<T>(A, ib, jp)[ii * A->bsize[jb] + jj] = v;
+            return;
+        }
+    if (A->nnzb[ib] == A->MB)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "Number of non-zeroes blocks per row > MB, Increase MB");
+        return;
+    }
+    const int jp = A->nnzb[ib];
+    T *b = hblk<T>(A, ib, jp);
+    memset(b, 0, sizeof(T) * A->bsize[ib] * A->bsize[jb]);
+    b[ii * A->bsize[jb] + jj] = v;
+    A->indexb[(size_t) ib * A->MB + jp] = jb;
+    A->nnzb[ib]++;
+}
+
+template <typename T> static void fill_eb(bml_matrix_ellblock_t *A, int kind)
+{
+    const int NB = A->NB, MB = A->MB;
+    const int *bsize = A->bsize;
+    if (kind == 1) // random (bml_allocate_ellblock_typed.c:336-393)
+    {
+        std::vector<int> marker(NB, -1), pos(MB);
+        for (int ib = 0; ib < NB; ib++)
+        {
+            int bcol = ib, n = 0;
+            for (int jb = 0; jb < MB; jb++)
+            {
+                if (marker[bcol] == -1)
+                {
+                    T *b = hblk<T>(A, ib, n);
+                    for (int ii = 0; ii < bsize[ib]; ii++)
+                        for (int jj = 0; jj < bsize[bcol]; jj++)
+                            b[ii * bsize[bcol] + jj] = rand() / (T) RAND_MAX;
+                    A->indexb[(size_t) ib * MB + n] = bcol;
+                    pos[n] = bcol;
+                    marker[bcol] = 1;
+                    n++;
+                }
+                bcol = rand() % NB;
+            }
+            A->nnzb[ib] = n;
+            for (int q = 0; q < n; q++)
+                marker[pos[q]] = -1;
+        }
+    }
+    else if (kind == 2) // banded through set_element_new (:171-187)
+    {
+        const int N = A->N, M = A->M;
+        for (int i = 0; i < N; i++)
+            for (int j = (i - M / 2 >= 0 ? i - M / 2 : 0); j < (i - M / 2 + M <= N ? i - M / 2 + M : N); j++)
+                eb_set_element_host<T>(A, i, j, rand() / (T) RAND_MAX, true);
+    }
+    else if (kind == 3) // identity (:421-443)
+    {
+        for (int ib = 0; ib < NB; ib++)
+        {
+            T *b = hblk<T>(A, ib, 0);
+            memset(b, 0, sizeof(T) * bsize[ib] * bsize[ib]);
+            for (int ii = 0; ii < bsize[ib]; ii++)
+                b[ii * bsize[ib] + ii] = (T) 1.0;
+            A->nnzb[ib] = 1;
+            A->indexb[(size_t) ib * MB] = ib;
+        }
+    }
+}
+
+bml_matrix_ellblock_t *eb_constructor(int kind, bml_matrix_precision_t prec, int N, int M,
+                                      bml_distribution_mode_t mode)
+{
+    if (N <= 0)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK N=%d", N);
+        return nullptr;
+    }
+    int *bsize = bml_get_block_sizes(N, M);
+    bml_matrix_ellblock_t *A = eb_alloc_blocks(prec, bml_get_nb(), bml_get_mb(), M, bsize, mode);
+    if (!A || kind == 0 || kind == 4)
+        return A;
+    if (prec == double_real)
+        fill_eb<double>(A, kind);
+    else
+        fill_eb<float>(A, kind);
+    eb_mark_host(A);
+    if (!eb_to_device(A))
+    {
+        eb_free(A);
+        return nullptr;
+    }
+    return A;
+}
+
+// ---------------------------------------------------------------------------
+// host-side element access on the mirror
+// ---------------------------------------------------------------------------
+void eb_set_element(bml_matrix_ellblock_t *A, int i, int j, const void *value, bool append_new)
+{
+    if (!A || !value || i < 0 || j < 0 || i >= A->N || j >= A->N)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK set_element (%d, %d)", i, j);
+        return;
+    }
+    if (!eb_to_host(A))
+        return;
+    if (A->matrix_precision == double_real)
+        eb_set_element_host<double>(A, i, j, *static_cast<const double *>(value), append_new);
+    else
+        eb_set_element_host<float>(A, i, j, *static_cast<const float *>(value), append_new);
+    host_pointers(A);
+    eb_mark_host(A);
+}
+
+template <typename T> static T eb_get_host(bml_matrix_ellblock_t *A, int i, int j, bool &found, T **where)
+{
+    int ib = 0, jb = 0, ii = i, jj = j;
+    while (ii >= A->bsize[ib])
+    {
+        ii -= A->bsize[ib];
+        ib++;
+    }
+    while (jj >= A->bsize[jb])
+    {
+        jj -= A->bsize[jb];
+        jb++;
+    }
+    for (int jp = 0; jp < A->nnzb[ib]; jp++)
+        if (A->indexb[(size_t) ib * A->MB + jp] == jb)
+        {
+            found = true;
+            *where = hblk<T>(A, ib, jp) + ii * A->bsize[jb] + jj;
+            return **where;
+        }
+    found = false;
+    return T(0);
+}
+
+void *eb_get_element(bml_matrix_ellblock_t *A, int i, int j)
+{
+    static double zd = 0.0, md = -1.0;
+    static float zf = 0.0f, mf = -1.0f;
+    const bool dbl = A && A->matrix_precision == double_real;
+    if (!A || i < 0 || j < 0 || i >= A->N || j >= A->N)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK get_element (%d, %d)", i, j);
+        return dbl ? (void *) &md : (void *) &mf;
+    }
+    if (!eb_to_host(A))
+        return nullptr;
+    bool found = false;
+    if (dbl)
+    {
+        double *w = nullptr;
+        eb_get_host<double>(A, i, j, found, &w);
+        return found ? (void *) w : (void *) &zd;
+    }
+    float *w = nullptr;
+    eb_get_host<float>(A, i, j, found, &w);
+    return found ? (void *) w : (void *) &zf;
+}
+
+void *eb_get_row(bml_matrix_ellblock_t *A, int i)
+{
+    if (!A || !eb_to_host(A))
+        return nullptr;
+    const size_t sz = prec_size(A->matrix_precision);
+    char *row = static_cast<char *>(calloc(A->N, sz));
+    if (!row || i < 0 || i >= A->N)
+        return row;
+    for (int j = 0; j < A->N; j++)
+    {
+        void *e = eb_get_element(A, i, j);
+        memcpy(row + j * sz, e, sz);
+    }
+    return row;
+}
+
+void *eb_get_diagonal(bml_matrix_ellblock_t *A)
+{
+    if (!A || !eb_to_host(A))
+        return nullptr;
+    const size_t sz = prec_size(A->matrix_precision);
+    char *d = static_cast<char *>(calloc(A->N, sz));
+    for (int i = 0; d && i < A->N; i++)
+        memcpy(d + i * sz, eb_get_element(A, i, i), sz);
+    return d;
+}
+
+int eb_row_bandwidth(bml_matrix_ellblock_t *A, int i)
+{
+    if (!A || !eb_to_host(A) || i < 0 || i >= A->N)
+        return -1;
+    int ib = 0, ii = i;
+    while (ii >= A->bsize[ib])
+    {
+        ii -= A->bsize[ib];
+        ib++;
+    }
+    int w = 0;
+    for (int jp = 0; jp < A->nnzb[ib]; jp++)
+        w += A->bsize[A->indexb[(size_t) ib * A->MB + jp]];
+    return w;
+}
+
+int eb_bandwidth(bml_matrix_ellblock_t *A)
+{
+    if (!A || !eb_to_host(A))
+        return -1;
+    int best = 0;
+    for (int ib = 0, i0 = 0; ib < A->NB; i0 += A->bsize[ib], ib++)
+    {
+        const int w = eb_row_bandwidth(A, i0);
+        best = w > best ? w : best;
+    }
+    return best;
+}
+
+double eb_sparsity(bml_matrix_ellblock_t *A, double threshold)
+{
+    if (!A || !eb_to_host(A))
+        return -1.0;
+    long long nz = 0;
+    const bool dbl = A->matrix_precision == double_real;
+    for (int ib = 0; ib < A->NB; ib++)
+        for (int jp = 0; jp < A->nnzb[ib]; jp++)
+        {
+            const int jb = A->indexb[(size_t) ib * A->MB + jp];
+            const int ne = A->bsize[ib] * A->bsize[jb];
+            for (int e = 0; e < ne; e++)
+            {
+                const double v = dbl ? hblk<double>(A, ib, jp)[e] : hblk<float>(A, ib, jp)[e];
+                if (fabs(v) > threshold)
+                    nz++;
+            }
+        }
+    return 1.0 - (double) nz / ((double) A->N * A->N);
+}
+
+long long eb_nnz(bml_matrix_ellblock_t *A)
+{
+    if (!A || !eb_to_host(A))
+        return -1;
+    long long n = 0;
+    for (int ib = 0; ib < A->NB; ib++)
+        for (int jp = 0; jp < A->nnzb[ib]; jp++)
+            n += (long long) A->bsize[ib] * A->bsize[A->indexb[(size_t) ib * A->MB + jp]];
+    return n;
+}
+
+// ---------------------------------------------------------------------------
+// device kernels, one block row per CTA
+// ---------------------------------------------------------------------------
+namespace {
+
+// max |x| over a block, as the double the reference's bml_norm_inf returns
+template <typename T> __device__ double block_norm_inf(const T *x, int ne, double *red)
+{
+    double m = 0.0;
+    for (int e = threadIdx.x; e < ne; e += blockDim.x)
+        m = fmax(m, (double) fabs(x[e]));
+    for (int o = 16; o; o >>= 1)
+        m = fmax(m, __shfl_xor_sync(FULL, m, o));
+    if ((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    double r = 0.0;
+    for (int w = 0; w < (int) (blockDim.x >> 5); ++w)
+        r = fmax(r, red[w]);
+    __syncthreads();
+    return r;
+}
+
+// copy B <- A (same partition)
+template <typename T> __global__ void eb_copy_kernel(EbView<T> A, EbView<T> B, int *overflow)
+{
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    {
+        const int n = A.nnzb[ib];
+        if (n > B.MB)
+        {
+            if (threadIdx.x == 0)
+                atomicExch(overflow, 1);
+            continue;
+        }
+        for (int jp = 0; jp < n; ++jp)
+        {
+            const int jb = A.indexb[(size_t) ib * A.MB + jp];
+            const int ne = A.bsize[ib] * A.bsize[jb];
+            const T *src = A.blk(ib, jp);
+            T *dst = B.blk(ib, jp);
+            for (int e = threadIdx.x; e < ne; e += blockDim.x)
+                dst[e] = src[e];
+            if (threadIdx.x == 0)
+                B.indexb[(size_t) ib * B.MB + jp] = jb;
+        }
+        if (threadIdx.x == 0)
+            B.nnzb[ib] = n;
+    }
+}
+
+// scale every stored element: x <- s*x (ellblock/bml_scale_ellblock_typed.c:66-87)
+template <typename T> __global__ void eb_scale_kernel(EbView<T> A, T s)
+{
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+        for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+        {
+            const int jb = A.indexb[(size_t) ib * A.MB + jp];
+            const int ne = A.bsize[ib] * A.bsize[jb];
+            T *x = A.blk(ib, jp);
+            for (int e = threadIdx.x; e < ne; e += blockDim.x)
+                x[e] = mul_rn(s, x[e]);
+        }
+}
+
+// A <- alpha*A + beta*B, block kept if max|x| > thr (norm rounded to the
+// matrix precision, as `REAL_T normx = bml_norm_inf(...)` does)
+// (ellblock/bml_add_ellblock_typed.c:35-197).  Blocks: A's in order, then
+// B's new ones in order.  The merged blocks are built in a per-CTA slab of
+// MBout slots and copied back.
+template <typename T>
+__global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double beta, double thr,
+                              T *slab, int *marks, int *overflow)
+{
+    __shared__ int list[1024];   // merged column-block list
+    __shared__ int src_a[1024];  // position in A or -1
+    __shared__ int src_b[1024];  // position in B or -1
+    __shared__ int nl, ll;
+    __shared__ double red[32];
+    const bool use_a = alpha > 0.0 || alpha < 0.0;
+    const bool use_b = beta > 0.0 || beta < 0.0;
+    T *myslab = slab + (size_t) blockIdx.x * A.MB * A.slot;
+    int *mark = marks + (size_t) blockIdx.x * A.NB;
+    const T thr_t = (T) thr;
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    {
+        if (threadIdx.x == 0)
+        {
+            int n = 0;
+            const int na = use_a ? A.nnzb[ib] : 0, nb = use_b ? B.nnzb[ib] : 0;
+            for (int p = 0; p < na && n < 1024; ++p)
+            {
+                const int jb = A.indexb[(size_t) ib * A.MB + p];
+                mark[jb] = n + 1;
+                list[n] = jb;
+                src_a[n] = p;
+                src_b[n] = -1;
+                n++;
+            }
+            for (int p = 0; p < nb && n < 1024; ++p)
+            {
+                const int jb = B.indexb[(size_t) ib * B.MB + p];
+                if (mark[jb])
+                    src_b[mark[jb] - 1] = p;
+                else
+                {
+                    mark[jb] = n + 1;
+                    list[n] = jb;
+                    src_a[n] = -1;
+                    src_b[n] = p;
+                    n++;
+                }
+            }
+            for (int q = 0; q < n; ++q)
+                mark[list[q]] = 0;
+            nl = n;
+            ll = 0;
+        }
+        __syncthreads();
+        const int n = nl;
+        int kept = 0;
+        for (int q = 0; q < n; ++q)
+        {
+            const int jb = list[q];
+            const int ne = A.bsize[ib] * A.bsize[jb];
+            T *x = myslab + (size_t) kept * A.slot;
+            const T *a = src_a[q] >= 0 ? A.blk(ib, src_a[q]) : nullptr;
+            const T *b = src_b[q] >= 0 ? B.blk(ib, src_b[q]) : nullptr;
+            for (int e = threadIdx.x; e < ne; e += blockDim.x)
+            {
+                T v = T(0);
+                if (a)
+                    v = axpy_d(v, alpha, a[e]);
+                if (b)
+                    v = axpy_d(v, beta, b[e]);
+                x[e] = v;
+            }
+            __syncthreads();
+            const T normx = (T) block_norm_inf(x, ne, red);
+            if (fabs(normx) > thr_t)
+            {
+                if (threadIdx.x == 0)
+                    list[kept] = jb; // q >= kept: safe in place
+                kept++;
+            }
+            __syncthreads();
+        }
+        if (kept > A.MB)
+        {
+            if (threadIdx.x == 0)
+                atomicExch(overflow, 1);
+            kept = A.MB;
+        }
+        for (int q = 0; q < kept; ++q)
+        {
+            const int jb = list[q];
+            const int ne = A.bsize[ib] * A.bsize[jb];
+            T *dst = A.blk(ib, q);
+            const T *src = myslab + (size_t) q * A.slot;
+            for (int e = threadIdx.x; e < ne; e += blockDim.x)
+                dst[e] = src[e];
+            if (threadIdx.x == 0)
+                A.indexb[(size_t) ib * A.MB + q] = jb;
+        }
+        if (threadIdx.x == 0)
+            A.nnzb[ib] = kept;
+        __syncthreads();
+    }
+}
+
+// threshold: drop blocks with max|x| <= thr (order kept), zero the elements
+// with |x| <= thr in the others (ellblock/bml_threshold_ellblock_typed.c:95-140)
+template <typename T> __global__ void eb_threshold_kernel(EbView<T> A, EbView<T> B, double thr)
+{
+    __shared__ double red[32];
+    const T thr_t = (T) thr;
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    {
+        int out = 0;
+        const int n = A.nnzb[ib];
+        for (int jp = 0; jp < n; ++jp)
+        {
+            const int jb = A.indexb[(size_t) ib * A.MB + jp];
+            const int ne = A.bsize[ib] * A.bsize[jb];
+            const T *x = A.blk(ib, jp);
+            const T normx = (T) block_norm_inf(x, ne, red);
+            if (fabs(normx) > thr_t)
+            {
+                T *y = B.blk(ib, out);
+                for (int e = threadIdx.x; e < ne; e += blockDim.x)
+                {
+                    const T v = x[e];
+                    y[e] = fabs(v) > thr_t ? v : T(0);
+                }
+                if (threadIdx.x == 0)
+                    B.indexb[(size_t) ib * B.MB + out] = jb;
+                out++;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            B.nnzb[ib] = out;
+        __syncthreads();
+    }
+}
+
+// per-block-row diagonal sums: first diagonal block of the row
+// (ellblock/bml_trace_ellblock_typed.c:27-58)
+template <typename T> __global__ void eb_diag_kernel(EbView<T> A, double *d)
+{
+    for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < A.NB; ib += gridDim.x * blockDim.x)
+    {
+        double s = 0.0;
+        T acc = T(0);
+        for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+            if (A.indexb[(size_t) ib * A.MB + jp] == ib)
+            {
+                const T *x = A.blk(ib, jp);
+                for (int ii = 0; ii < A.bsize[ib]; ++ii)
+                    acc = add_rn(acc, x[ii * A.bsize[ib] + ii]);
+                break;
+            }
+        s = (double) acc;
+        d[ib] = s;
+    }
+}
+
+// trace(A*B) = sum over ib, A's blocks (ib, jb), B's blocks (jb, ib) of
+// sum_ii sum_jj A[ii][jj] B[jj][ii] (ellblock/bml_trace_ellblock_typed.c:69-122)
+template <typename T> __global__ void eb_trace_mult_kernel(EbView<T> A, EbView<T> B, double *part)
+{
+    __shared__ double red[32];
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    {
+        double s = 0.0;
+        for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+        {
+            const int jb = A.indexb[(size_t) ib * A.MB + jp];
+            const T *a = A.blk(ib, jp);
+            for (int kp = 0; kp < B.nnzb[jb]; ++kp)
+                if (B.indexb[(size_t) jb * B.MB + kp] == ib)
+                {
+                    const T *b = B.blk(jb, kp);
+                    const int bi = A.bsize[ib], bj = A.bsize[jb];
+                    for (int e = threadIdx.x; e < bi * bj; e += blockDim.x)
+                    {
+                        const int ii = e / bj, jj = e % bj;
+                        s += (double) mul_rn(a[ii * bj + jj], b[jj * bi + ii]);
+                    }
+                }
+        }
+        for (int o = 16; o; o >>= 1)
+            s += __shfl_xor_sync(FULL, s, o);
+        if ((threadIdx.x & 31) == 0)
+            red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double t = 0.0;
+            for (int w = 0; w < (int) (blockDim.x >> 5); ++w)
+                t += red[w];
+            part[ib] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// Gershgorin per scalar row (ellblock/bml_normalize_ellblock_typed.c:97-150):
+// dval = the diagonal element, rad += (double)|a| over all other elements of
+// the row, in block order; hi/lo = dval +/- rad in the matrix precision.
+template <typename T> __global__ void eb_gersh_kernel(EbView<T> A, double *hi, double *lo)
+{
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+        for (int ii = threadIdx.x; ii < A.bsize[ib]; ii += blockDim.x)
+        {
+            T rad = T(0), dval = T(0);
+            for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+            {
+                const int jb = A.indexb[(size_t) ib * A.MB + jp];
+                const T *x = A.blk(ib, jp) + ii * A.bsize[jb];
+                for (int jj = 0; jj < A.bsize[jb]; ++jj)
+                {
+                    if (ib == jb && ii == jj)
+                        dval = x[jj];
+                    else
+                        rad = (T) __dadd_rn((double) rad, (double) fabs(x[jj]));
+                }
+            }
+            const int i = A.boff[ib] + ii;
+            hi[i] = (double) add_rn(dval, rad);
+            lo[i] = (double) add_rn(dval, (T) -rad);
+        }
+}
+
+// transpose: block (ib, jb) -> (jb, ib) transposed, appended to block row jb
+// in ascending ib (the serial order of ellblock/bml_transpose_ellblock_typed.c:
+// 29-70).  One thread per destination block row gathers its blocks in order.
+template <typename T> __global__ void eb_transpose_kernel(EbView<T> A, EbView<T> B, int *overflow)
+{
+    for (int jb = blockIdx.x; jb < A.NB; jb += gridDim.x)
+    {
+        __shared__ int n;
+        if (threadIdx.x == 0)
+            n = 0;
+        __syncthreads();
+        for (int ib = 0; ib < A.NB; ++ib)
+        {
+            __shared__ int found;
+            if (threadIdx.x == 0)
+            {
+                found = -1;
+                for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+                    if (A.indexb[(size_t) ib * A.MB + jp] == jb)
+                    {
+                        found = jp;
+                        break;
+                    }
+            }
+            __syncthreads();
+            if (found >= 0)
+            {
+                if (n >= B.MB)
+                {
+                    if (threadIdx.x == 0)
+                        atomicExch(overflow, 1);
+                }
+                else
+                {
+                    const int bi = A.bsize[ib], bj = A.bsize[jb];
+                    const T *a = A.blk(ib, found);
+                    T *b = B.blk(jb, n);
+                    for (int e = threadIdx.x; e < bi * bj; e += blockDim.x)
+                    {
+                        const int ii = e / bj, jj = e % bj;
+                        b[jj * bi + ii] = a[e];
+                    }
+                    if (threadIdx.x == 0)
+                        B.indexb[(size_t) jb * B.MB + n] = ib;
+                }
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    n++;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            B.nnzb[jb] = n < B.MB ? n : B.MB;
+        __syncthreads();
+    }
+}
+
+// dense import/export (ellblock/bml_import_ellblock_typed.c, bml_export_ellblock_typed.c)
+template <typename T>
+__global__ void eb_import_kernel(EbView<T> A, const T *D, int N, int colmajor, double thr, int *overflow)
+{
+    __shared__ double red[32];
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    {
+        int n = 0;
+        for (int jb = 0; jb < A.NB; ++jb)
+        {
+            const int bi = A.bsize[ib], bj = A.bsize[jb];
+            const int r0 = A.boff[ib], c0 = A.boff[jb];
+            double m = 0.0;
+            for (int e = threadIdx.x; e < bi * bj; e += blockDim.x)
+            {
+                const int ii = e / bj, jj = e % bj;
+                const T v = colmajor ? D[(size_t) (c0 + jj) * N + r0 + ii] : D[(size_t) (r0 + ii) * N + c0 + jj];
+                m = fmax(m, (double) fabs(v));
+            }
+            for (int o = 16; o; o >>= 1)
+                m = fmax(m, __shfl_xor_sync(FULL, m, o));
+            if ((threadIdx.x & 31) == 0)
+                red[threadIdx.x >> 5] = m;
+            __syncthreads();
+            double norm = 0.0;
+            for (int w = 0; w < (int) (blockDim.x >> 5); ++w)
+                norm = fmax(norm, red[w]);
+            __syncthreads();
+            if (norm > thr)
+            {
+                if (n < A.MB)
+                {
+                    T *x = A.blk(ib, n);
+                    for (int e = threadIdx.x; e < bi * bj; e += blockDim.x)
+                    {
+                        const int ii = e / bj, jj = e % bj;
+                        x[e] = colmajor ? D[(size_t) (c0 + jj) * N + r0 + ii] : D[(size_t) (r0 + ii) * N + c0 + jj];
+                    }
+                    if (threadIdx.x == 0)
+                        A.indexb[(size_t) ib * A.MB + n] = jb;
+                }
+                else if (threadIdx.x == 0)
+                    atomicExch(overflow, 1);
+                n++;
+            }
+        }
+        if (threadIdx.x == 0)
+            A.nnzb[ib] = n < A.MB ? n : A.MB;
+        __syncthreads();
+    }
+}
+
+template <typename T> __global__ void eb_export_kernel(EbView<T> A, T *D, int N, int colmajor)
+{
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+        for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+        {
+            const int jb = A.indexb[(size_t) ib * A.MB + jp];
+            const int bi = A.bsize[ib], bj = A.bsize[jb];
+            const int r0 = A.boff[ib], c0 = A.boff[jb];
+            const T *x = A.blk(ib, jp);
+            for (int e = threadIdx.x; e < bi * bj; e += blockDim.x)
+            {
+                const int ii = e / bj, jj = e % bj;
+                if (colmajor)
+                    D[(size_t) (c0 + jj) * N + r0 + ii] = x[e];
+                else
+                    D[(size_t) (r0 + ii) * N + c0 + jj] = x[e];
+            }
+        }
+}
+
+// ---------------------------------------------------------------------------
+// X^2 / A*B, exact form (ellblock/bml_multiply_ellblock_typed.c:246-442 and
+// :455-621).  One CTA per block row ib.  For every (jp, kp) in order the
+// block product X[ib,jb] X[jb,kb] is added into the accumulator of kb (first
+// touch: kb appended to the row's list, accumulator zeroed), element (ii, jj)
+// as x = x + s with s = a0*b0 + a1*b1 + ... summed left to right, exactly the
+// reference micro-kernel's expression.  Accumulators live in a per-CTA slab
+// in device memory (MB_out slots); each thread owns fixed elements of every
+// accumulator, so the only barriers are around the staging of the two
+// blocks in shared memory.  Kept blocks (kb == ib or max|x| > thr) are copied
+// to C in first-touch order.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, EbView<T> C, double thr,
+                                                     int use_norm_inf_fast, T *slab, int *marks,
+                                                     double *dA, double *dC, int *flags)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int maxbs = (int) sqrtf((float) A.slot + 0.5f);
+    T *sL = reinterpret_cast<T *>(smem);
+    T *sR = sL + (size_t) maxbs * maxbs;
+    int *list = reinterpret_cast<int *>(sR + (size_t) maxbs * maxbs); // kb in first-touch order
+    __shared__ int lb, firstflag, slotq;
+    __shared__ double red[32];
+    const int cap = min(C.MB + 1, 1024); // slab slots (one spare to detect overflow)
+    T *myslab = slab + (size_t) blockIdx.x * cap * A.slot;
+    int *mark = marks + (size_t) blockIdx.x * B.NB;
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    {
+        if (threadIdx.x == 0)
+            lb = 0;
+        __syncthreads();
+        T trA = T(0);
+        const int bi = A.bsize[ib];
+        for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+        {
+            const int jb = A.indexb[(size_t) ib * A.MB + jp];
+            const int bj = A.bsize[jb];
+            const T *L = A.blk(ib, jp);
+            for (int e = threadIdx.x; e < bi * bj; e += blockDim.x)
+                sL[e] = L[e];
+            if (jb == ib)
+                for (int kk = 0; kk < bi; ++kk)
+                    trA = add_rn(trA, L[kk * (1 + bi)]);
+            for (int kp = 0; kp < B.nnzb[jb]; ++kp)
+            {
+                const int kb = B.indexb[(size_t) jb * B.MB + kp];
+                const int bk = B.bsize[kb];
+                const T *R = B.blk(jb, kp);
+                if (threadIdx.x == 0)
+                {
+                    const int m = mark[kb];
+                    if (m == 0)
+                    {
+                        firstflag = 1;
+                        slotq = lb;
+                        if (lb < 1024)
+                            list[lb] = kb;
+                        mark[kb] = lb + 1;
+                        lb++;
+                    }
+                    else
+                    {
+                        firstflag = 0;
+                        slotq = m - 1;
+                    }
+                }
+                for (int e = threadIdx.x; e < bj * bk; e += blockDim.x)
+                    sR[e] = R[e];
+                __syncthreads();
+                const int q = slotq;
+                const bool first = firstflag;
+                if (q < cap)
+                {
+                    T *x = myslab + (size_t) q * A.slot;
+                    for (int e = threadIdx.x; e < bi * bk; e += blockDim.x)
+                    {
+                        const int ii = e / bk, jj = e % bk;
+                        T s = mul_rn(sL[ii * bj], sR[jj]);
+                        for (int l = 1; l < bj; ++l)
+                            s = add_rn(s, mul_rn(sL[ii * bj + l], sR[l * bk + jj]));
+                        x[e] = add_rn(first ? T(0) : x[e], s);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // keep and copy out in first-touch order
+        const int n = lb;
+        int kept = 0;
+        T trC = T(0);
+        for (int q = 0; q < n; ++q)
+        {
+            const int kb = list[q];
+            const int bk = B.bsize[kb];
+            if (threadIdx.x == 0)
+                mark[kb] = 0;
+            if (q >= cap)
+                continue;
+            const T *x = myslab + (size_t) q * A.slot;
+            const double normx = block_norm_inf(x, bi * bk, red);
+            const bool keep = kb == ib || (use_norm_inf_fast ? normx > thr : (T) normx > (T) thr);
+            if (keep)
+            {
+                if (kb == ib)
+                    for (int kk = 0; kk < bi; ++kk)
+                        trC = add_rn(trC, x[kk * (1 + bi)]);
+                if (kept < C.MB)
+                {
+                    T *dst = C.blk(ib, kept);
+                    for (int e = threadIdx.x; e < bi * bk; e += blockDim.x)
+                        dst[e] = x[e];
+                    if (threadIdx.x == 0)
+                        C.indexb[(size_t) ib * C.MB + kept] = kb;
+                }
+                kept++;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+        {
+            C.nnzb[ib] = kept < C.MB ? kept : C.MB;
+            atomicMax(&flags[1], kept);
+            if (kept > C.MB || n > cap)
+                atomicExch(&flags[0], 1);
+            if (dA)
+                dA[ib] = (double) trA;
+            if (dC)
+                dC[ib] = (double) trC;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T> int eb_grid(B200Context *c, int NB, int per_sm) { return max(1, min(NB, c->sm_count * per_sm)); }
+
+int *eb_flags(B200Context *c)
+{
+    int *f = reinterpret_cast<int *>(static_cast<unsigned char *>(c->d_small) + 4096);
+    if (!CUDA_OK(cudaMemsetAsync(f, 0, 16, c->stream)))
+        return nullptr;
+    return f;
+}
+
+bool eb_read_flags(B200Context *c, int *f, int *out, int n)
+{
+    int *pin = reinterpret_cast<int *>(static_cast<unsigned char *>(c->pinned) + 4096);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, f, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+        return false;
+    for (int q = 0; q < n; q++)
+        out[q] = pin[q];
+    return true;
+}
+
+bool same_partition(const bml_matrix_ellblock_t *A, const bml_matrix_ellblock_t *B, const char *op)
+{
+    if (!A || !B)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK %s: NULL matrix", op);
+        return false;
+    }
+    if (A->NB != B->NB || A->matrix_precision != B->matrix_precision ||
+        memcmp(A->bsize, B->bsize, sizeof(int) * A->NB) != 0)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK %s: block partitions or precisions differ", op);
+        return false;
+    }
+    return true;
+}
+
+template <typename T>
+bool eb_multiply_typed(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_matrix_ellblock_t *C,
+                       double thr, bool fast_norm, double *trace)
+{
+    B200Context *c = b200_ctx();
+    if (!c)
+        return false;
+    if (A->maxbs > 64)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "ELLBLOCK multiply: blocks larger than 64");
+        return false;
+    }
+    const int grid = eb_grid<T>(c, A->NB, 2);
+    const int cap = C->MB + 1 < 1024 ? C->MB + 1 : 1024;
+    const size_t slab = (size_t) grid * cap * A->slot_elems * sizeof(T);
+    const size_t marks = (size_t) grid * B->NB * sizeof(int);
+    const size_t diag = (size_t) 2 * A->NB * sizeof(double);
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(slab + marks + diag + 1024));
+    if (!scr)
+        return false;
+    T *dslab = reinterpret_cast<T *>(scr);
+    int *dmarks = reinterpret_cast<int *>(scr + slab);
+    double *dA = reinterpret_cast<double *>(scr + ((slab + marks + 255) & ~size_t(255)));
+    double *dC = dA + A->NB;
+    int *flags = eb_flags(c);
+    if (!flags || !CUDA_OK(cudaMemsetAsync(dmarks, 0, marks, c->stream)))
+        return false;
+    const size_t smem = 2 * (size_t) A->slot_elems * sizeof(T) + 1024 * sizeof(int);
+    auto k = eb_mul_kernel<T>;
+    if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+        return false;
+    k<<<grid, 256, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0, dslab,
+                                     dmarks, trace ? dA : nullptr, trace ? dC : nullptr, flags);
+    if (!LAUNCH_OK("eb_mul_kernel"))
+        return false;
+    if (trace)
+    {
+        double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 64);
+        b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(dA, dC, A->NB, out);
+        if (!LAUNCH_OK("b200_sum_rows_kernel"))
+            return false;
+    }
+    int hf[2 + 4];
+    int *pin = reinterpret_cast<int *>(static_cast<unsigned char *>(c->pinned) + 4096);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 64 + 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+        return false;
+    memcpy(hf, pin, sizeof(int) * 2);
+    eb_mark_device(C);
+    if (trace)
+    {
+        const double *t = reinterpret_cast<const double *>(reinterpret_cast<unsigned char *>(pin) + 64);
+        trace[0] = t[0];
+        trace[1] = t[1];
+    }
+    if (hf[0])
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW,
+                       "Number of non-zeroes blocks per row > MB, Increase MB (need %d, MB = %d)", hf[1], C->MB);
+        return false;
+    }
+    return true;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// entry points used by the C API
+// ---------------------------------------------------------------------------
+#define EB_DISPATCH(A, call) ((A)->matrix_precision == double_real ? call<double> : call<float>)
+
+bool eb_copy(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B)
+{
+    if (!same_partition(A, B, "copy"))
+        return false;
+    if (A == B)
+        return true;
+    B200Context *c = b200_ctx();
+    if (!c || !eb_to_device(A))
+        return false;
+    if (B->mirror == MIRROR_HOST_NEWER)
+        B->mirror = MIRROR_SYNCED;
+    int *f = eb_flags(c);
+    if (!f)
+        return false;
+    const int grid = A->matrix_precision == double_real ? eb_grid<double>(c, A->NB, 8) : eb_grid<float>(c, A->NB, 8);
+    if (A->matrix_precision == double_real)
+        eb_copy_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), view<double>(B), f);
+    else
+        eb_copy_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), view<float>(B), f);
+    if (!LAUNCH_OK("eb_copy_kernel"))
+        return false;
+    eb_mark_device(B);
+    int hf = 0;
+    if (!eb_read_flags(c, f, &hf, 1))
+        return false;
+    if (hf)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "ELLBLOCK copy: a block row of A exceeds B's MB");
+        return false;
+    }
+    return true;
+}
+
+bml_matrix_ellblock_t *eb_copy_new(bml_matrix_ellblock_t *A)
+{
+    if (!A)
+        return nullptr;
+    bml_matrix_ellblock_t *B = eb_alloc_blocks(A->matrix_precision, A->NB, A->MB, A->M, A->bsize,
+                                               A->distribution_mode);
+    if (B && !eb_copy(A, B))
+    {
+        eb_free(B);
+        return nullptr;
+    }
+    return B;
+}
+
+bool eb_scale(const void *scale, bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B)
+{
+    if (!scale || !same_partition(A, B, "scale"))
+        return false;
+    if (A != B && !eb_copy(A, B))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !eb_to_device(B))
+        return false;
+    const int grid = eb_grid<double>(c, B->NB, 8);
+    if (B->matrix_precision == double_real)
+        eb_scale_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(B), *static_cast<const double *>(scale));
+    else
+        eb_scale_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(B), *static_cast<const float *>(scale));
+    if (!LAUNCH_OK("eb_scale_kernel"))
+        return false;
+    eb_mark_device(B);
+    return true;
+}
+
+bool eb_add(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, double alpha, double beta, double threshold)
+{
+    if (!same_partition(A, B, "add"))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !eb_to_device(A) || !eb_to_device(B))
+        return false;
+    if (A == B)
+    {
+        bml_matrix_ellblock_t *T0 = eb_copy_new(A);
+        if (!T0)
+            return false;
+        const bool ok = eb_add(A, T0, alpha, beta, threshold);
+        eb_free(T0);
+        return ok;
+    }
+    const int grid = eb_grid<double>(c, A->NB, 4);
+    const size_t sz = prec_size(A->matrix_precision);
+    const size_t slab = (size_t) grid * A->MB * A->slot_elems * sz;
+    const size_t marks = (size_t) grid * A->NB * sizeof(int);
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(slab + marks + 256));
+    int *f = eb_flags(c);
+    if (!scr || !f || !CUDA_OK(cudaMemsetAsync(scr + slab, 0, marks, c->stream)))
+        return false;
+    if (A->matrix_precision == double_real)
+        eb_add_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), view<double>(B), alpha, beta, threshold,
+                                                           reinterpret_cast<double *>(scr),
+                                                           reinterpret_cast<int *>(scr + slab), f);
+    else
+        eb_add_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), view<float>(B), alpha, beta, threshold,
+                                                          reinterpret_cast<float *>(scr),
+                                                          reinterpret_cast<int *>(scr + slab), f);
+    if (!LAUNCH_OK("eb_add_kernel"))
+        return false;
+    eb_mark_device(A);
+    int hf = 0;
+    if (!eb_read_flags(c, f, &hf, 1))
+        return false;
+    if (hf)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "ELLBLOCK add: a block row of the sum exceeds MB=%d", A->MB);
+        return false;
+    }
+    return true;
+}
+
+// A + beta*I through an identity matrix and add, as the reference does
+// (ellblock/bml_add_ellblock_typed.c:355-368).
+bool eb_add_identity(bml_matrix_ellblock_t *A, double beta, double threshold)
+{
+    if (!A)
+        return false;
+    bml_matrix_ellblock_t *I = eb_alloc_blocks(A->matrix_precision, A->NB, A->MB, A->M, A->bsize,
+                                               A->distribution_mode);
+    if (!I)
+        return false;
+    if (A->matrix_precision == double_real)
+        fill_eb<double>(I, 3);
+    else
+        fill_eb<float>(I, 3);
+    eb_mark_host(I);
+    const bool ok = eb_to_device(I) && eb_add(A, I, 1.0, beta, threshold);
+    eb_free(I);
+    return ok;
+}
+
+bool eb_scale_add_identity(bml_matrix_ellblock_t *A, double alpha, double beta, double threshold)
+{
+    if (!A)
+        return false;
+    float af = (float) alpha;
+    return eb_scale(A->matrix_precision == double_real ? (void *) &alpha : (void *) &af, A, A) &&
+           eb_add_identity(A, beta, threshold);
+}
+
+bml_matrix_ellblock_t *eb_threshold_new(bml_matrix_ellblock_t *A, double threshold)
+{
+    if (!A)
+        return nullptr;
+    bml_matrix_ellblock_t *B = eb_alloc_blocks(A->matrix_precision, A->NB, A->MB, A->M, A->bsize,
+                                               A->distribution_mode);
+    B200Context *c = b200_ctx();
+    if (!B || !c || !eb_to_device(A))
+    {
+        eb_free(B);
+        return nullptr;
+    }
+    const int grid = eb_grid<double>(c, A->NB, 8);
+    if (A->matrix_precision == double_real)
+        eb_threshold_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), view<double>(B), threshold);
+    else
+        eb_threshold_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), view<float>(B), threshold);
+    if (!LAUNCH_OK("eb_threshold_kernel"))
+    {
+        eb_free(B);
+        return nullptr;
+    }
+    eb_mark_device(B);
+    return B;
+}
+
+bool eb_threshold(bml_matrix_ellblock_t *A, double threshold)
+{
+    B200Context *c = b200_ctx();
+    if (!A || !c || !eb_to_device(A))
+        return false;
+    // in place: each block row's surviving blocks move to lower positions only
+    const int grid = eb_grid<double>(c, A->NB, 8);
+    if (A->matrix_precision == double_real)
+        eb_threshold_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), view<double>(A), threshold);
+    else
+        eb_threshold_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), view<float>(A), threshold);
+    if (!LAUNCH_OK("eb_threshold_kernel"))
+        return false;
+    eb_mark_device(A);
+    return true;
+}
+
+static bool eb_sum_to_host(B200Context *c, double *d, int n, double *out2)
+{
+    double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 128);
+    b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(d, nullptr, n, out);
+    if (!LAUNCH_OK("b200_sum_rows_kernel"))
+        return false;
+    double *pin = reinterpret_cast<double *>(static_cast<unsigned char *>(c->pinned) + 4096 + 128);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+        return false;
+    out2[0] = pin[0];
+    return true;
+}
+
+bool eb_trace(bml_matrix_ellblock_t *A, double *trace)
+{
+    B200Context *c = b200_ctx();
+    if (!A || !c || !eb_to_device(A))
+        return false;
+    double *d = static_cast<double *>(b200_scratch((size_t) A->NB * sizeof(double)));
+    if (!d)
+        return false;
+    const int grid = max(1, min(b200_ceil_div(A->NB, 256), c->sm_count * 4));
+    if (A->matrix_precision == double_real)
+        eb_diag_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), d);
+    else
+        eb_diag_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), d);
+    if (!LAUNCH_OK("eb_diag_kernel"))
+        return false;
+    return eb_sum_to_host(c, d, A->NB, trace);
+}
+
+bool eb_trace_mult(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, double *trace)
+{
+    if (!same_partition(A, B, "trace_mult"))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !eb_to_device(A) || !eb_to_device(B))
+        return false;
+    double *d = static_cast<double *>(b200_scratch((size_t) A->NB * sizeof(double)));
+    if (!d)
+        return false;
+    const int grid = eb_grid<double>(c, A->NB, 8);
+    if (A->matrix_precision == double_real)
+        eb_trace_mult_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), view<double>(B), d);
+    else
+        eb_trace_mult_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), view<float>(B), d);
+    if (!LAUNCH_OK("eb_trace_mult_kernel"))
+        return false;
+    return eb_sum_to_host(c, d, A->NB, trace);
+}
+
+bml_matrix_ellblock_t *eb_transpose_new(bml_matrix_ellblock_t *A)
+{
+    B200Context *c = b200_ctx();
+    if (!A || !c || !eb_to_device(A))
+        return nullptr;
+    bml_matrix_ellblock_t *B = eb_alloc_blocks(A->matrix_precision, A->NB, A->MB, A->M, A->bsize,
+                                               A->distribution_mode);
+    int *f = eb_flags(c);
+    if (!B || !f)
+    {
+        eb_free(B);
+        return nullptr;
+    }
+    const int grid = eb_grid<double>(c, A->NB, 8);
+    if (A->matrix_precision == double_real)
+        eb_transpose_kernel<double><<<grid, 128, 0, c->stream>>>(view<double>(A), view<double>(B), f);
+    else
+        eb_transpose_kernel<float><<<grid, 128, 0, c->stream>>>(view<float>(A), view<float>(B), f);
+    int hf = 0;
+    if (!LAUNCH_OK("eb_transpose_kernel") || !eb_read_flags(c, f, &hf, 1))
+    {
+        eb_free(B);
+        return nullptr;
+    }
+    eb_mark_device(B);
+    if (hf)
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "ELLBLOCK transpose: a block column exceeds MB");
+    return B;
+}
+
+bool eb_transpose(bml_matrix_ellblock_t *A)
+{
+    bml_matrix_ellblock_t *B = eb_transpose_new(A);
+    if (!B)
+        return false;
+    const bool ok = eb_copy(B, A);
+    eb_free(B);
+    return ok;
+}
+
+bool eb_gershgorin(bml_matrix_ellblock_t *A, double *bounds)
+{
+    B200Context *c = b200_ctx();
+    if (!A || !c || !eb_to_device(A))
+        return false;
+    double *hi = static_cast<double *>(b200_scratch((size_t) 2 * A->N * sizeof(double)));
+    if (!hi)
+        return false;
+    double *lo = hi + A->N;
+    const int grid = eb_grid<double>(c, A->NB, 8);
+    if (A->matrix_precision == double_real)
+        eb_gersh_kernel<double><<<grid, 64, 0, c->stream>>>(view<double>(A), hi, lo);
+    else
+        eb_gersh_kernel<float><<<grid, 64, 0, c->stream>>>(view<float>(A), hi, lo);
+    double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 192);
+    b200_count_launch();
+    b200_maxmin_rows_kernel<<<1, 1024, 0, c->stream>>>(hi, lo, A->N, DBL_MIN, DBL_MAX, out);
+    if (!LAUNCH_OK("eb gershgorin"))
+        return false;
+    double *pin = reinterpret_cast<double *>(static_cast<unsigned char *>(c->pinned) + 4096 + 192);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+        return false;
+    bounds[0] = pin[1];
+    bounds[1] = pin[0];
+    return true;
+}
+
+bool eb_normalize(bml_matrix_ellblock_t *A, double mineval, double maxeval)
+{
+    const double mm = maxeval - mineval;
+    double sd = -1.0 / mm;
+    float sf = (float) (-1.0 / mm);
+    return A && eb_scale(A->matrix_precision == double_real ? (void *) &sd : (void *) &sf, A, A) &&
+           eb_add_identity(A, maxeval / mm, 0.0);
+}
+
+bml_matrix_ellblock_t *eb_import_dense(bml_matrix_precision_t prec, bml_dense_order_t order, int N, int M,
+                                       void *D, double threshold, bml_distribution_mode_t mode)
+{
+    bml_matrix_ellblock_t *A = eb_constructor(0, prec, N, M, mode);
+    B200Context *c = b200_ctx();
+    if (!A || !c)
+        return A;
+    if (A->N != N)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK import: block sizes sum to %d, N=%d", A->N, N);
+        eb_free(A);
+        return nullptr;
+    }
+    const size_t sz = prec_size(prec);
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch((size_t) N * N * sz));
+    int *f = eb_flags(c);
+    if (!scr || !f || !CUDA_OK(cudaMemcpyAsync(scr, D, (size_t) N * N * sz, cudaMemcpyHostToDevice, c->stream)))
+    {
+        eb_free(A);
+        return nullptr;
+    }
+    const int grid = eb_grid<double>(c, A->NB, 8);
+    const int colmajor = order == dense_column_major;
+    if (prec == double_real)
+        eb_import_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), reinterpret_cast<double *>(scr), N,
+                                                              colmajor, threshold, f);
+    else
+        eb_import_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), reinterpret_cast<float *>(scr), N,
+                                                             colmajor, threshold, f);
+    int hf = 0;
+    if (!LAUNCH_OK("eb_import_kernel") || !eb_read_flags(c, f, &hf, 1))
+    {
+        eb_free(A);
+        return nullptr;
+    }
+    eb_mark_device(A);
+    if (hf)
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "ELLBLOCK import: more than MB blocks above threshold in a row");
+    return A;
+}
+
+void *eb_export_dense(bml_matrix_ellblock_t *A, bml_dense_order_t order)
+{
+    B200Context *c = b200_ctx();
+    if (!A || !c || !eb_to_device(A))
+        return nullptr;
+    const size_t sz = prec_size(A->matrix_precision);
+    const size_t bytes = (size_t) A->N * A->N * sz;
+    void *D = calloc((size_t) A->N * A->N, sz);
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(bytes));
+    if (!D || !scr || !CUDA_OK(cudaMemsetAsync(scr, 0, bytes, c->stream)))
+    {
+        free(D);
+        return nullptr;
+    }
+    const int grid = eb_grid<double>(c, A->NB, 8);
+    const int colmajor = order == dense_column_major;
+    if (A->matrix_precision == double_real)
+        eb_export_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), reinterpret_cast<double *>(scr), A->N,
+                                                              colmajor);
+    else
+        eb_export_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), reinterpret_cast<float *>(scr), A->N,
+                                                             colmajor);
+    if (!LAUNCH_OK("eb_export_kernel") ||
+        !CUDA_OK(cudaMemcpyAsync(D, scr, bytes, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+    {
+        free(D);
+        return nullptr;
+    }
+    return D;
+}
+
+bool eb_multiply_x2(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, double threshold, double *trace)
+{
+    if (!same_partition(X, X2, "multiply_x2") || X == X2)
+        return false;
+    if (!eb_to_device(X) || !eb_to_device(X2))
+        return false;
+    if (X2->mirror == MIRROR_HOST_NEWER)
+        X2->mirror = MIRROR_SYNCED;
+    double tr[2] = {0, 0};
+    const bool ok = X->matrix_precision == double_real
+                        ? eb_multiply_typed<double>(X, X, X2, threshold, true, tr)
+                        : eb_multiply_typed<float>(X, X, X2, threshold, true, tr);
+    if (trace)
+    {
+        trace[0] = tr[0];
+        trace[1] = tr[1];
+    }
+    return ok;
+}
+
+bool eb_multiply_AB(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_matrix_ellblock_t *C, double threshold)
+{
+    if (!same_partition(A, B, "multiply_AB") || !same_partition(A, C, "multiply_AB") || C == A || C == B)
+        return false;
+    if (!eb_to_device(A) || !eb_to_device(B) || !eb_to_device(C))
+        return false;
+    return A->matrix_precision == double_real ? eb_multiply_typed<double>(A, B, C, threshold, false, nullptr)
+                                              : eb_multiply_typed<float>(A, B, C, threshold, false, nullptr);
+}
+
+// C <- alpha*A*B + beta*C (ellblock/bml_multiply_ellblock_typed.c:183-231)
+bool eb_multiply(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_matrix_ellblock_t *C, double alpha,
+                 double beta, double threshold)
+{
+    if (A == B && alpha == 1.0 && beta == 0.0)
+        return eb_multiply_x2(A, C, threshold, nullptr);
+    bml_matrix_ellblock_t *T0 = eb_alloc_blocks(C->matrix_precision, C->NB, C->MB, C->M, C->bsize,
+                                                C->distribution_mode);
+    if (!T0)
+        return false;
+    bool ok = A == B ? eb_multiply_x2(A, T0, threshold, nullptr) : eb_multiply_AB(A, B, T0, threshold);
+    if (ok)
+        ok = eb_add(C, T0, beta, alpha, threshold);
+    eb_free(T0);
+    return ok;
+}

@@ -64,6 +64,17 @@ struct MulArgs
 };
 
 // Tiers: A (warp, 1024 slots), B1 (2048), B2 (4096), B3 (8192), C (dense).
+// B200_X2_TIERS: bit t set = tier t in use (rows skip unused tiers);
+// B200_C_BLOCKS: blocks per SM of the dense tier.
+// Measured on B200 (SP2 on the 40^3 lattice): past ~1280 distinct columns a
+// row runs faster in the dense tier at full occupancy than in the 4096- and
+// 8192-slot shared-memory tables, so those two tiers are off by default.
+#ifndef B200_X2_TIERS
+#define B200_X2_TIERS 0x13
+#endif
+#ifndef B200_C_BLOCKS
+#define B200_C_BLOCKS 8
+#endif
 constexpr int NTIERS = 5;
 __constant__ int TIER_CAP[NTIERS] = {640, 1280, 2560, 5120, 0x7fffffff};
 
@@ -128,7 +139,7 @@ __global__ void plan_kernel(MulArgs g, int ncols, int skip_mid, TierLists *tl, i
                     est = h;
             }
             int t = 0;
-            while (t < NTIERS - 1 && est > TIER_CAP[t])
+            while (t < NTIERS - 1 && (est > TIER_CAP[t] || !((B200_X2_TIERS >> t) & 1)))
                 ++t;
             if (skip_mid && t > 0)
                 t = NTIERS - 1;
@@ -443,7 +454,7 @@ template <typename T, int W, int LOGTS, int STAGES, int CHUNK> struct TeamCfg
 
 template <typename T, int W, int LOGTS, int STAGES, int CHUNK, int MINB>
 __global__ void __launch_bounds__(W * 32, MINB) team_kernel(MulArgs g, const int *rows, TierLists *tl,
-                                                           int tier, int *next_rows)
+                                                           int tier, int next_tier, int *next_rows)
 {
     using Cfg = TeamCfg<T, W, LOGTS, STAGES, CHUNK>;
     constexpr int TS = Cfg::TS, NT = Cfg::NT, SPW = Cfg::SPW;
@@ -626,7 +637,7 @@ __global__ void __launch_bounds__(W * 32, MINB) team_kernel(MulArgs g, const int
         if (aborted)
         {
             if (tid == 0)
-                next_rows[atomicAdd(&tl->count[tier + 1], 1)] = i;
+                next_rows[atomicAdd(&tl->count[next_tier], 1)] = i;
             continue;
         }
 
@@ -686,7 +697,7 @@ __global__ void __launch_bounds__(W * 32, MINB) team_kernel(MulArgs g, const int
 constexpr int C_W = 8;
 
 template <typename T>
-__global__ void __launch_bounds__(256, 4) dense_tier_kernel(MulArgs g, int smax, int ncols,
+__global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs g, int smax, int ncols,
                                                         const int *rows, TierLists *tl,
                                                         unsigned char *slabs)
 {
@@ -857,7 +868,7 @@ __global__ void __launch_bounds__(256, 4) dense_tier_kernel(MulArgs g, int smax,
 
 template <typename T, int W, int LOGTS, int STAGES, int CHUNK, int MINB>
 bool launch_team(B200Context *c, const MulArgs &g, const int *rows, TierLists *tl, int tier,
-                 int *next_rows)
+                 int next_tier, int *next_rows)
 {
     using Cfg = TeamCfg<T, W, LOGTS, STAGES, CHUNK>;
     auto k = team_kernel<T, W, LOGTS, STAGES, CHUNK, MINB>;
@@ -866,11 +877,11 @@ bool launch_team(B200Context *c, const MulArgs &g, const int *rows, TierLists *t
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, W * 32, Cfg::bytes);
     const int grid = c->sm_count * (occ > 0 ? occ : 1);
-    k<<<grid, W * 32, Cfg::bytes, c->stream>>>(g, rows, tl, tier, next_rows);
+    k<<<grid, W * 32, Cfg::bytes, c->stream>>>(g, rows, tl, tier, next_tier, next_rows);
     return LAUNCH_OK("team_kernel");
 }
 
-constexpr int C_BLOCKS_PER_SM = 4;
+constexpr int C_BLOCKS_PER_SM = B200_C_BLOCKS;
 
 // Distinct-column counts of the last multiply, reused as the next call's
 // tier estimate when the row count matches (SP2 multiplies the same-size
@@ -961,14 +972,32 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
         return false;
     int occA = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occA, tierA_kernel<T>, 32 * A_WARPS, smemA);
+    int nextA = 1;
+    while (nextA < NTIERS - 1 && !((B200_X2_TIERS >> nextA) & 1))
+        ++nextA;
     tierA_kernel<T><<<c->sm_count * max(occA, 1), 32 * A_WARPS, smemA, c->stream>>>(
-        g, list(0), tl, 1, list(1));
+        g, list(0), tl, nextA, list(nextA));
     if (!LAUNCH_OK("tierA_kernel"))
         return false;
-    if (!launch_team<T, B1_CFG>(c, g, list(1), tl, 1, list(2)) ||
-        !launch_team<T, B2_CFG>(c, g, list(2), tl, 2, list(3)) ||
-        !launch_team<T, B3_CFG>(c, g, list(3), tl, 3, list(4)))
-        return false;
+    // Rows a tier cannot hold go to the next tier in use (the dense tier
+    // always is); tiers switched off are not launched.
+    {
+        auto next_on = [](int t) {
+            int n = t + 1;
+            while (n < NTIERS - 1 && !((B200_X2_TIERS >> n) & 1))
+                ++n;
+            return n;
+        };
+        if ((B200_X2_TIERS >> 1) & 1)
+            if (!launch_team<T, B1_CFG>(c, g, list(1), tl, 1, next_on(1), list(next_on(1))))
+                return false;
+        if ((B200_X2_TIERS >> 2) & 1)
+            if (!launch_team<T, B2_CFG>(c, g, list(2), tl, 2, next_on(2), list(next_on(2))))
+                return false;
+        if ((B200_X2_TIERS >> 3) & 1)
+            if (!launch_team<T, B3_CFG>(c, g, list(3), tl, 3, next_on(3), list(next_on(3))))
+                return false;
+    }
     if (!CUDA_OK(cudaFuncSetAttribute(dense_tier_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
         return false;

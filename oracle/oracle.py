@@ -229,3 +229,39 @@ def same_rows_exact(a, b, Ma, Mb):
         if not np.array_equal(va[i * Ma:i * Ma + n].view(np.uint8), vb[i * Mb:i * Mb + n].view(np.uint8)):
             return False
     return True
+
+
+def rest_ellblock_x2(bsize, indexb, nnzb, MB, dense, thr, MB2, trace_quirk=0):
+    """ELLBLOCK X^2 by the restatement; blocks of `dense` at the positions the
+    block lists name.  Returns (dense X^2, traces, widest block row)."""
+    lib = rest()
+    bsize = np.asarray(bsize, np.int32)
+    NB = len(bsize)
+    off = np.concatenate([[0], np.cumsum(bsize)])
+    maxbs = int(bsize.max())
+    pool = np.zeros((NB * MB, maxbs * maxbs))
+    for ib in range(NB):
+        for jp in range(int(nnzb[ib])):
+            jb = int(indexb[ib * MB + jp])
+            blk = dense[off[ib]:off[ib + 1], off[jb]:off[jb + 1]]
+            pool[ib * MB + jp, :blk.size] = blk.reshape(-1)
+    out = np.zeros((NB * MB2, maxbs * maxbs))
+    ptrs = (C.POINTER(C.c_double) * (NB * MB))(*[pool[q].ctypes.data_as(C.POINTER(C.c_double)) for q in range(NB * MB)])
+    optrs = (C.POINTER(C.c_double) * (NB * MB2))(*[out[q].ctypes.data_as(C.POINTER(C.c_double)) for q in range(NB * MB2)])
+    oix = np.zeros(NB * MB2, np.int32)
+    onz = np.zeros(NB, np.int32)
+    tr = np.zeros(2)
+    ib_ = np.ascontiguousarray(indexb, np.int32)
+    nb_ = np.ascontiguousarray(nnzb, np.int32)
+    lib.oracle_ellblock_x2_d.restype = C.c_int
+    w = lib.oracle_ellblock_x2_d(NB, MB, _p(bsize, C.c_int), ptrs, _p(ib_, C.c_int), _p(nb_, C.c_int),
+                                 C.c_double(thr), MB2, optrs, _p(oix, C.c_int), _p(onz, C.c_int),
+                                 _p(tr, C.c_double), trace_quirk)
+    N = int(off[-1])
+    d2 = np.zeros((N, N))
+    for ib in range(NB):
+        for jp in range(int(onz[ib])):
+            jb = int(oix[ib * MB2 + jp])
+            r, c = bsize[ib], bsize[jb]
+            d2[off[ib]:off[ib + 1], off[jb]:off[jb + 1]] = out[ib * MB2 + jp, :r * c].reshape(r, c)
+    return d2, tr, w

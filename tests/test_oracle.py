@@ -1,0 +1,102 @@
+"""The CPU oracle is pinned before it is trusted: the C restatement
+(oracle/bml_oracle.c) must reproduce, bit for bit, the golden fixtures made
+from the reference library (tests/golden/make_golden.py) and, where the
+reference library is built here (oracle/_ref/libbml_ref.so), the reference
+itself on further inputs.  CPU only."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import bml_b200 as B
+from oracle import oracle as O
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def gold(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def test_generators_match_digests():
+    dig = json.load(open(os.path.join(GOLD, "generators.json")))
+    for name, args in (("chain_4096_128", lambda: B.gen_chain(4096, 128, 0)),
+                       ("lattice_40_r3_256", lambda: B.gen_lattice(40, 3, 64000, 256, 0))):
+        h = hashlib.sha256()
+        for a in args():
+            h.update(np.ascontiguousarray(a).tobytes())
+        assert h.hexdigest() == dig[name], name
+
+
+def test_restatement_x2_matches_golden_chain():
+    g = gold("x2_chain.npz")
+    N, M, M2 = 256, 64, int(g["M2"])
+    v, ix, nz = B.gen_chain(N, M, 0)
+    (ov, oix, onz), tr, _ = O.rest_x2(v, ix, nz, N, M, 1e-5, M2)
+    assert O.same_rows_exact((ov, oix, onz), (g["value"], g["index"], g["nnz"]), M2, M2)
+    assert np.array_equal(tr, g["trace"])  # single-threaded reference sums in row order
+
+
+def test_restatement_x2_matches_reference_test_matrix():
+    g = gold("x2_random.npz")
+    (ov, oix, onz), tr, _ = O.rest_x2(g["value"], g["index"], g["nnz"], 13, 13, 0.0, 13)
+    assert O.same_rows_exact((ov, oix, onz), (g["value2"], g["index2"], g["nnz2"]), 13, 13)
+    # the reference test's own check: X^2 equals the dense product to 1e-12
+    d = np.zeros((13, 13))
+    for i in range(13):
+        for p in range(g["nnz"][i]):
+            d[i, g["index"][i * 13 + p]] = g["value"][i * 13 + p]
+    d2 = np.zeros((13, 13))
+    for i in range(13):
+        for p in range(onz[i]):
+            d2[i, oix[i * 13 + p]] = ov[i * 13 + p]
+    assert np.abs(d2 - d @ d).max() < 1e-12
+
+
+def test_restatement_sp2_matches_golden():
+    g = gold("sp2_chain.npz")
+    N, M = 256, int(g["M"])
+    v, ix, nz = B.gen_chain(N, 64, 0)
+    pad = lambda a: np.pad(a.reshape(N, 64), ((0, 0), (0, M - 64))).reshape(-1)
+    (dv, dix, dnz), info = O.rest_sp2(pad(v), pad(ix), nz, N, M, 1e-5, N / 2.0, 12, 0.0, 0)
+    assert info[0] == 12
+    assert O.same_rows_exact((dv, dix, dnz), (g["value"], g["index"], g["nnz"]), M, M)
+
+
+def test_restatement_ellblock_matches_golden():
+    g = gold("ellblock_x2.npz")
+    d2, tr, _ = O.rest_ellblock_x2(g["bsize"], g["indexb"], g["nnzb"], int(g["MB"]), g["dense"], 0.0,
+                                   int(g["MB"]), trace_quirk=1)
+    assert np.array_equal(d2, g["dense2"])
+    assert tr[0] == g["trace"][0] and tr[1] == g["trace"][1]
+    # the true trace of X^2 (what libbml_b200 returns) differs where block sizes vary
+    _, tr_true, _ = O.rest_ellblock_x2(g["bsize"], g["indexb"], g["nnzb"], int(g["MB"]), g["dense"], 0.0,
+                                       int(g["MB"]), trace_quirk=0)
+    assert tr_true[1] == pytest.approx(np.trace(g["dense2"]), rel=1e-12)
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not os.path.exists(O.REF_PATH):
+        pytest.skip("reference library not built (needs the reference sources)")
+    return O
+
+
+@pytest.mark.parametrize("thr", [0.0, 1e-5, 1e-2])
+@pytest.mark.parametrize("prec", [O.DOUBLE, O.SINGLE])
+def test_restatement_x2_matches_reference(ref, thr, prec):
+    # (M2 = N: a row wider than M2 makes the reference exit the process,
+    # bml_multiply_ellpack_typed.c:325-330 and bml_logger.c:111-115)
+    for (v, ix, nz), N, M in ((B.gen_lattice(9, 3, 729, 128, 1), 729, 128), (B.gen_chain(500, 40, 2), 500, 40)):
+        M2 = N
+        A = ref.ref_ellpack(v, ix, nz, N, M, prec)
+        R2 = ref.ref().bml_zero_matrix(2, prec, N, M2, 0)
+        tr = ref.ref_x2(A, R2, thr)
+        r = ref.ref_ellpack_arrays(R2)
+        o, otr, _ = ref.rest_x2(v, ix, nz, N, M, thr, M2, prec)
+        assert ref.same_rows_exact(r, o, M2, M2)
+        assert otr[1] == pytest.approx(tr[1], rel=1e-5 if prec == O.SINGLE else 1e-12)
+        ref.ref_free(A)
+        ref.ref_free(R2)
