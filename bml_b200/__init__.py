@@ -115,6 +115,7 @@ _PROTOS = {
     "bml_b200_launch_count": (C.c_ulonglong, []),
     "bml_b200_event_record": (_i, [_i]),
     "bml_b200_event_elapsed": (_i, [_i, _i, C.POINTER(C.c_float)]),
+    "bml_b200_ellpack_trace_noalloc": (_i, [_vp, _ip, _ip, _i, _i, _i, _dp, _vp]),
 }
 
 for _name, (_res, _args) in _PROTOS.items():

@@ -296,6 +296,27 @@ BML_B200_API int bml_b200_event_elapsed(int a, int b, float *ms);
 /* Device properties this library uses: SM count, device ordinal. */
 BML_B200_API int bml_b200_device_info(int *sm_count, int *device);
 
+/* Trace of an ELLPACK matrix without allocating memory.  No counterpart in
+ * the reference: for callers that may not have the library allocate -- an
+ * application that owns all device memory through its own fixed pool, or a
+ * latency-critical loop where cudaMalloc/cudaFree (which synchronise the
+ * device) are not acceptable.  Inputs are the matrix's device arrays (as
+ * bml_b200_ellpack_device_arrays returns them, or the caller's own):
+ * row-major value[N*ld] of the given precision (single_real or double_real),
+ * index[N*ld], nnz[N]; the trace is written to *d_trace, one double in device
+ * memory owned by the caller; the kernels run on `stream` (NULL: the default
+ * stream) and the call returns without waiting for them.  Scratch is a fixed
+ * array of 2^19 doubles (4 MiB) compiled into the library, held on every GPU
+ * that loads it until the process exits: N above 2^19 is rejected with
+ * BML_B200_ERR_INVALID.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress, with the device current); make that
+ * first call before any stream capture.  All calls share the array and it
+ * keeps the last call's contents, so calls that overlap on the GPU race on
+ * it; calls on one stream are safe.  No cudaMalloc, cudaFree or allocating
+ * library routine is called. */
+BML_B200_API int bml_b200_ellpack_trace_noalloc(const void *d_value, const int *d_index,
+    const int *d_nnz, int N, int ld, int precision, double *d_trace, void *stream);
+
 /* SP2 density-matrix purification (Niklasson, PRB 66, 155115 (2002)), the
  * consumer loop around bml_multiply_x2 that PROGRESS/LATTE write on top of bml:
  *   X0 = (emax I - H)/(emax - emin) with Gershgorin bounds of H;
