@@ -111,6 +111,7 @@ _PROTOS = {
     "bml_b200_gen_lattice": (_i, [_i, _i, _i, _i, C.c_ulonglong, _dp, _ip, _ip]),
     "bml_b200_reset_block_sizes": (None, []),
     "bml_b200_last_tier_counts": (_i, [_ip, _i]),
+    "bml_b200_set_x2_tiers": (_i, [_i]),
     "bml_b200_set_device": (_i, [_i]),
     "bml_b200_launch_count": (C.c_ulonglong, []),
     "bml_b200_event_record": (_i, [_i]),
@@ -241,10 +242,23 @@ def multiply_x2(X, X2, threshold):
     return st, (tr[0], tr[1])
 
 
+# Multiply tiers in the order of bml_b200_last_tier_counts.
+X2_TIERS = ("A", "W8", "B1", "W16", "K4", "K8", "C")
+
+
 def last_tier_counts():
     out = (C.c_int * 8)()
     n = lib.bml_b200_last_tier_counts(out, 8)
     return list(out[:n])
+
+
+def set_x2_tiers(*names):
+    """Restrict later multiplies to the named tiers (C is always on); no
+    names restores the default.  Returns the previous mask."""
+    mask = 0
+    for n in names:
+        mask |= 1 << X2_TIERS.index(n)
+    return lib.bml_b200_set_x2_tiers(mask)
 
 
 def event_ms(a, b):

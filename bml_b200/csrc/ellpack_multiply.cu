@@ -23,11 +23,17 @@
 //
 // Tiers, chosen per row by a planning kernel from a bound or an estimate of
 // the row's distinct columns (the previous call's counts, when the matrix
-// size matches), each handing rows that outgrow it to the next:
+// size matches), each handing rows that outgrow it to the next tier in use:
 //   A   1 warp per row, 1024-slot hash, direct loads (4 rows per block);
-//   B1  4 warps, 2048-slot hash, TMA staging;
-//   B2  4 warps, 4096-slot hash, TMA staging;
-//   B3  16 warps, 8192-slot hash, TMA staging;
+//   W8  8 warps per row, each owning 4 of the 32 column classes k % 32,
+//       256-slot private hash per warp, no barrier between jps;
+//   B1  4 warps sharing a 2048-slot hash, rows of B staged by TMA;
+//   W16 16 warps (2 classes each), 256 slots per warp;
+//   K4  8 warps, two passes: a bitmap of the row's column window ranks the
+//       columns into a compact accumulator of up to 4096 entries;
+//   K8  as K4 with up to 8192 entries in shared memory, more in a compact
+//       per-block slab in device memory (any width up to a 65536-column
+//       window and 2048 kept columns);
 //   C   8 warps, dense accumulator over all columns in global memory (the
 //       reference's own x[N]/ix[N]/jx[N] scheme; any width).
 // All tiers are persistent grids pulling rows from device-side lists, so a
@@ -63,20 +69,25 @@ struct MulArgs
     int *hint_out;    // distinct-column counts of this call
 };
 
-// Tiers: A (warp, 1024 slots), B1 (2048), B2 (4096), B3 (8192), C (dense).
-// B200_X2_TIERS: bit t set = tier t in use (rows skip unused tiers);
-// B200_C_BLOCKS: blocks per SM of the dense tier.
-// Measured on B200 (SP2 on the 40^3 lattice): past ~1280 distinct columns a
-// row runs faster in the dense tier at full occupancy than in the 4096- and
-// 8192-slot shared-memory tables, so those two tiers are off by default.
+// Tiers in routing order: A, W8, B1, W16, K4, K8, C (dense).
+// B200_X2_TIERS: bit t set = tier t in use (rows skip unused tiers; the dense
+// tier is always in use); B200_C_BLOCKS: blocks per SM of the dense tier.
+// Measured on B200 over 4 FP64 SP2 iterations on the 40^3 lattice (N=64000,
+// radius 3): A + B1 + C 776 ms, A + K8 791 ms, A + B1 + K4 + K8 927 ms,
+// A + W8 + W16 + K4 + K8 994 ms.  The rows there reach 8000+ distinct
+// columns before thresholding, where the dense tier's device-memory
+// accumulator still wins; the other tiers stay selectable at run time.
 #ifndef B200_X2_TIERS
-#define B200_X2_TIERS 0x13
+#define B200_X2_TIERS 0x05
 #endif
 #ifndef B200_C_BLOCKS
 #define B200_C_BLOCKS 8
 #endif
-constexpr int NTIERS = 5;
-__constant__ int TIER_CAP[NTIERS] = {640, 1280, 2560, 5120, 0x7fffffff};
+constexpr int NTIERS = 7;
+constexpr int TIER_W8 = 1, TIER_B1 = 2, TIER_W16 = 3, TIER_K4 = 4, TIER_K8 = 5, TIER_C = NTIERS - 1;
+constexpr int BUCKET_TIERS_MASK = (1 << TIER_W8) | (1 << TIER_W16) | (1 << TIER_K4) | (1 << TIER_K8);
+constexpr int WINDOW_TIERS_MASK = (1 << TIER_K4) | (1 << TIER_K8);
+__constant__ int TIER_CAP[NTIERS] = {640, 1100, 1280, 2200, 4096, 0x7fffffff, 0x7fffffff};
 
 struct TierLists
 {
@@ -95,7 +106,7 @@ struct TeamMisc
 // Planning: product-count bound per row, input validation, tier choice.
 // One warp per row.
 // -------------------------------------------------------------------------
-__global__ void plan_kernel(MulArgs g, int ncols, int skip_mid, TierLists *tl, int *lists)
+__global__ void plan_kernel(MulArgs g, int ncols, int tmask, TierLists *tl, int *lists)
 {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -134,15 +145,13 @@ __global__ void plan_kernel(MulArgs g, int ncols, int skip_mid, TierLists *tl, i
             long long est = P < ncols ? P : ncols;
             if (g.hint)
             {
-                const long long h = (long long) g.hint[i] + g.hint[i] / 4 + 16;
+                const long long h = 2 * (long long) g.hint[i] + 16;
                 if (h < est)
                     est = h;
             }
             int t = 0;
-            while (t < NTIERS - 1 && (est > TIER_CAP[t] || !((B200_X2_TIERS >> t) & 1)))
+            while (t < NTIERS - 1 && (est > TIER_CAP[t] || !((tmask >> t) & 1)))
                 ++t;
-            if (skip_mid && t > 0)
-                t = NTIERS - 1;
             lists[(size_t) t * g.NA + atomicAdd(&tl->count[t], 1)] = i;
         }
     }
@@ -689,6 +698,965 @@ __global__ void __launch_bounds__(W * 32, MINB) team_kernel(MulArgs g, const int
 }
 
 // -------------------------------------------------------------------------
+// Wide tiers W8, W16: a team of W warps per row (one team per
+// block).  Columns fall in 32 classes, k % 32, and warp w owns the classes
+// [w*32/W, (w+1)*32/W).  Each warp keeps a private hash of its own columns and
+// walks every jp of the row in order over its share of row j of B, so each
+// x[k] is summed by one warp in the reference order and the warps never wait
+// for one another inside a row.
+// B's rows are first regrouped by class into a bucketed copy (stable, so each
+// bucket keeps the row's order, with every entry's original position): a
+// warp's share of row j is one contiguous range, read with coalesced loads,
+// PF jps ahead of the one it is summing.
+// A warp's inserts carry the key (jp << 16 | original position); sorted by
+// that key (already sorted when a warp owns one class) a list is the
+// reference's first-touch order restricted to the warp's columns, and a kept
+// entry's output slot is the number of kept entries with a smaller key in all
+// W lists.
+// Shared memory per warp: vals[TS] | keys[TS] | okey[LP] (u32) |
+//                         oslot[LP] (u16) | kcnt[CAP+1] (u16, kept prefix)
+// -------------------------------------------------------------------------
+constexpr int NCLS = 32; // column classes
+constexpr int PF = 4;    // jps of prefetch
+
+struct BucketArgs
+{
+    void *v;           // values [NB][ldb], matrix precision
+    int *c;            // columns [NB][ldb]
+    unsigned short *p; // original position of each entry within its row [NB][ldb]
+    int *off;          // [NB][NCLS + 1]: start of bucket b; off[NCLS] = row length
+    int *cmin, *cmax;  // [NB]: smallest / largest column of each row (empty: INT_MAX / -1)
+};
+
+// Stable regrouping of every row of B by column class.  One warp per row;
+// eight warps per block.
+template <typename T>
+__global__ void __launch_bounds__(256) bucket_kernel(const T *__restrict__ Bv, const int *__restrict__ Bi,
+                                                     const int *__restrict__ Bn, int ldb, int NB,
+                                                     BucketArgs ba)
+{
+    __shared__ int run_s[8][NCLS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int *run = run_s[wib];
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    T *Pv = static_cast<T *>(ba.v);
+    for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < NB; j += warps)
+    {
+        int nj = Bn[j];
+        if (nj < 0 || nj > ldb) // rejected by the plan; keep the copy in bounds
+            nj = 0;
+        const size_t rb = (size_t) j * ldb;
+        run[lane] = 0;
+        __syncwarp();
+        for (int c0 = 0; c0 < nj; c0 += 32)
+        {
+            const int q = c0 + lane;
+            const int b = q < nj ? (Bi[rb + q] & (NCLS - 1)) : -1;
+            const unsigned same = __match_any_sync(FULL, b);
+            if (b >= 0 && (same & lanemask_lt()) == 0)
+                run[b] += __popc(same);
+            __syncwarp();
+        }
+        const int cnt = run[lane];
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        int *off = ba.off + (size_t) j * (NCLS + 1);
+        off[lane] = incl - cnt;
+        if (lane == 31)
+            off[NCLS] = incl;
+        int mn = 0x7fffffff, mx = -1;
+        for (int q = lane; q < nj; q += 32)
+        {
+            const int k = Bi[rb + q];
+            mn = min(mn, k);
+            mx = max(mx, k);
+        }
+        mn = __reduce_min_sync(FULL, mn);
+        mx = __reduce_max_sync(FULL, mx);
+        if (lane == 0)
+        {
+            ba.cmin[j] = mn;
+            ba.cmax[j] = mx;
+        }
+        __syncwarp();
+        run[lane] = incl - cnt;
+        __syncwarp();
+        for (int c0 = 0; c0 < nj; c0 += 32)
+        {
+            const int q = c0 + lane;
+            int k = 0, b = -1;
+            T v = T(0);
+            if (q < nj)
+            {
+                k = Bi[rb + q];
+                v = Bv[rb + q];
+                b = k & (NCLS - 1);
+            }
+            const unsigned same = __match_any_sync(FULL, b);
+            if (b >= 0)
+            {
+                const size_t dst = rb + run[b] + __popc(same & lanemask_lt());
+                Pv[dst] = v;
+                ba.c[dst] = k;
+                ba.p[dst] = (unsigned short) q;
+            }
+            __syncwarp();
+            if (b >= 0 && (same & lanemask_lt()) == 0)
+                run[b] += __popc(same);
+            __syncwarp();
+        }
+    }
+}
+
+struct WideMisc
+{
+    double diag;
+    int row;
+    int abort;
+    int dw[32];   // list length per warp
+    int kept[32]; // kept entries per warp
+};
+
+constexpr int pow2_ceil(int x)
+{
+    int p = 1;
+    while (p < x)
+        p <<= 1;
+    return p;
+}
+
+constexpr int ilog2(int x)
+{
+    int l = 0;
+    while ((1 << (l + 1)) <= x)
+        ++l;
+    return l;
+}
+
+template <typename T, int W, int TS> struct WideCfg
+{
+    static constexpr int R = NCLS / W;        // buckets per warp
+    static constexpr int CAP = TS * 11 / 16;  // distinct columns per warp before handing on
+    static constexpr int LP = R > 1 ? pow2_ceil(CAP) : CAP; // list length (sort padding)
+    static constexpr size_t off_keys = size_t(TS) * sizeof(T);
+    static constexpr size_t off_okey = off_keys + size_t(TS) * sizeof(int);
+    static constexpr size_t off_oslot = off_okey + size_t(LP) * sizeof(unsigned);
+    static constexpr size_t off_kcnt = off_oslot + size_t(LP) * sizeof(unsigned short);
+    static constexpr size_t warp_bytes =
+        (off_kcnt + size_t(CAP + 1) * sizeof(unsigned short) + 15) / 16 * 16;
+    static constexpr size_t off_misc = W * warp_bytes;
+    static constexpr size_t bytes = off_misc + sizeof(WideMisc);
+};
+
+// Open-addressing slot of column k in a table of TS slots (any TS): the
+// column rotated right by 5 (class bits on top), Fibonacci-hashed, scaled.
+template <int TS> __device__ __forceinline__ unsigned wide_hash(int k)
+{
+    const unsigned x = (((unsigned) k >> 5) | ((unsigned) k << 27)) * 2654435761u;
+    if ((TS & (TS - 1)) == 0)
+        return x >> (32 - ilog2(TS));
+    return __umulhi(x, (unsigned) TS);
+}
+
+template <int TS>
+__device__ __forceinline__ int wide_probe(int *keys, int k, bool &inserted)
+{
+    unsigned h = wide_hash<TS>(k);
+    volatile int *vk = keys;
+#pragma unroll 1
+    for (int p = 0; p < TS; ++p)
+    {
+        const int cur = vk[h];
+        if (cur == k)
+        {
+            inserted = false;
+            return (int) h;
+        }
+        if (cur == B200_EMPTY_KEY)
+        {
+            const int old = atomicCAS(&keys[h], B200_EMPTY_KEY, k);
+            if (old == B200_EMPTY_KEY)
+            {
+                inserted = true;
+                return (int) h;
+            }
+            if (old == k)
+            {
+                inserted = false;
+                return (int) h;
+            }
+        }
+        h = (h + 1 == TS) ? 0 : h + 1;
+    }
+    inserted = false;
+    return -1;
+}
+
+// Row meta of one block of 32 jps, one jp per lane: A's value, the B row, and
+// the warp's bucket range in that row.
+template <typename T> struct JpMeta
+{
+    T a;
+    int j, lo, hi;
+};
+
+template <typename T, int W, int TS, int MINB>
+__global__ void __launch_bounds__(W * 32, MINB)
+    wide_kernel(MulArgs g, BucketArgs ba, const int *rows, TierLists *tl, int tier, int next_tier,
+                int *next_rows)
+{
+    using Cfg = WideCfg<T, W, TS>;
+    constexpr int R = Cfg::R, CAP = Cfg::CAP, LP = Cfg::LP;
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (g.flags->bad_input)
+        return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char *mine = smem + (size_t) warp * Cfg::warp_bytes;
+    T *vals = reinterpret_cast<T *>(mine);
+    int *keys = reinterpret_cast<int *>(mine + Cfg::off_keys);
+    unsigned *okey = reinterpret_cast<unsigned *>(mine + Cfg::off_okey);
+    unsigned short *oslot = reinterpret_cast<unsigned short *>(mine + Cfg::off_oslot);
+    unsigned short *kcnt = reinterpret_cast<unsigned short *>(mine + Cfg::off_kcnt);
+    WideMisc *misc = reinterpret_cast<WideMisc *>(smem + Cfg::off_misc);
+    volatile int *vabort = &misc->abort;
+
+    const int nrows = tl->count[tier];
+    const T *Av = static_cast<const T *>(g.Av);
+    const T *Pv = static_cast<const T *>(ba.v);
+    const int *Pc = ba.c;
+    const unsigned short *Pp = ba.p;
+    T *Cv = static_cast<T *>(g.Cv);
+    const T thr = (T) g.thr;
+    const int blo = warp * R; // this warp's buckets: [blo, blo + R)
+
+    for (;;)
+    {
+        __syncthreads(); // every warp is done with the previous row's lists
+        if (tid == 0)
+        {
+            misc->row = atomicAdd(&tl->cursor[tier], 1);
+            misc->abort = 0;
+            misc->diag = 0.0;
+        }
+        __syncthreads();
+        const int pos = misc->row;
+        if (pos >= nrows)
+            break;
+        const int i = rows[pos];
+        for (int s = lane; s < TS; s += 32)
+        {
+            keys[s] = B200_EMPTY_KEY;
+            vals[s] = T(0);
+        }
+        __syncwarp();
+        const int ni = g.An[i];
+        const T *arow = Av + (size_t) i * g.lda;
+        const int *airow = g.Ai + (size_t) i * g.lda;
+
+        // meta of jp block b into m (lanes past the row hold an empty range)
+        auto load_aj = [&](int b, JpMeta<T> &m) {
+            const int q = b * 32 + lane;
+            m.a = T(0);
+            m.j = 0;
+            m.lo = m.hi = 0;
+            if (q < ni)
+            {
+                m.a = arow[q];
+                m.j = airow[q];
+            }
+        };
+        auto load_off = [&](int b, JpMeta<T> &m) {
+            if (b * 32 + lane < ni)
+            {
+                const int *o = ba.off + (size_t) m.j * (NCLS + 1) + blo;
+                m.lo = o[0];
+                m.hi = o[R];
+            }
+        };
+        JpMeta<T> m0, m1; // blocks cb and cb + 1
+        int cb = 0;
+        load_aj(0, m0);
+        load_aj(1, m1);
+        load_off(0, m0);
+        load_off(1, m1);
+        bool m1_off = true; // m1's ranges are loaded
+
+        // prefetch ring: the first 32 entries of the warp's share of the B
+        // row of jp t sit in slot t % PF
+        int cq[PF];
+        T bq[PF];
+        auto meta_of = [&](int t, T &a, int &j, int &k0, int &k1) {
+            const bool first = (t >> 5) == cb;
+            const int src = t & 31;
+            a = __shfl_sync(FULL, first ? m0.a : m1.a, src);
+            j = __shfl_sync(FULL, first ? m0.j : m1.j, src);
+            k0 = __shfl_sync(FULL, first ? m0.lo : m1.lo, src);
+            k1 = __shfl_sync(FULL, first ? m0.hi : m1.hi, src);
+        };
+#pragma unroll
+        for (int s = 0; s < PF; ++s)
+        {
+            cq[s] = 0;
+            bq[s] = T(0);
+            if (s < ni)
+            {
+                T a;
+                int j, k0, k1;
+                meta_of(s, a, j, k0, k1);
+                const int kp = k0 + lane;
+                if (kp < k1)
+                {
+                    cq[s] = Pc[(size_t) j * g.ldb + kp];
+                    bq[s] = Pv[(size_t) j * g.ldb + kp];
+                }
+            }
+        }
+
+        int d = 0;
+        T dA = T(0);
+        bool ab = false;
+        // one (c, b) entry of jp t: accumulate and record a first touch
+        auto take = [&](bool valid, int c, T b, T a, size_t rb, int kp, unsigned jkey) {
+            bool ins = false;
+            int slot = -1;
+            if (valid)
+            {
+                const T p = mul_rn(a, b);
+                slot = wide_probe<TS>(keys, c, ins);
+                if (slot >= 0)
+                    vals[slot] = add_rn(vals[slot], p);
+            }
+            const unsigned bal = __ballot_sync(FULL, ins);
+            if (ins)
+            {
+                const int r = d + __popc(bal & lanemask_lt());
+                if (r < CAP)
+                {
+                    oslot[r] = (unsigned short) slot;
+                    okey[r] = jkey | Pp[rb + kp];
+                }
+            }
+            d += __popc(bal);
+            if (__any_sync(FULL, valid && slot < 0))
+                d = CAP + 1; // table full: cannot happen below CAP
+        };
+
+        for (int t0 = 0; t0 < ni && !ab; t0 += PF)
+        {
+#pragma unroll
+            for (int s = 0; s < PF; ++s)
+            {
+                const int t = t0 + s;
+                if (t >= ni || ab)
+                    break;
+                if ((t & 31) == 0 && t > 0)
+                {
+                    // entering block cb + 1: shift, start loading the next one
+                    m0 = m1;
+                    ++cb;
+                    load_aj(cb + 1, m1);
+                    m1_off = false;
+                    if (*vabort)
+                    {
+                        ab = true;
+                        break;
+                    }
+                }
+                if (!m1_off && (t & 31) == 8)
+                {
+                    load_off(cb + 1, m1);
+                    m1_off = true;
+                }
+                T a;
+                int j, k0, k1;
+                meta_of(t, a, j, k0, k1);
+                if (j == i)
+                    dA = add_rn(dA, a);
+                const size_t rb = (size_t) j * g.ldb;
+                const unsigned jkey = (unsigned) t << 16;
+                take(k0 + lane < k1, cq[s], bq[s], a, rb, k0 + lane, jkey);
+                for (int kb = k0 + 32; kb < k1; kb += 32)
+                {
+                    const int kp = kb + lane;
+                    int c = 0;
+                    T b = T(0);
+                    if (kp < k1)
+                    {
+                        c = Pc[rb + kp];
+                        b = Pv[rb + kp];
+                    }
+                    take(kp < k1, c, b, a, rb, kp, jkey);
+                }
+                if (d > CAP)
+                {
+                    ab = true;
+                    break;
+                }
+                // refill this slot with jp t + PF
+                const int u = t + PF;
+                if (u < ni)
+                {
+                    T au;
+                    int ju, u0, u1;
+                    meta_of(u, au, ju, u0, u1);
+                    const int kp = u0 + lane;
+                    if (kp < u1)
+                    {
+                        cq[s] = Pc[(size_t) ju * g.ldb + kp];
+                        bq[s] = Pv[(size_t) ju * g.ldb + kp];
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (ab)
+            *vabort = 1;
+        __syncthreads();
+        if (*vabort)
+        {
+            if (tid == 0)
+                next_rows[atomicAdd(&tl->count[next_tier], 1)] = i;
+            continue;
+        }
+
+        if (R > 1)
+        {
+            // A warp with several classes took each jp's entries class by
+            // class: bitonic-sort its list by key (padded to a power of two).
+            int n = 1;
+            while (n < d)
+                n <<= 1;
+            for (int p = d + lane; p < n; p += 32)
+                okey[p] = 0xffffffffu;
+            __syncwarp();
+            for (int size = 2; size <= n; size <<= 1)
+                for (int stride = size >> 1; stride > 0; stride >>= 1)
+                {
+                    for (int x = lane; x < (n >> 1); x += 32)
+                    {
+                        const int lo = 2 * stride * (x / stride) + (x % stride), hi = lo + stride;
+                        const bool up = (lo & size) == 0;
+                        const unsigned ka = okey[lo], kb = okey[hi];
+                        if ((ka > kb) == up)
+                        {
+                            okey[lo] = kb;
+                            okey[hi] = ka;
+                            const unsigned short sa = oslot[lo];
+                            oslot[lo] = oslot[hi];
+                            oslot[hi] = sa;
+                        }
+                    }
+                    __syncwarp();
+                }
+        }
+        static_assert(LP >= CAP, "list shorter than its capacity");
+
+        // Keep flags and the exclusive count of kept entries along this list.
+        int kept = 0;
+        for (int c0 = 0; c0 < d; c0 += 32)
+        {
+            const int p = c0 + lane;
+            bool keep = false;
+            if (p < d)
+            {
+                const int s = oslot[p];
+                const int k = keys[s];
+                const T x = vals[s];
+                if (k == i)
+                {
+                    keep = true;
+                    misc->diag = (double) x;
+                }
+                else
+                    keep = fabs(x) > thr;
+            }
+            const unsigned bal = __ballot_sync(FULL, keep);
+            if (p < d)
+                kcnt[p] = (unsigned short) (kept + __popc(bal & lanemask_lt()));
+            kept += __popc(bal);
+        }
+        if (lane == 0)
+        {
+            kcnt[d] = (unsigned short) kept;
+            misc->dw[warp] = d;
+            misc->kept[warp] = kept;
+        }
+        __syncthreads();
+        // Output slot of a kept entry: kept entries before it in its own list
+        // plus, in every other list, the kept entries with a smaller key.
+        for (int c0 = 0; c0 < d; c0 += 32)
+        {
+            const int p = c0 + lane;
+            if (p >= d)
+                continue;
+            const int s = oslot[p];
+            const int k = keys[s];
+            const T x = vals[s];
+            if (!(k == i || fabs(x) > thr))
+                continue;
+            const unsigned key = okey[p];
+            int out = kcnt[p];
+            for (int w2 = 0; w2 < W; ++w2)
+            {
+                if (w2 == warp)
+                    continue;
+                const unsigned char *ob = smem + (size_t) w2 * Cfg::warp_bytes;
+                const unsigned *ok2 = reinterpret_cast<const unsigned *>(ob + Cfg::off_okey);
+                const unsigned short *kc2 = reinterpret_cast<const unsigned short *>(ob + Cfg::off_kcnt);
+                int lo2 = 0, hi2 = misc->dw[w2];
+                while (lo2 < hi2)
+                {
+                    const int mid = (lo2 + hi2) >> 1;
+                    if (ok2[mid] < key)
+                        lo2 = mid + 1;
+                    else
+                        hi2 = mid;
+                }
+                out += kc2[lo2];
+            }
+            if (out < g.Mc)
+            {
+                Cv[(size_t) i * g.ldc + out] = x;
+                g.Ci[(size_t) i * g.ldc + out] = k;
+            }
+        }
+        if (tid == 0)
+        {
+            int ll = 0, distinct = 0;
+            for (int w = 0; w < W; ++w)
+            {
+                ll += misc->kept[w];
+                distinct += misc->dw[w];
+            }
+            finish_row<T>(g, i, ll, distinct, dA, misc->diag);
+        }
+    }
+}
+
+// -------------------------------------------------------------------------
+// Window tiers K4, K8: two passes over the row with a bitmap of its columns.
+// A team of KW = 8 warps per row, warp w owning the column classes
+// [4w, 4w+4) of the bucketed copy of B, as in the wide tiers.
+//   pass 1: every product column sets its bit in a bitmap over the row's
+//           column window [min, max] of the B rows it references; the owner
+//           warp, walking jp in order, records the first touch of each
+//           column (key jp << 16 | position) in global scratch.
+//   rank:   a prefix of the bitmap's popcounts gives every column a compact
+//           slot: vals needs only one entry per distinct column.
+//   pass 2: the owner warps walk the jps again and sum each product into its
+//           column's slot, in jp order.
+//   output: the kept columns (k == i or |x| > threshold) are sorted by their
+//           first-touch keys, which is the reference's output order.
+// Shared memory: vals[DCAP] | bitmap {bits, prefix}[NWCAP] | kept keys[KCAP]
+// -------------------------------------------------------------------------
+constexpr int KW = 8;
+constexpr int KR = NCLS / KW;
+constexpr int K_NWCAP = 2048; // bitmap words: windows of up to 65536 columns
+constexpr int K_KCAP = 2048;  // kept columns per row
+constexpr int KU = 4;         // 32-entry steps per share held in registers
+constexpr int KPF = 2;        // jps of prefetch
+
+struct KMisc
+{
+    double diag;
+    int row, base, nw, D, kept, pad;
+    int red[2 * KW];
+};
+
+template <typename T, int DCAP> struct KCfg
+{
+    static constexpr size_t off_bmp = (size_t(DCAP) * sizeof(T) + 15) / 16 * 16;
+    static constexpr size_t off_kbuf = off_bmp + size_t(K_NWCAP) * sizeof(uint2);
+    static constexpr size_t off_misc = off_kbuf + size_t(K_KCAP) * sizeof(unsigned long long);
+    static constexpr size_t bytes = off_misc + sizeof(KMisc);
+};
+
+// Sum of A's entries on the diagonal of row i, in row order (one warp).
+template <typename T>
+__device__ __forceinline__ T row_diag_sum(const T *arow, const int *airow, int ni, int i, int lane)
+{
+    T dA = T(0);
+    for (int jp0 = 0; jp0 < ni; jp0 += 32)
+    {
+        const int q = jp0 + lane;
+        const bool hit = q < ni && airow[q] == i;
+        const T av = hit ? arow[q] : T(0);
+        unsigned bal = __ballot_sync(FULL, hit);
+        while (bal)
+        {
+            const int src = __ffs(bal) - 1;
+            bal &= bal - 1;
+            dA = add_rn(dA, __shfl_sync(FULL, av, src));
+        }
+    }
+    return dA;
+}
+
+// Walks the jps of row i in order over this warp's buckets [blo, blo + KR)
+// of each B row, calling op(valid, c, b, a, rb, kp, t) once per 32-entry step
+// (every lane; `valid` says whether the lane holds an entry).  The first
+// KU*32 entries of each share are loaded KPF jps ahead.
+template <typename T, bool NEED_B, typename Op>
+__device__ __forceinline__ void walk_shares(const MulArgs &g, const BucketArgs &ba, const T *arow,
+                                            const int *airow, int ni, int blo, int lane, Op &op)
+{
+    const T *Pv = static_cast<const T *>(ba.v);
+    const int *Pc = ba.c;
+    auto load_aj = [&](int b, JpMeta<T> &m) {
+        const int q = b * 32 + lane;
+        m.a = T(0);
+        m.j = 0;
+        m.lo = m.hi = 0;
+        if (q < ni)
+        {
+            m.a = arow[q];
+            m.j = airow[q];
+        }
+    };
+    auto load_off = [&](int b, JpMeta<T> &m) {
+        if (b * 32 + lane < ni)
+        {
+            const int *o = ba.off + (size_t) m.j * (NCLS + 1) + blo;
+            m.lo = o[0];
+            m.hi = o[KR];
+        }
+    };
+    JpMeta<T> m0, m1;
+    int cb = 0;
+    load_aj(0, m0);
+    load_aj(1, m1);
+    load_off(0, m0);
+    load_off(1, m1);
+    bool m1_off = true;
+    auto meta_of = [&](int t, T &a, int &j, int &k0, int &k1) {
+        const bool first = (t >> 5) == cb;
+        const int src = t & 31;
+        a = __shfl_sync(FULL, first ? m0.a : m1.a, src);
+        j = __shfl_sync(FULL, first ? m0.j : m1.j, src);
+        k0 = __shfl_sync(FULL, first ? m0.lo : m1.lo, src);
+        k1 = __shfl_sync(FULL, first ? m0.hi : m1.hi, src);
+    };
+    int cq[KPF][KU];
+    T bq[KPF][KU];
+    auto fill = [&](int u, int s) {
+        T a;
+        int j, k0, k1;
+        meta_of(u, a, j, k0, k1);
+        const size_t rb = (size_t) j * g.ldb;
+#pragma unroll
+        for (int x = 0; x < KU; ++x)
+        {
+            const int kp = k0 + x * 32 + lane;
+            cq[s][x] = 0;
+            bq[s][x] = T(0);
+            if (kp < k1)
+            {
+                cq[s][x] = Pc[rb + kp];
+                if (NEED_B)
+                    bq[s][x] = Pv[rb + kp];
+            }
+        }
+    };
+#pragma unroll
+    for (int s = 0; s < KPF; ++s)
+        if (s < ni)
+            fill(s, s);
+    for (int t0 = 0; t0 < ni; t0 += KPF)
+    {
+#pragma unroll
+        for (int s = 0; s < KPF; ++s)
+        {
+            const int t = t0 + s;
+            if (t >= ni)
+                break;
+            if ((t & 31) == 0 && t > 0)
+            {
+                m0 = m1;
+                ++cb;
+                load_aj(cb + 1, m1);
+                m1_off = false;
+            }
+            if (!m1_off && (t & 31) == 8)
+            {
+                load_off(cb + 1, m1);
+                m1_off = true;
+            }
+            T a;
+            int j, k0, k1;
+            meta_of(t, a, j, k0, k1);
+            const size_t rb = (size_t) j * g.ldb;
+#pragma unroll
+            for (int x = 0; x < KU; ++x)
+                if (k0 + x * 32 < k1)
+                    op(k0 + x * 32 + lane < k1, cq[s][x], bq[s][x], a, rb, k0 + x * 32 + lane, t);
+            for (int kb = k0 + KU * 32; kb < k1; kb += 32)
+            {
+                const int kp = kb + lane;
+                int c = 0;
+                T b = T(0);
+                if (kp < k1)
+                {
+                    c = Pc[rb + kp];
+                    if (NEED_B)
+                        b = Pv[rb + kp];
+                }
+                op(kp < k1, c, b, a, rb, kp, t);
+            }
+            if (t + KPF < ni)
+                fill(t + KPF, s);
+            __syncwarp();
+        }
+    }
+}
+
+template <typename T, int DCAP, int MINB>
+__global__ void __launch_bounds__(KW * 32, MINB)
+    window_kernel(MulArgs g, BucketArgs ba, const int *rows, TierLists *tl, int tier, int next_tier,
+                  int *next_rows, unsigned *keyg, void *gvals)
+{
+    using Cfg = KCfg<T, DCAP>;
+    constexpr int NT = KW * 32;
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (g.flags->bad_input)
+        return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    T *vals = reinterpret_cast<T *>(smem);
+    uint2 *bmp = reinterpret_cast<uint2 *>(smem + Cfg::off_bmp);
+    unsigned long long *kbuf = reinterpret_cast<unsigned long long *>(smem + Cfg::off_kbuf);
+    KMisc *misc = reinterpret_cast<KMisc *>(smem + Cfg::off_misc);
+    unsigned *mykey = keyg + (size_t) blockIdx.x * (K_NWCAP * 32);
+    // accumulator of rows wider than DCAP: a compact slab of this block in
+    // device memory (one entry per distinct column, so it stays in L2)
+    T *myvals = static_cast<T *>(gvals) + (size_t) blockIdx.x * (K_NWCAP * 32);
+    const unsigned short *Pp = ba.p;
+    const int nrows = tl->count[tier];
+    const T *Av = static_cast<const T *>(g.Av);
+    T *Cv = static_cast<T *>(g.Cv);
+    const T thr = (T) g.thr;
+    const int blo = warp * KR;
+
+    for (;;)
+    {
+        __syncthreads(); // the previous row is written out
+        if (tid == 0)
+        {
+            misc->row = atomicAdd(&tl->cursor[tier], 1);
+            misc->diag = 0.0;
+            misc->kept = 0;
+        }
+        __syncthreads();
+        const int pos = misc->row;
+        if (pos >= nrows)
+            break;
+        const int i = rows[pos];
+        const int ni = g.An[i];
+        const T *arow = Av + (size_t) i * g.lda;
+        const int *airow = g.Ai + (size_t) i * g.lda;
+
+        // column window of the row: the B rows' column ranges
+        int mn = 0x7fffffff, mx = -1;
+        for (int q = tid; q < ni; q += NT)
+        {
+            const int j = airow[q];
+            mn = min(mn, ba.cmin[j]);
+            mx = max(mx, ba.cmax[j]);
+        }
+        mn = __reduce_min_sync(FULL, mn);
+        mx = __reduce_max_sync(FULL, mx);
+        if (lane == 0)
+        {
+            misc->red[warp] = mn;
+            misc->red[KW + warp] = mx;
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            for (int w = 1; w < KW; ++w)
+            {
+                mn = min(mn, misc->red[w]);
+                mx = max(mx, misc->red[KW + w]);
+            }
+            misc->base = mx < 0 ? 0 : (mn & ~31);
+            misc->nw = mx < 0 ? 0 : (mx >> 5) - (mn >> 5) + 1;
+        }
+        __syncthreads();
+        const int base = misc->base, nw = misc->nw;
+        if (nw > K_NWCAP)
+        {
+            if (tid == 0)
+                next_rows[atomicAdd(&tl->count[next_tier], 1)] = i;
+            continue;
+        }
+        for (int w = tid; w < nw; w += NT)
+            bmp[w] = make_uint2(0u, 0u);
+        __syncthreads();
+
+        // pass 1: bitmap of the row's columns, first-touch keys
+        auto mark = [&](bool valid, int c, T, T, size_t rb, int kp, int t) {
+            if (valid)
+            {
+                const int bit = c - base;
+                const unsigned m = 1u << (bit & 31);
+                // most products land on a column already marked: test first
+                if (!(bmp[bit >> 5].x & m))
+                {
+                    const unsigned old = atomicOr(&bmp[bit >> 5].x, m);
+                    if (!(old & m))
+                        mykey[bit] = ((unsigned) t << 16) | Pp[rb + kp];
+                }
+            }
+        };
+        walk_shares<T, false>(g, ba, arow, airow, ni, blo, lane, mark);
+        __syncthreads();
+
+        // rank: exclusive prefix of the popcounts, words split into NT runs
+        {
+            const int per = (nw + NT - 1) / NT;
+            const int w0 = min(tid * per, nw), w1 = min(w0 + per, nw);
+            int sum = 0;
+            for (int w = w0; w < w1; ++w)
+                sum += __popc(bmp[w].x);
+            int incl = sum;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o)
+                    incl += y;
+            }
+            if (lane == 31)
+                misc->red[warp] = incl;
+            __syncthreads();
+            int before = 0;
+            for (int w = 0; w < warp; ++w)
+                before += misc->red[w];
+            int run = before + incl - sum;
+            for (int w = w0; w < w1; ++w)
+            {
+                bmp[w].y = (unsigned) run;
+                run += __popc(bmp[w].x);
+            }
+            if (tid == NT - 1)
+                misc->D = before + incl;
+        }
+        __syncthreads();
+        const int D = misc->D;
+        T *acc_v = D <= DCAP ? vals : myvals;
+        for (int s = tid; s < D; s += NT)
+            acc_v[s] = T(0);
+        __syncthreads();
+
+        // pass 2: sums in jp order, one owner warp per column
+        if (D <= DCAP)
+        {
+            auto acc = [&](bool valid, int c, T b, T a, size_t, int, int) {
+                if (valid)
+                {
+                    const int bit = c - base;
+                    const uint2 pr = bmp[bit >> 5];
+                    const int slot = (int) pr.y + __popc(pr.x & ((1u << (bit & 31)) - 1u));
+                    vals[slot] = add_rn(vals[slot], mul_rn(a, b));
+                }
+            };
+            walk_shares<T, true>(g, ba, arow, airow, ni, blo, lane, acc);
+        }
+        else
+        {
+            auto acc = [&](bool valid, int c, T b, T a, size_t, int, int) {
+                if (valid)
+                {
+                    const int bit = c - base;
+                    const uint2 pr = bmp[bit >> 5];
+                    const int slot = (int) pr.y + __popc(pr.x & ((1u << (bit & 31)) - 1u));
+                    myvals[slot] = add_rn(myvals[slot], mul_rn(a, b));
+                }
+            };
+            walk_shares<T, true>(g, ba, arow, airow, ni, blo, lane, acc);
+        }
+        T dA = T(0);
+        if (warp == 0)
+            dA = row_diag_sum<T>(arow, airow, ni, i, lane);
+        __syncthreads();
+
+        // kept columns with their first-touch keys
+        for (int w = tid; w < nw; w += NT)
+        {
+            const uint2 pr = bmp[w];
+            unsigned bits = pr.x;
+            int slot = (int) pr.y;
+            while (bits)
+            {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const int c = base + 32 * w + b;
+                const T x = acc_v[slot++];
+                bool keep;
+                if (c == i)
+                {
+                    keep = true;
+                    misc->diag = (double) x;
+                }
+                else
+                    keep = fabs(x) > thr;
+                if (keep)
+                {
+                    const int p = atomicAdd(&misc->kept, 1);
+                    if (p < K_KCAP)
+                        kbuf[p] = ((unsigned long long) mykey[c - base] << 32) | (unsigned) c;
+                }
+            }
+        }
+        __syncthreads();
+        const int kept = misc->kept;
+        if (kept > K_KCAP)
+        {
+            if (tid == 0)
+                next_rows[atomicAdd(&tl->count[next_tier], 1)] = i;
+            continue;
+        }
+        // first-touch order: bitonic sort of the kept keys
+        int n = 1;
+        while (n < kept)
+            n <<= 1;
+        for (int p = kept + tid; p < n; p += NT)
+            kbuf[p] = ~0ull;
+        __syncthreads();
+        for (int size = 2; size <= n; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1)
+            {
+                for (int x = tid; x < (n >> 1); x += NT)
+                {
+                    const int lo = 2 * stride * (x / stride) + (x % stride), hi = lo + stride;
+                    const bool up = (lo & size) == 0;
+                    const unsigned long long ka = kbuf[lo], kb = kbuf[hi];
+                    if ((ka > kb) == up)
+                    {
+                        kbuf[lo] = kb;
+                        kbuf[hi] = ka;
+                    }
+                }
+                __syncthreads();
+            }
+        const int nout = min(kept, g.Mc);
+        for (int p = tid; p < nout; p += NT)
+        {
+            const int c = (int) (unsigned) kbuf[p];
+            const int bit = c - base;
+            const uint2 pr = bmp[bit >> 5];
+            const int slot = (int) pr.y + __popc(pr.x & ((1u << (bit & 31)) - 1u));
+            Cv[(size_t) i * g.ldc + p] = acc_v[slot];
+            g.Ci[(size_t) i * g.ldc + p] = c;
+        }
+        if (tid == 0)
+            finish_row<T>(g, i, kept, D, dA, misc->diag);
+    }
+}
+
+// -------------------------------------------------------------------------
 // Tier C: dense accumulator over all columns, in global memory, one slab per
 // block: acc[ncols] (T), mark[ncols] (int, row+1 while the column is live),
 // order[ncols] (int, column ids in first-touch order).  Marks are cleared
@@ -861,10 +1829,8 @@ __global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs 
     }
 }
 
-// Team tier configurations: (W, LOGTS, STAGES, CHUNK, min blocks per SM)
+// Team tier B1: (W, LOGTS, STAGES, CHUNK, min blocks per SM)
 #define B1_CFG 4, 11, 3, 256, 4
-#define B2_CFG 4, 12, 3, 256, 3
-#define B3_CFG 16, 13, 3, 512, 1
 
 template <typename T, int W, int LOGTS, int STAGES, int CHUNK, int MINB>
 bool launch_team(B200Context *c, const MulArgs &g, const int *rows, TierLists *tl, int tier,
@@ -881,6 +1847,58 @@ bool launch_team(B200Context *c, const MulArgs &g, const int *rows, TierLists *t
     return LAUNCH_OK("team_kernel");
 }
 
+// Wide tiers: (warps, slots per warp, min blocks per SM)
+#define W8_CFG 8, 256, 4
+#define W16_CFG 16, 256, 2
+// Window tiers: (distinct columns held, min blocks per SM)
+#define K4_CFG 4096, 3
+#define K8_CFG 8192, 2
+
+template <typename T, int DCAP, int MINB> constexpr size_t window_bytes()
+{
+    return KCfg<T, DCAP>::bytes;
+}
+
+template <typename T, int DCAP, int MINB> int window_grid(B200Context *c)
+{
+    auto k = window_kernel<T, DCAP, MINB>;
+    if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) KCfg<T, DCAP>::bytes)))
+        return 0;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, KW * 32, KCfg<T, DCAP>::bytes);
+    return c->sm_count * (occ > 0 ? occ : 1);
+}
+
+template <typename T, int DCAP, int MINB>
+bool launch_window(B200Context *c, int grid, const MulArgs &g, const BucketArgs &ba, const int *rows,
+                   TierLists *tl, int tier, int next_tier, int *next_rows, unsigned *keyg, void *gvals)
+{
+    window_kernel<T, DCAP, MINB><<<grid, KW * 32, KCfg<T, DCAP>::bytes, c->stream>>>(
+        g, ba, rows, tl, tier, next_tier, next_rows, keyg, gvals);
+    return LAUNCH_OK("window_kernel");
+}
+
+template <typename T, int W, int TS, int MINB> constexpr size_t wide_bytes()
+{
+    return WideCfg<T, W, TS>::bytes;
+}
+
+template <typename T, int W, int TS, int MINB>
+bool launch_wide(B200Context *c, const MulArgs &g, const BucketArgs &ba, const int *rows,
+                 TierLists *tl, int tier, int next_tier, int *next_rows)
+{
+    using Cfg = WideCfg<T, W, TS>;
+    auto k = wide_kernel<T, W, TS, MINB>;
+    if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg::bytes)))
+        return false;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, W * 32, Cfg::bytes);
+    const int grid = c->sm_count * (occ > 0 ? occ : 1);
+    k<<<grid, W * 32, Cfg::bytes, c->stream>>>(g, ba, rows, tl, tier, next_tier, next_rows);
+    return LAUNCH_OK("wide_kernel");
+}
+
 constexpr int C_BLOCKS_PER_SM = B200_C_BLOCKS;
 
 // Distinct-column counts of the last multiply, reused as the next call's
@@ -890,6 +1908,7 @@ int *g_hint = nullptr;
 int g_hint_n = 0;
 bool g_hint_valid = false;
 int g_last_tiers[NTIERS] = {0};
+int g_tier_mask = B200_X2_TIERS;
 
 template <typename T>
 bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
@@ -923,10 +1942,43 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     g.hint = g_hint_valid ? g_hint : nullptr;
     g.hint_out = g_hint;
 
-    // scratch: NTIERS lists of N ints, diag arrays (2N doubles), dense slabs
-    size_t off_diag = ((size_t) NTIERS * N * sizeof(int) + 255) & ~size_t(255);
-    size_t off_slabs = (off_diag + (size_t) 2 * N * sizeof(double) + 255) & ~size_t(255);
-    size_t total = off_slabs + (size_t) gridC * slab_bytes;
+    // Tiers in use for this call.  The P tiers key order entries by
+    // (jp << 16 | position), so both row lengths must stay below 2^16, and
+    // their shared memory must fit the device.
+    int tmask = g_tier_mask | (1 << TIER_C);
+    if (g.lda >= 65536 || g.ldb >= 65536)
+        tmask &= ~BUCKET_TIERS_MASK;
+    if (wide_bytes<T, W8_CFG>() > c->smem_optin)
+        tmask &= ~(1 << TIER_W8);
+    if (wide_bytes<T, W16_CFG>() > c->smem_optin)
+        tmask &= ~(1 << TIER_W16);
+    if (window_bytes<T, K4_CFG>() > c->smem_optin)
+        tmask &= ~(1 << TIER_K4);
+    if (window_bytes<T, K8_CFG>() > c->smem_optin)
+        tmask &= ~(1 << TIER_K8);
+    const int gridK4 = ((tmask >> TIER_K4) & 1) ? window_grid<T, K4_CFG>(c) : 0;
+    const int gridK8 = ((tmask >> TIER_K8) & 1) ? window_grid<T, K8_CFG>(c) : 0;
+    if (((tmask >> TIER_K4) & 1) && !gridK4)
+        return false;
+    if (((tmask >> TIER_K8) & 1) && !gridK8)
+        return false;
+    const int gridK = gridK4 > gridK8 ? gridK4 : gridK8;
+    const bool use_p = (tmask & BUCKET_TIERS_MASK) != 0;
+
+    // scratch: NTIERS lists of N ints, diag arrays (2N doubles), dense slabs,
+    // and (P tiers) the bucketed copy of B: values, columns, positions, offsets
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t nbe = (size_t) g.NB * g.ldb;
+    const size_t off_diag = al((size_t) NTIERS * N * sizeof(int));
+    const size_t off_slabs = al(off_diag + (size_t) 2 * N * sizeof(double));
+    const size_t off_pv = al(off_slabs + (size_t) gridC * slab_bytes);
+    const size_t off_pc = al(off_pv + (use_p ? nbe * sizeof(T) : 0));
+    const size_t off_pp = al(off_pc + (use_p ? nbe * sizeof(int) : 0));
+    const size_t off_po = al(off_pp + (use_p ? nbe * sizeof(unsigned short) : 0));
+    const size_t off_mm = al(off_po + (use_p ? (size_t) g.NB * (NCLS + 1) * sizeof(int) : 0));
+    const size_t off_keyg = al(off_mm + (use_p ? (size_t) 2 * g.NB * sizeof(int) : 0));
+    const size_t off_gvals = al(off_keyg + (size_t) gridK * K_NWCAP * 32 * sizeof(unsigned));
+    const size_t total = al(off_gvals + (size_t) gridK * K_NWCAP * 32 * sizeof(T));
     unsigned char *scr = static_cast<unsigned char *>(b200_scratch(total));
     if (!scr)
         return false;
@@ -934,6 +1986,11 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     double *diagA = reinterpret_cast<double *>(scr + off_diag);
     double *diagC = diagA + N;
     unsigned char *slabs = scr + off_slabs;
+    BucketArgs ba{scr + off_pv, reinterpret_cast<int *>(scr + off_pc),
+                  reinterpret_cast<unsigned short *>(scr + off_pp), reinterpret_cast<int *>(scr + off_po),
+                  reinterpret_cast<int *>(scr + off_mm), reinterpret_cast<int *>(scr + off_mm) + g.NB};
+    unsigned *keyg = reinterpret_cast<unsigned *>(scr + off_keyg);
+    void *gvals = scr + off_gvals;
 
     // small device block: TierLists | MulFlags | trace[2]
     unsigned char *small = static_cast<unsigned char *>(c->d_small);
@@ -961,10 +2018,16 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     if (!LAUNCH_OK("validate_cols_kernel"))
         return false;
     const int pgrid = max(1, min(b200_ceil_div(N, 8), c->sm_count * 16));
-    // The team tiers keep order positions in 16 bits: tables of at most 8192.
-    plan_kernel<<<pgrid, 256, 0, c->stream>>>(g, ncols, 0, tl, lists);
+    plan_kernel<<<pgrid, 256, 0, c->stream>>>(g, ncols, tmask, tl, lists);
     if (!LAUNCH_OK("plan_kernel"))
         return false;
+    if (use_p)
+    {
+        bucket_kernel<T><<<vgrid, 256, 0, c->stream>>>(static_cast<const T *>(g.Bv), g.Bi, g.Bn, g.ldb,
+                                                       g.NB, ba);
+        if (!LAUNCH_OK("bucket_kernel"))
+            return false;
+    }
 
     auto list = [&](int t) { return lists + (size_t) t * N; };
     if (!CUDA_OK(cudaFuncSetAttribute(tierA_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -972,36 +2035,45 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
         return false;
     int occA = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occA, tierA_kernel<T>, 32 * A_WARPS, smemA);
-    int nextA = 1;
-    while (nextA < NTIERS - 1 && !((B200_X2_TIERS >> nextA) & 1))
-        ++nextA;
-    tierA_kernel<T><<<c->sm_count * max(occA, 1), 32 * A_WARPS, smemA, c->stream>>>(
-        g, list(0), tl, nextA, list(nextA));
-    if (!LAUNCH_OK("tierA_kernel"))
-        return false;
     // Rows a tier cannot hold go to the next tier in use (the dense tier
     // always is); tiers switched off are not launched.
+    auto next_on = [tmask](int t) {
+        int n = t + 1;
+        while (n < NTIERS - 1 && !((tmask >> n) & 1))
+            ++n;
+        return n;
+    };
+    if (tmask & 1)
     {
-        auto next_on = [](int t) {
-            int n = t + 1;
-            while (n < NTIERS - 1 && !((B200_X2_TIERS >> n) & 1))
-                ++n;
-            return n;
-        };
-        if ((B200_X2_TIERS >> 1) & 1)
-            if (!launch_team<T, B1_CFG>(c, g, list(1), tl, 1, next_on(1), list(next_on(1))))
-                return false;
-        if ((B200_X2_TIERS >> 2) & 1)
-            if (!launch_team<T, B2_CFG>(c, g, list(2), tl, 2, next_on(2), list(next_on(2))))
-                return false;
-        if ((B200_X2_TIERS >> 3) & 1)
-            if (!launch_team<T, B3_CFG>(c, g, list(3), tl, 3, next_on(3), list(next_on(3))))
-                return false;
+        tierA_kernel<T><<<c->sm_count * max(occA, 1), 32 * A_WARPS, smemA, c->stream>>>(
+            g, list(0), tl, next_on(0), list(next_on(0)));
+        if (!LAUNCH_OK("tierA_kernel"))
+            return false;
     }
+    if ((tmask >> TIER_W8) & 1)
+        if (!launch_wide<T, W8_CFG>(c, g, ba, list(TIER_W8), tl, TIER_W8, next_on(TIER_W8),
+                                    list(next_on(TIER_W8))))
+            return false;
+    if ((tmask >> TIER_B1) & 1)
+        if (!launch_team<T, B1_CFG>(c, g, list(TIER_B1), tl, TIER_B1, next_on(TIER_B1),
+                                    list(next_on(TIER_B1))))
+            return false;
+    if ((tmask >> TIER_W16) & 1)
+        if (!launch_wide<T, W16_CFG>(c, g, ba, list(TIER_W16), tl, TIER_W16, next_on(TIER_W16),
+                                     list(next_on(TIER_W16))))
+            return false;
+    if ((tmask >> TIER_K4) & 1)
+        if (!launch_window<T, K4_CFG>(c, gridK4, g, ba, list(TIER_K4), tl, TIER_K4, next_on(TIER_K4),
+                                      list(next_on(TIER_K4)), keyg, gvals))
+            return false;
+    if ((tmask >> TIER_K8) & 1)
+        if (!launch_window<T, K8_CFG>(c, gridK8, g, ba, list(TIER_K8), tl, TIER_K8, next_on(TIER_K8),
+                                      list(next_on(TIER_K8)), keyg, gvals))
+            return false;
     if (!CUDA_OK(cudaFuncSetAttribute(dense_tier_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
         return false;
-    dense_tier_kernel<T><<<gridC, 256, smemC, c->stream>>>(g, smaxC, ncols, list(NTIERS - 1), tl, slabs);
+    dense_tier_kernel<T><<<gridC, 256, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs);
     if (!LAUNCH_OK("dense_tier_kernel"))
         return false;
 
@@ -1096,10 +2168,20 @@ bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matri
 }
 
 // Rows handled by each multiply tier in the last call on this process
-// (A, O1, O2, O3, C; a row handed on is counted in every tier it entered).
+// (A, W8, B1, W16, K4, K8, C; a row handed on is counted in every tier it entered).
 extern "C" BML_B200_API int bml_b200_last_tier_counts(int *counts, int n)
 {
     for (int t = 0; t < n && t < NTIERS; ++t)
         counts[t] = g_last_tiers[t];
     return NTIERS;
+}
+
+// Tier selection for later multiplies (bit t = tier t in the order above; 0
+// restores the default).  Also forgets the per-row estimates of the last call.
+extern "C" BML_B200_API int bml_b200_set_x2_tiers(int mask)
+{
+    const int old = g_tier_mask;
+    g_tier_mask = mask ? (mask & ((1 << NTIERS) - 1)) : B200_X2_TIERS;
+    g_hint_valid = false;
+    return old;
 }

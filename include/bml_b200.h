@@ -266,10 +266,21 @@ BML_B200_API int bml_b200_multiply_x2(bml_matrix_t *X, bml_matrix_t *X2,
  * truncation to M (lets a caller size M exactly after ROW_OVERFLOW). */
 BML_B200_API int bml_b200_last_required_M(void);
 
-/* Diagnostics of the last ELLPACK multiply: rows per kernel tier (tier A:
- * one warp and a 1024-slot table; O1-O3: sixteen warps and 2048/4096/8192
- * slots; C: dense accumulator in device memory).  Returns the tier count. */
+/* Diagnostics of the last ELLPACK multiply: rows per kernel tier, in the
+ * order A (one warp, 1024-slot table), W8, B1 (four warps, 2048 slots,
+ * TMA-staged rows), W16 (8/16 warps per row, each warp owning a share of the
+ * column classes k % 32 with a 256-slot table), K4, K8 (8 warps, bitmap-ranked
+ * accumulator of up to 4096/8192 columns), C (dense accumulator in device
+ * memory).  Returns the tier count. */
 BML_B200_API int bml_b200_last_tier_counts(int *counts, int n);
+
+/* Selects the multiply tiers later ELLPACK multiplies may use: bit t enables
+ * tier t in the order of bml_b200_last_tier_counts; the dense tier C is
+ * always enabled; 0 restores the default.  Any choice gives the same result
+ * (the tiers differ only in speed), and rows a tier cannot hold move on to the
+ * next enabled one.  Also discards the per-row width estimates kept from the
+ * last multiply.  Returns the previous mask.  No reference counterpart. */
+BML_B200_API int bml_b200_set_x2_tiers(int mask);
 
 /* Raw ELLPACK transfer between the device matrix and caller host arrays laid
  * out like the reference (row-major value[N*M], index[N*M], nnz[N]). */
