@@ -16,10 +16,13 @@ def pytest_configure(config):
 def _ensure_built():
     lib = os.path.join(ROOT, "bml_b200", "libbml_b200.so")
     if not os.path.exists(lib):
-        sys.path.insert(0, ROOT)
-        from bml_b200 import build as _b  # noqa: F401
-        import importlib
-        importlib.import_module("bml_b200.build").build()
+        # load build.py on its own: importing the package needs the library
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("bml_b200_build",
+                                                      os.path.join(ROOT, "bml_b200", "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
     ora = os.path.join(ROOT, "oracle", "_ref", "libbml_oracle.so")
     if not os.path.exists(ora):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True,
