@@ -78,6 +78,9 @@ _PROTOS = {
     "bml_threshold": (None, [_vp, _d]),
     "bml_trace": (_d, [_vp]),
     "bml_trace_mult": (_d, [_vp, _vp]),
+    "bml_sum_squares": (_d, [_vp]),
+    "bml_fnorm": (_d, [_vp]),
+    "bml_fnorm2": (_d, [_vp, _vp]),
     "bml_transpose_new": (_vp, [_vp]),
     "bml_transpose": (None, [_vp]),
     "bml_scale_new": (_vp, [_vp, _vp]),
@@ -107,6 +110,7 @@ _PROTOS = {
     "bml_b200_synchronize": (_i, []),
     "bml_b200_device_info": (_i, [_ip, _ip]),
     "bml_b200_sp2": (_i, [_vp, _vp, _d, _d, _i, _d, _i, _dp]),
+    "bml_b200_sp2_mixed": (_i, [_vp, _vp, _d, _d, _i, _d, _i, _i, _dp]),
     "bml_b200_gen_chain": (_i, [_i, _i, C.c_ulonglong, _dp, _ip, _ip]),
     "bml_b200_gen_lattice": (_i, [_i, _i, _i, _i, C.c_ulonglong, _dp, _ip, _ip]),
     "bml_b200_reset_block_sizes": (None, []),

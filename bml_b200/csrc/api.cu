@@ -341,9 +341,29 @@ bml_matrix_t *bml_convert(bml_matrix_t *A, bml_matrix_type_t matrix_type,
                           bml_matrix_precision_t matrix_precision, int M,
                           bml_distribution_mode_t distrib_mode)
 {
-    // Through a dense copy, as the reference does (bml_convert.c:20-63).
     if (!A)
         return nullptr;
+    if (type_of(A) == ellpack && matrix_type == ellpack && real_prec(matrix_precision))
+    {
+        // ELLPACK to ELLPACK: the same entries, each rounded to the new
+        // precision, on the device.  (The reference sets every one of the
+        // N*N elements, zeros included, through bml_set_element,
+        // ellpack/bml_convert_ellpack_typed.c:13-36, which needs M = N.)
+        bml_matrix_ellpack_t *E = as_ell(A, "convert");
+        if (!E)
+            return nullptr;
+        bml_matrix_t *B = bml_zero_matrix(ellpack, matrix_precision, E->N, M, distrib_mode);
+        if (!B)
+            return nullptr;
+        if (!ell_convert(E, static_cast<bml_matrix_ellpack_t *>(B)))
+        {
+            bml_deallocate(&B);
+            return nullptr;
+        }
+        return B;
+    }
+    // Other types through a dense copy, as the reference does
+    // (bml_convert.c:20-63).
     void *D = bml_export_to_dense(A, dense_row_major);
     if (!D)
         return nullptr;
@@ -355,6 +375,32 @@ bml_matrix_t *bml_convert(bml_matrix_t *A, bml_matrix_type_t matrix_type,
         unsupported(A, "convert between precisions");
     free(D);
     return B;
+}
+
+// ---------------------------------------------------------------------------
+// norms (bml_norm.h): ELLPACK
+// ---------------------------------------------------------------------------
+double bml_sum_squares(bml_matrix_t *A)
+{
+    bml_matrix_ellpack_t *E = as_ell(A, "sum_squares");
+    double s = 0.0;
+    if (E)
+        ell_sum_squares(E, &s);
+    return s;
+}
+
+double bml_fnorm(bml_matrix_t *A)
+{
+    return sqrt(bml_sum_squares(A));
+}
+
+double bml_fnorm2(bml_matrix_t *A, bml_matrix_t *B)
+{
+    bml_matrix_ellpack_t *EA = as_ell(A, "fnorm2"), *EB = as_ell(B, "fnorm2");
+    double f = 0.0;
+    if (EA && EB)
+        ell_fnorm2(EA, EB, &f);
+    return f;
 }
 
 // ---------------------------------------------------------------------------

@@ -993,3 +993,252 @@ bool ell_gershgorin(bml_matrix_ellpack_t *A, double *bounds)
     bounds[1] = pin[0]; // emax
     return true;
 }
+
+// ---------------------------------------------------------------------------
+// Norms.  sum_squares: sum of a*a over the stored entries
+// (ellpack/bml_norm_ellpack_typed.c:31-60); fnorm2: ||A - B||_F over A's
+// entries, with B's entry of the same column or 0, plus B's entries whose
+// column A lacks or holds as exactly 0 (:371-440).  Each product is formed in
+// the matrix precision as in the reference; the sums are FP64, one per row,
+// then added in a fixed order.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+__global__ void sumsq_kernel(const T *V, const int *Nz, int ld, int N, double *rows)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        double s = 0.0;
+        for (int p = lane; p < Nz[i]; p += 32)
+        {
+            const T x = V[(size_t) i * ld + p];
+            s += (double) (x * x);
+        }
+        for (int o = 16; o; o >>= 1)
+            s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0)
+            rows[i] = s;
+    }
+}
+
+// One block per row; tables map each row's columns to positions.
+template <typename T>
+__global__ void __launch_bounds__(256) fnorm2_kernel(const T *Av, const int *Ai, const int *An, int lda,
+                                                     const T *Bv, const int *Bi, const int *Bn, int ldb,
+                                                     int N, int logts, double *rows)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int TS = 1 << logts;
+    const unsigned mask = TS - 1;
+    int *ka = reinterpret_cast<int *>(smem);
+    int *pa = ka + TS;
+    int *kb = pa + TS;
+    int *pb = kb + TS;
+    __shared__ double part[8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = blockIdx.x; i < N; i += gridDim.x)
+    {
+        for (int s = tid; s < TS; s += 256)
+        {
+            ka[s] = B200_EMPTY_KEY;
+            kb[s] = B200_EMPTY_KEY;
+        }
+        __syncthreads();
+        const int na = An[i], nb = Bn[i];
+        // columns are distinct within a row, so each key is put once
+        for (int p = tid; p < na; p += 256)
+            hash_put(ka, pa, mask, Ai[(size_t) i * lda + p], p);
+        for (int p = tid; p < nb; p += 256)
+            hash_put(kb, pb, mask, Bi[(size_t) i * ldb + p], p);
+        __syncthreads();
+        double s = 0.0;
+        for (int p = tid; p < na; p += 256)
+        {
+            const int q = hash_get(kb, pb, mask, Ai[(size_t) i * lda + p]);
+            const T r = q >= 0 ? Bv[(size_t) i * ldb + q] : T(0);
+            const T d = Av[(size_t) i * lda + p] - r;
+            s += (double) (d * d);
+        }
+        for (int p = tid; p < nb; p += 256)
+        {
+            const int q = hash_get(ka, pa, mask, Bi[(size_t) i * ldb + p]);
+            const T r = q >= 0 ? Av[(size_t) i * lda + q] : T(0);
+            if (r == T(0))
+            {
+                const T x = Bv[(size_t) i * ldb + p];
+                s += (double) (x * x);
+            }
+        }
+        for (int o = 16; o; o >>= 1)
+            s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0)
+            part[warp] = s;
+        __syncthreads();
+        if (tid == 0)
+        {
+            double t = 0.0;
+            for (int w = 0; w < 8; ++w)
+                t += part[w];
+            rows[i] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// Entry-for-entry copy between precisions (round to nearest).
+template <typename S, typename D>
+__global__ void convert_kernel(const S *Av, const int *Ai, const int *An, int lda, D *Bv, int *Bi,
+                               int *Bn, int ldb, int Mb, int N, int *overflow)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int n = An[i];
+        const int m = min(n, Mb);
+        for (int p = lane; p < m; p += 32)
+        {
+            Bv[(size_t) i * ldb + p] = (D) Av[(size_t) i * lda + p];
+            Bi[(size_t) i * ldb + p] = Ai[(size_t) i * lda + p];
+        }
+        if (lane == 0)
+        {
+            Bn[i] = m;
+            if (n > Mb)
+                atomicExch(overflow, 1);
+        }
+    }
+}
+
+bool sum_rows_to_host(B200Context *c, double *rows, int N, double *result)
+{
+    double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
+    b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(rows, nullptr, N, out);
+    if (!LAUNCH_OK("b200_sum_rows_kernel"))
+        return false;
+    double *pin = reinterpret_cast<double *>(static_cast<unsigned char *>(c->pinned) + 3072);
+    if (!CUDA_OK(cudaMemcpyAsync(pin, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream)) ||
+        !b200_sync())
+        return false;
+    *result = pin[0];
+    return true;
+}
+
+} // namespace
+
+bool ell_sum_squares(bml_matrix_ellpack_t *A, double *result)
+{
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A))
+        return false;
+    double *rows = static_cast<double *>(b200_scratch((size_t) A->N * sizeof(double)));
+    if (!rows)
+        return false;
+    const int grid = rows_grid(c, A->N, 8);
+    if (A->matrix_precision == double_real)
+        sumsq_kernel<double><<<grid, 256, 0, c->stream>>>(static_cast<const double *>(A->d_value),
+                                                          A->d_nnz, A->ld, A->N, rows);
+    else
+        sumsq_kernel<float><<<grid, 256, 0, c->stream>>>(static_cast<const float *>(A->d_value),
+                                                         A->d_nnz, A->ld, A->N, rows);
+    if (!LAUNCH_OK("sumsq_kernel"))
+        return false;
+    return sum_rows_to_host(c, rows, A->N, result);
+}
+
+bool ell_fnorm2(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *result)
+{
+    if (!check_pair(A, B, "fnorm2"))
+        return false;
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A) || !ell_to_device(B))
+        return false;
+    int logts = 5;
+    while ((1 << logts) < 2 * (A->M > B->M ? A->M : B->M))
+        ++logts;
+    const size_t smem = (size_t) 4 * (1 << logts) * sizeof(int);
+    if (smem > c->smem_optin)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "fnorm2: rows of width %d are too wide", A->M);
+        return false;
+    }
+    double *rows = static_cast<double *>(b200_scratch((size_t) A->N * sizeof(double)));
+    if (!rows)
+        return false;
+    const int grid = max(1, min(A->N, c->sm_count * 8));
+    if (A->matrix_precision == double_real)
+    {
+        auto k = fnorm2_kernel<double>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 256, smem, c->stream>>>(static_cast<const double *>(A->d_value), A->d_index, A->d_nnz,
+                                          A->ld, static_cast<const double *>(B->d_value), B->d_index,
+                                          B->d_nnz, B->ld, A->N, logts, rows);
+    }
+    else
+    {
+        auto k = fnorm2_kernel<float>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 256, smem, c->stream>>>(static_cast<const float *>(A->d_value), A->d_index, A->d_nnz,
+                                          A->ld, static_cast<const float *>(B->d_value), B->d_index,
+                                          B->d_nnz, B->ld, A->N, logts, rows);
+    }
+    if (!LAUNCH_OK("fnorm2_kernel"))
+        return false;
+    double ss = 0.0;
+    if (!sum_rows_to_host(c, rows, A->N, &ss))
+        return false;
+    *result = sqrt(ss);
+    return true;
+}
+
+bool ell_convert(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B)
+{
+    if (!A || !B || A->N != B->N)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "convert: matrices differ in size");
+        return false;
+    }
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(A))
+        return false;
+    if (B->mirror == MIRROR_HOST_NEWER)
+        B->mirror = MIRROR_SYNCED; // overwritten entirely below
+    int *ovf = zeroed_flag(c);
+    if (!ovf)
+        return false;
+    const int grid = rows_grid(c, A->N, 8);
+    const bool ad = A->matrix_precision == double_real, bd = B->matrix_precision == double_real;
+    if (ad && bd)
+        convert_kernel<double, double><<<grid, 256, 0, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<double *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, A->N, ovf);
+    else if (ad)
+        convert_kernel<double, float><<<grid, 256, 0, c->stream>>>(
+            static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<float *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, A->N, ovf);
+    else if (bd)
+        convert_kernel<float, double><<<grid, 256, 0, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<double *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, A->N, ovf);
+    else
+        convert_kernel<float, float><<<grid, 256, 0, c->stream>>>(
+            static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld,
+            static_cast<float *>(B->d_value), B->d_index, B->d_nnz, B->ld, B->M, A->N, ovf);
+    if (!LAUNCH_OK("convert_kernel"))
+        return false;
+    ell_mark_device(B);
+    int hov = 0;
+    if (!read_flag(c, ovf, &hov))
+        return false;
+    if (hov)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "convert: a row of A is wider than B's M=%d", B->M);
+        return false;
+    }
+    return true;
+}

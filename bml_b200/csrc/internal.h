@@ -145,6 +145,9 @@ bool ell_trace_mult(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *tr
 bool ell_transpose_new(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B);
 bool ell_copy(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B);
 bool ell_gershgorin(bml_matrix_ellpack_t *A, double *bounds);
+bool ell_sum_squares(bml_matrix_ellpack_t *A, double *result);
+bool ell_fnorm2(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *result);
+bool ell_convert(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B); // any precisions, same entries
 bool ell_import_dense(bml_matrix_ellpack_t *A, const void *dense, bml_dense_order_t order,
                       double threshold);
 bool ell_export_dense(bml_matrix_ellpack_t *A, void *dense, bml_dense_order_t order);

@@ -197,6 +197,12 @@ BML_B200_API double bml_trace_mult(bml_matrix_t *A, bml_matrix_t *B);
 /* Transpose (bml_transpose.h:9-12; bml_transpose.c:21-85). */
 BML_B200_API bml_matrix_t *bml_transpose_new(bml_matrix_t *A);
 BML_B200_API void bml_transpose(bml_matrix_t *A);
+/* Norms (bml_norm.h:8-45), ELLPACK.  bml_fnorm2 is ||A - B||_F with the
+ * reference's rule for entries of B that A lacks or holds as 0. */
+BML_B200_API double bml_sum_squares(bml_matrix_t *A);                      /* bml_norm.h:9  */
+BML_B200_API double bml_fnorm(bml_matrix_t *A);                            /* bml_norm.h:35 */
+BML_B200_API double bml_fnorm2(bml_matrix_t *A, bml_matrix_t *B);          /* bml_norm.h:39 */
+
 /* Scaling (bml_scale.h:8-17). scale_factor points to a value of A's precision. */
 BML_B200_API bml_matrix_t *bml_scale_new(void *scale_factor, bml_matrix_t *A);
 BML_B200_API void bml_scale(void *scale_factor, bml_matrix_t *A, bml_matrix_t *B);
@@ -343,6 +349,19 @@ BML_B200_API int bml_b200_ellpack_trace_noalloc(const void *d_value, const int *
  * [4] max row width seen, [5] seconds spent in X^2 calls. */
 BML_B200_API int bml_b200_sp2(bml_matrix_t *H, bml_matrix_t *D, double threshold,
     double occupation, int maxiter, double tol, int stall, double *info);
+
+/* SP2 in mixed precision (no reference counterpart).  H and D are
+ * double_real ELLPACK.  The Gershgorin bounds and X0 are formed in FP64; the
+ * first iterations (up to maxiter - nclose, with the tol/stall rules of
+ * bml_b200_sp2) run on an FP32 copy of X: FP32 products and sums in X^2, FP32
+ * adds, with the traces summed in FP64 and the branch choice and stop tests
+ * made in FP64.  The last nclose iterations run in FP64 on X converted back,
+ * as a closing refinement (they always run).  info (may be NULL) receives
+ * the eight values [0] iterations run in all, [1] stop rule of the FP32
+ * phase, [2] tr D, [3] last |t - t2|, [4] max row width, [5] seconds in all
+ * X^2 calls, [6] FP32 iterations, [7] seconds in the FP32 X^2 calls. */
+BML_B200_API int bml_b200_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold,
+    double occupation, int maxiter, double tol, int stall, int nclose, double *info);
 
 /* Synthetic Hamiltonians (host arrays in the reference ELLPACK layout), seeded
  * splitmix64 + Box-Muller, symmetric.  Used to give the oracle and this

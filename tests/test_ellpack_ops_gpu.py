@@ -208,3 +208,52 @@ def test_bad_index_rejected_without_fault():
     B.lib.bml_b200_set_verbose(1)
     B.clear_error()
     assert st == B.ERR_INVALID
+
+
+@pytest.mark.parametrize("prec", [DOUBLE, SINGLE])
+def test_norms_match_reference(oracle_mod, prec):
+    """bml_sum_squares, bml_fnorm and bml_fnorm2 against the reference (FP64
+    sums in a different order: 1e-12 relative; the reference sums FP32
+    matrices in FP32: 1e-5)."""
+    O = oracle_mod
+    v1, ix1, nz1, N, M = lattice(seed=2)
+    v2, ix2, nz2, _, _ = lattice(seed=3, radius=2)
+    # entries of B that A holds as exactly 0 count in full, as in the reference
+    v1 = v1.copy()
+    v1[::7] = 0.0
+    RA, GA = both(O, v1, ix1, nz1, N, M, prec)
+    RB, GB = both(O, v2, ix2, nz2, N, M, prec)
+    ref = O.ref()
+    for f in ("bml_sum_squares", "bml_fnorm", "bml_fnorm2"):
+        getattr(ref, f).restype = C.c_double
+    ref.bml_fnorm2.argtypes = [C.c_void_p, C.c_void_p]
+    ref.bml_sum_squares.argtypes = [C.c_void_p]
+    ref.bml_fnorm.argtypes = [C.c_void_p]
+    tol = 1e-12 if prec == DOUBLE else 1e-5
+    assert B.lib.bml_sum_squares(GA.h) == pytest.approx(ref.bml_sum_squares(RA), rel=tol)
+    assert B.lib.bml_fnorm(GA.h) == pytest.approx(ref.bml_fnorm(RA), rel=tol)
+    assert B.lib.bml_fnorm2(GA.h, GB.h) == pytest.approx(ref.bml_fnorm2(RA, RB), rel=tol)
+    assert B.lib.bml_fnorm2(GB.h, GA.h) == pytest.approx(ref.bml_fnorm2(RB, RA), rel=tol)
+    assert B.lib.bml_fnorm2(GA.h, GA.h) == 0.0
+    B.check()
+    for R in (RA, RB):
+        O.ref_free(R)
+
+
+def test_convert_between_precisions():
+    """ELLPACK to ELLPACK across precisions keeps every entry in place and
+    rounds its value to the new precision."""
+    v, ix, nz, N, M = lattice(seed=4)
+    G = B.Ellpack.from_arrays(v, ix, nz, N, M)
+    F = B.Ellpack(N, M, prec=SINGLE, handle=B.lib.bml_convert(G.h, 2, SINGLE, M, 0))
+    B.check()
+    fv, fix, fnz = F.download()
+    assert np.array_equal(fnz, nz)
+    mask = (np.arange(M)[None, :] < nz[:, None]).reshape(-1)
+    assert np.array_equal(fix[mask], ix[mask])
+    assert np.array_equal(fv[mask], v[mask].astype(np.float32))
+    D = B.Ellpack(N, M, handle=B.lib.bml_convert(F.h, 2, DOUBLE, M, 0))
+    B.check()
+    dv, dix, dnz = D.download()
+    assert np.array_equal(dnz, nz) and np.array_equal(dix[mask], ix[mask])
+    assert np.array_equal(dv[mask], fv[mask].astype(np.float64))

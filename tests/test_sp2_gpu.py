@@ -57,3 +57,45 @@ def test_sp2_overflow_stops_with_status():
     B.lib.bml_b200_set_verbose(1)
     B.clear_error()
     assert st == B.ERR_ROW_OVERFLOW and info[1] == 4
+
+
+def _padded(a, N, M, M2):
+    return np.pad(a.reshape(N, M), ((0, 0), (0, M2 - M))).reshape(-1)
+
+
+@pytest.mark.parametrize("case", ["chain", "lattice"])
+def test_sp2_mixed_against_fp64(case):
+    """Mixed precision (FP32 bulk, two closing FP64 iterations) against the
+    FP64 solve on the same input and iteration count.  Bounds for the mixed
+    path: relative trace error <= 2e-6, relative band-energy error tr(DH)
+    <= 5e-6, ||D_mixed - D_fp64||_F / ||D_fp64||_F <= 5e-5."""
+    if case == "chain":
+        N, MH, M, iters = 4096, 128, 512, 30
+        v, ix, nz = B.gen_chain(N, MH, 0)
+    else:
+        L, MH = 16, 160
+        N, M, iters = L ** 3, L ** 3, 4
+        v, ix, nz = B.gen_lattice(L, 3, N, MH, 0)
+    H = B.Ellpack.from_arrays(_padded(v, N, MH, M), _padded(ix, N, MH, M), nz, N, M)
+    D64, Dm = B.Ellpack(N, M), B.Ellpack(N, M)
+    info64, infom = (C.c_double * 6)(), (C.c_double * 8)()
+    assert B.lib.bml_b200_sp2(H.h, D64.h, 1e-5, N / 2.0, iters, -1.0, 0, info64) == B.OK
+    assert B.lib.bml_b200_sp2_mixed(H.h, Dm.h, 1e-5, N / 2.0, iters, -1.0, 0, 2, infom) == B.OK
+    assert infom[0] == iters and infom[6] == iters - 2
+    assert abs(infom[2] - info64[2]) <= 2e-6 * abs(info64[2])
+    e64 = B.lib.bml_trace_mult(D64.h, H.h)
+    em = B.lib.bml_trace_mult(Dm.h, H.h)
+    assert abs(em - e64) <= 5e-6 * abs(e64)
+    assert B.lib.bml_fnorm2(Dm.h, D64.h) <= 5e-5 * B.lib.bml_fnorm(D64.h)
+    B.check()
+
+
+def test_sp2_mixed_rejects_single_precision_input():
+    N, M = 64, 8
+    H = B.Ellpack(N, M, prec=1)
+    D = B.Ellpack(N, M, prec=1)
+    B.lib.bml_b200_set_verbose(0)
+    st = B.lib.bml_b200_sp2_mixed(H.h, D.h, 1e-5, N / 2.0, 4, -1.0, 0, 2, None)
+    B.lib.bml_b200_set_verbose(1)
+    assert st == B.ERR_INVALID
+    B.clear_error()
