@@ -169,21 +169,32 @@ def run_b200(args, rank, world, local):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):
+    # The clock sampler starts before the last warm-up step, so that its own
+    # start-up (nvidia-smi and NVML) falls outside the timed region.
+    clocks = ClockSampler(local)
+    for k in range(args.warmup):
+        if k == args.warmup - 1:
+            clocks.start()
         step()
+    if args.warmup == 0:
+        clocks.start()
     B.check(B.lib.bml_b200_synchronize())
     # X^2 roofline inputs from the last warm-up run
     x2_seconds_per_run = info[5]
     widths = info[4]
     barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
     launches0 = B.lib.bml_b200_launch_count()
     B.check(B.lib.bml_b200_event_record(0))
-    for _ in range(args.steps):
+    step_ev = []
+    for k in range(args.steps):
         step()
+        if k < 32:
+            slot = 16 + k
+            B.check(B.lib.bml_b200_event_record(slot))
+            step_ev.append(slot)
     B.check(B.lib.bml_b200_event_record(1))
     ms = B.event_ms(0, 1)
+    step_ms = [B.event_ms(a, b) for a, b in zip([0] + step_ev[:-1], step_ev)]
     launches = B.lib.bml_b200_launch_count() - launches0
     clk = clocks.stop()
     barrier()
@@ -208,9 +219,10 @@ def run_b200(args, rank, world, local):
 
     # per-X^2 roofline: one X^2 on the iterate of iteration SP2_ITERS-1
     rl = x2_roofline(B, H, info)
+    mixed = mixed_leg(B, v, ix, nz, max(3, min(args.steps, 5)))
     res = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": False,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded splitmix64 lattice Hamiltonian, generated on the host)",
         "config": {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
@@ -223,6 +235,7 @@ def run_b200(args, rank, world, local):
         "clocks": clk,
         "sp2": {"iterations": info[0], "trace": info[2], "idempotency": info[3], "max_row_width": widths,
                 "x2_seconds_per_run": x2_seconds_per_run},
+        "mixed": mixed,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res["cpu_baseline"] = cpu_baseline()
@@ -230,6 +243,69 @@ def run_b200(args, rank, world, local):
         pg.barrier()
         pg.destroy_process_group()
     return res if rank == 0 else None
+
+
+def mixed_leg(B, v, ix, nz, reps):
+    """The mixed-precision form on the same workload: the first SP2_ITERS-2
+    iterations in FP32 (FP64 traces, branch and stop tests), the last two in
+    FP64.  Timed like the main leg (CUDA events on the library stream around
+    `reps` runs), then compared with the FP64 solve: relative errors of tr D
+    and of the band energy tr(DH), ||D_mixed - D_fp64||_F / ||D_fp64||_F, and
+    the idempotency ||X^2 - X||_F of both results (X^2 thresholded at 1e-5)."""
+    import numpy as np
+    pad = lambda a: np.pad(a.reshape(N, M_H), ((0, 0), (0, M_X - M_H))).reshape(-1)
+    Hp = B.Ellpack.from_arrays(pad(v), pad(ix), nz, N, M_X)
+    nclose = 2
+
+    def timed(fn, reps):
+        fn()
+        B.check(B.lib.bml_b200_synchronize())
+        B.check(B.lib.bml_b200_event_record(4))
+        for _ in range(reps):
+            fn()
+        B.check(B.lib.bml_b200_event_record(5))
+        return B.event_ms(4, 5) / 1e3 / reps
+
+    D64, Dm = B.Ellpack(N, M_X), B.Ellpack(N, M_X)
+    i64, im = (C.c_double * 6)(), (C.c_double * 8)()
+    t64 = timed(lambda: B.check(B.lib.bml_b200_sp2(Hp.h, D64.h, THRESHOLD, OCC, SP2_ITERS, 1e-8, 0, i64)), reps)
+    tm = timed(lambda: B.check(B.lib.bml_b200_sp2_mixed(Hp.h, Dm.h, THRESHOLD, OCC, SP2_ITERS, 1e-8, 0,
+                                                        nclose, im)), reps)
+    e64 = B.lib.bml_trace_mult(D64.h, Hp.h)
+    em = B.lib.bml_trace_mult(Dm.h, Hp.h)
+    n64 = B.lib.bml_fnorm(D64.h)
+    dist = B.lib.bml_fnorm2(Dm.h, D64.h)
+    T = B.Ellpack(N, 2 * M_X)
+
+    def idem(D):
+        st, _ = B.multiply_x2(D, T, THRESHOLD)
+        B.check(st)
+        return B.lib.bml_fnorm2(T.h, D.h)
+
+    res = {"value": tm, "unit": "s", "fp64_value": t64, "speedup_vs_fp64": t64 / tm,
+           "fp32_iterations": int(im[6]), "fp64_closing_iterations": nclose,
+           "trace_rel_err": abs(im[2] - i64[2]) / abs(i64[2]),
+           "energy_trDH_rel_err": abs(em - e64) / abs(e64),
+           "density_rel_fro_err": dist / n64,
+           "idempotency_fro": {"fp64": idem(D64), "mixed": idem(Dm)},
+           "target": "mixed >= 2x faster than FP64 at <= 1e-6 relative trace/energy error"}
+    for m in (Hp, D64, Dm, T):
+        m.free()
+    return res
+
+
+def products(X, n):
+    """Product terms of X^2: P = sum_i sum_{j in row i} nnz_j."""
+    import numpy as np
+    xv, xix, xnz = X.download()
+    rows = xix.reshape(n, -1)
+    width = rows.shape[1]
+    P = 0
+    for i in range(0, n, 4096):
+        blk = rows[i:i + 4096]
+        mask = np.arange(width)[None, :] < xnz[i:i + 4096, None]
+        P += int(xnz[blk[mask]].astype(np.int64).sum())
+    return P
 
 
 def x2_roofline(B, H, info):
@@ -259,14 +335,7 @@ def x2_roofline(B, H, info):
     t = B.event_ms(2, 3) / 1e3 / reps
     nnz_x = B.lib.bml_b200_nnz(X.h)
     nnz_x2 = B.lib.bml_b200_nnz(X2.h)
-    xv, xix, xnz = X.download()
-    # product terms P = sum_i sum_{j in row i} nnz_j
-    P = 0
-    rows = xix.reshape(N, M_X)
-    for i in range(0, N, 4096):
-        blk = rows[i:i + 4096]
-        mask = np.arange(M_X)[None, :] < xnz[i:i + 4096, None]
-        P += int(xnz[blk[mask]].astype(np.int64).sum())
+    P = products(X, N)
     bytes_alg = 12 * nnz_x + 12 * nnz_x2 + 8 * N
     achieved = bytes_alg / t / 1e9
     return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
@@ -374,7 +443,9 @@ def run_profile_case():
     tr = (C.c_double * 2)()
     B.check(B.lib.bml_b200_multiply_x2(D.h, X2.h, THRESHOLD, tr))
     print(json.dumps({"profile_case": "30^3 lattice, X^2 after 3 SP2 iterations", "trace": list(tr),
-                      "tiers": B.last_tier_counts(), "width": B.lib.bml_b200_last_required_M()}))
+                      "tiers": B.last_tier_counts(), "width": B.lib.bml_b200_last_required_M(),
+                      "products": products(D, Np), "nnz_x": B.lib.bml_b200_nnz(D.h),
+                      "nnz_x2": B.lib.bml_b200_nnz(X2.h)}))
 
 
 def main():

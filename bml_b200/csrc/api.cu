@@ -1119,6 +1119,10 @@ int bml_b200_ellpack_device_arrays(bml_matrix_t *A, void **d_value, int **d_inde
         *d_nnz = E->d_nnz;
     if (ld)
         *ld = E->ld;
+    // The caller may use these arrays on any stream: finish the library's
+    // queued work on them (and their stream-ordered allocation) first.
+    if (!b200_sync())
+        return b200_get_error();
     // The caller may write through these pointers: treat the device as newer.
     ell_mark_device(E);
     return BML_B200_OK;

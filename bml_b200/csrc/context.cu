@@ -91,6 +91,18 @@ B200Context *b200_ctx()
     g_ctx.smem_optin = prop.sharedMemPerBlockOptin;
     if (!CUDA_OK(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking)))
         return nullptr;
+    // Matrices and scratch come from the device's stream-ordered pool on the
+    // library stream; the pool keeps freed memory for reuse (no release
+    // threshold), so SP2's per-call temporaries of a few GB cost neither a
+    // device synchronisation nor a trip to the driver after the first call.
+    {
+        cudaMemPool_t pool;
+        if (!CUDA_OK(cudaDeviceGetDefaultMemPool(&pool, g_ctx.device)))
+            return nullptr;
+        unsigned long long keep = ~0ull;
+        if (!CUDA_OK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)))
+            return nullptr;
+    }
     if (!CUDA_OK(cudaMallocHost(&g_ctx.pinned, 65536)))
         return nullptr;
     if (!CUDA_OK(cudaMalloc(&g_ctx.d_small, 65536)))
@@ -106,16 +118,14 @@ void *b200_scratch(size_t bytes)
         return nullptr;
     if (bytes <= c->scratch_bytes)
         return c->scratch;
-    // Grow geometrically; the old arena may still be in use by queued kernels,
-    // so drain the stream before releasing it.
-    if (!CUDA_OK(cudaStreamSynchronize(c->stream)))
-        return nullptr;
+    // Grow geometrically.  The old arena may still be in use by queued
+    // kernels: it is freed in stream order, after them.
     if (c->scratch)
-        cudaFree(c->scratch);
+        cudaFreeAsync(c->scratch, c->stream);
     c->scratch = nullptr;
     c->scratch_bytes = 0;
     size_t want = bytes + bytes / 4 + (1 << 20);
-    if (cudaMalloc(&c->scratch, want) != cudaSuccess)
+    if (cudaMallocAsync(&c->scratch, want, c->stream) != cudaSuccess)
     {
         cudaGetLastError();
         b200_set_error(BML_B200_ERR_ALLOC, "device scratch of %zu bytes", want);
@@ -223,9 +233,9 @@ void bml_shutdown(void)
     std::lock_guard<std::mutex> lock(g_ctx_mutex);
     if (!g_ctx_ready)
         return;
-    cudaStreamSynchronize(g_ctx.stream);
     if (g_ctx.scratch)
-        cudaFree(g_ctx.scratch);
+        cudaFreeAsync(g_ctx.scratch, g_ctx.stream);
+    cudaStreamSynchronize(g_ctx.stream);
     if (g_ctx.d_small)
         cudaFree(g_ctx.d_small);
     if (g_ctx.pinned)

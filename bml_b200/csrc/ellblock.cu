@@ -116,11 +116,11 @@ bml_matrix_ellblock_t *eb_alloc_blocks(bml_matrix_precision_t prec, int NB, int 
     bool ok = A->bsize && A->indexb && A->nnzb && A->ptr_value && A->h_pool;
     if (ok)
     {
-        cudaError_t e1 = cudaMalloc(&A->d_pool, eb_pool_elems(A) * sz);
-        cudaError_t e2 = cudaMalloc(reinterpret_cast<void **>(&A->d_indexb), sizeof(int) * (size_t) NB * MB);
-        cudaError_t e3 = cudaMalloc(reinterpret_cast<void **>(&A->d_nnzb), sizeof(int) * NB);
-        cudaError_t e4 = cudaMalloc(reinterpret_cast<void **>(&A->d_bsize), sizeof(int) * NB);
-        cudaError_t e5 = cudaMalloc(reinterpret_cast<void **>(&A->d_boff), sizeof(int) * (NB + 1));
+        cudaError_t e1 = cudaMallocAsync(&A->d_pool, eb_pool_elems(A) * sz, c->stream);
+        cudaError_t e2 = cudaMallocAsync(reinterpret_cast<void **>(&A->d_indexb), sizeof(int) * (size_t) NB * MB, c->stream);
+        cudaError_t e3 = cudaMallocAsync(reinterpret_cast<void **>(&A->d_nnzb), sizeof(int) * NB, c->stream);
+        cudaError_t e4 = cudaMallocAsync(reinterpret_cast<void **>(&A->d_bsize), sizeof(int) * NB, c->stream);
+        cudaError_t e5 = cudaMallocAsync(reinterpret_cast<void **>(&A->d_boff), sizeof(int) * (NB + 1), c->stream);
         if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess ||
             e5 != cudaSuccess)
         {
@@ -155,12 +155,14 @@ void eb_free(bml_matrix_ellblock_t *A)
         return;
     B200Context *c = b200_ctx();
     if (c)
-        cudaStreamSynchronize(c->stream);
-    cudaFree(A->d_pool);
-    cudaFree(A->d_indexb);
-    cudaFree(A->d_nnzb);
-    cudaFree(A->d_bsize);
-    cudaFree(A->d_boff);
+    {
+        // freed in stream order, after the kernels queued on these arrays
+        for (void *p : {static_cast<void *>(A->d_pool), static_cast<void *>(A->d_indexb),
+                        static_cast<void *>(A->d_nnzb), static_cast<void *>(A->d_bsize),
+                        static_cast<void *>(A->d_boff)})
+            if (p)
+                cudaFreeAsync(p, c->stream);
+    }
     free(A->h_pool);
     free(A->ptr_value);
     free(A->indexb);

@@ -105,9 +105,9 @@ bml_matrix_ellpack_t *ell_alloc(bml_matrix_precision_t prec, int N, int M,
     if (ok)
     {
         const size_t elems = (size_t) N * A->ld;
-        cudaError_t e1 = cudaMalloc(&A->d_value, elems * sz);
-        cudaError_t e2 = cudaMalloc(reinterpret_cast<void **>(&A->d_index), elems * sizeof(int));
-        cudaError_t e3 = cudaMalloc(reinterpret_cast<void **>(&A->d_nnz), (size_t) N * sizeof(int));
+        cudaError_t e1 = cudaMallocAsync(&A->d_value, elems * sz, c->stream);
+        cudaError_t e2 = cudaMallocAsync(reinterpret_cast<void **>(&A->d_index), elems * sizeof(int), c->stream);
+        cudaError_t e3 = cudaMallocAsync(reinterpret_cast<void **>(&A->d_nnz), (size_t) N * sizeof(int), c->stream);
         if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
         {
             cudaGetLastError();
@@ -139,13 +139,17 @@ void ell_free(bml_matrix_ellpack_t *A)
         return;
     if (A->d_value || A->d_index || A->d_nnz)
     {
-        // Kernels queued on these arrays must finish first.
+        // Freed in stream order, after the kernels queued on these arrays.
         B200Context *c = b200_ctx();
         if (c)
-            cudaStreamSynchronize(c->stream);
-        cudaFree(A->d_value);
-        cudaFree(A->d_index);
-        cudaFree(A->d_nnz);
+        {
+            if (A->d_value)
+                cudaFreeAsync(A->d_value, c->stream);
+            if (A->d_index)
+                cudaFreeAsync(A->d_index, c->stream);
+            if (A->d_nnz)
+                cudaFreeAsync(A->d_nnz, c->stream);
+        }
     }
     free(A->value);
     free(A->index);
