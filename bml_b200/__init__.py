@@ -111,6 +111,7 @@ _PROTOS = {
     "bml_b200_device_info": (_i, [_ip, _ip]),
     "bml_b200_sp2": (_i, [_vp, _vp, _d, _d, _i, _d, _i, _dp]),
     "bml_b200_sp2_mixed": (_i, [_vp, _vp, _d, _d, _i, _d, _i, _i, _dp]),
+    "bml_b200_sp2_adjoint": (_i, [_vp, _vp, _d, _d, _i, _i, _i, _vp, _dp]),
     "bml_b200_gen_chain": (_i, [_i, _i, C.c_ulonglong, _dp, _ip, _ip]),
     "bml_b200_gen_lattice": (_i, [_i, _i, _i, _i, C.c_ulonglong, _dp, _ip, _ip]),
     "bml_b200_reset_block_sizes": (None, []),

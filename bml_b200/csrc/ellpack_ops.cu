@@ -1242,3 +1242,112 @@ bool ell_convert(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B)
     }
     return true;
 }
+
+// ---------------------------------------------------------------------------
+// restrict: out takes P's pattern (P's columns, in P's order) with S's value
+// at each of those columns, 0 where S has none.  Used by the SP2 adjoint to
+// keep a gradient on the entries a thresholded product retained.  One block
+// per row; P's row is hashed (column -> position) and S's row streams past.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(256) restrict_kernel(const T *Sv, const int *Si, const int *Sn, int lds,
+                                                       const int *Pi, const int *Pn, int ldp, T *Ov,
+                                                       int *Oi, int *On, int ldo, int N, int logts)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int TS = 1 << logts;
+    const unsigned mask = TS - 1;
+    int *keys = reinterpret_cast<int *>(smem);
+    int *pos = keys + TS;
+    const int tid = threadIdx.x;
+    for (int i = blockIdx.x; i < N; i += gridDim.x)
+    {
+        for (int s = tid; s < TS; s += 256)
+            keys[s] = B200_EMPTY_KEY;
+        __syncthreads();
+        const int np = Pn[i];
+        for (int p = tid; p < np; p += 256)
+        {
+            const int k = Pi[(size_t) i * ldp + p];
+            Oi[(size_t) i * ldo + p] = k;
+            Ov[(size_t) i * ldo + p] = T(0);
+            hash_put(keys, pos, mask, k, p);
+        }
+        __syncthreads();
+        const int ns = Sn[i];
+        for (int p = tid; p < ns; p += 256)
+        {
+            const int q = hash_get(keys, pos, mask, Si[(size_t) i * lds + p]);
+            if (q >= 0)
+                Ov[(size_t) i * ldo + q] = Sv[(size_t) i * lds + p];
+        }
+        if (tid == 0)
+            On[i] = np;
+        __syncthreads();
+    }
+}
+
+} // namespace
+
+bool ell_restrict(bml_matrix_ellpack_t *S, bml_matrix_ellpack_t *P, bml_matrix_ellpack_t *O)
+{
+    if (!S || !P || !O || S->N != P->N || S->N != O->N || S->matrix_precision != O->matrix_precision)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "restrict: matrices differ in size or precision");
+        return false;
+    }
+    if (O == S)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "restrict: output aliases the source");
+        return false;
+    }
+    long long tot = 0;
+    int maxrow = 0;
+    if (!ell_nnz_total(P, &tot, &maxrow))
+        return false;
+    if (maxrow > O->M)
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "restrict: a row of the pattern has %d entries, M=%d",
+                       maxrow, O->M);
+        return false;
+    }
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(S) || !ell_to_device(P))
+        return false;
+    if (O != P && O->mirror == MIRROR_HOST_NEWER)
+        O->mirror = MIRROR_SYNCED; // overwritten entirely below
+    int logts = 5;
+    while ((1 << logts) < 2 * (maxrow > 16 ? maxrow : 16))
+        ++logts;
+    const size_t smem = (size_t) 2 * (1 << logts) * sizeof(int);
+    if (smem > c->smem_optin)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "restrict: pattern rows of %d entries are too wide", maxrow);
+        return false;
+    }
+    const int grid = max(1, min(S->N, c->sm_count * 8));
+    if (S->matrix_precision == double_real)
+    {
+        auto k = restrict_kernel<double>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 256, smem, c->stream>>>(static_cast<const double *>(S->d_value), S->d_index, S->d_nnz, S->ld,
+                                          P->d_index, P->d_nnz, P->ld, static_cast<double *>(O->d_value),
+                                          O->d_index, O->d_nnz, O->ld, S->N, logts);
+    }
+    else
+    {
+        auto k = restrict_kernel<float>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 256, smem, c->stream>>>(static_cast<const float *>(S->d_value), S->d_index, S->d_nnz, S->ld,
+                                          P->d_index, P->d_nnz, P->ld, static_cast<float *>(O->d_value),
+                                          O->d_index, O->d_nnz, O->ld, S->N, logts);
+    }
+    if (!LAUNCH_OK("restrict_kernel"))
+        return false;
+    ell_mark_device(O);
+    return true;
+}

@@ -148,6 +148,8 @@ bool ell_gershgorin(bml_matrix_ellpack_t *A, double *bounds);
 bool ell_sum_squares(bml_matrix_ellpack_t *A, double *result);
 bool ell_fnorm2(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *result);
 bool ell_convert(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B); // any precisions, same entries
+// O <- S's values on P's pattern (P's order; 0 where S lacks the column); O may be P.
+bool ell_restrict(bml_matrix_ellpack_t *S, bml_matrix_ellpack_t *P, bml_matrix_ellpack_t *O);
 bool ell_import_dense(bml_matrix_ellpack_t *A, const void *dense, bml_dense_order_t order,
                       double threshold);
 bool ell_export_dense(bml_matrix_ellpack_t *A, void *dense, bml_dense_order_t order);

@@ -363,6 +363,19 @@ BML_B200_API int bml_b200_sp2(bml_matrix_t *H, bml_matrix_t *D, double threshold
 BML_B200_API int bml_b200_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold,
     double occupation, int maxiter, double tol, int stall, int nclose, double *info);
 
+/* Density-matrix response of SP2 (no reference counterpart): the gradient of
+ * L = sum_ij D_ij V_ij with respect to the stored entries of H, where D is X
+ * after `iters` iterations of bml_b200_sp2's loop from H (fixed count, no stop
+ * test).  Thresholds and branch choices are held fixed; the Gershgorin bounds'
+ * dependence on H is included.  The forward pass keeps X every `every`
+ * iterations and recomputes the iterates in between on the way back, so at
+ * most iters/every + every iterates are held.  Iterates have M entries per
+ * row.  H, V, dH: ELLPACK of one precision and N; dH receives the gradient on
+ * H's pattern (H's order) and must be distinct from H and V.  *loss (may be
+ * NULL) receives L. */
+BML_B200_API int bml_b200_sp2_adjoint(bml_matrix_t *H, bml_matrix_t *V, double threshold,
+    double occupation, int iters, int every, int M, bml_matrix_t *dH, double *loss);
+
 /* Synthetic Hamiltonians (host arrays in the reference ELLPACK layout), seeded
  * splitmix64 + Box-Muller, symmetric.  Used to give the oracle and this
  * library byte-identical inputs.
