@@ -1,0 +1,785 @@
+// ELLBLOCK X^2 on the tcgen05 tensor cores, BF16 with a hi/lo split (mixed
+// precision; no reference counterpart: the reference multiplies blocks in the
+// matrix precision, ellblock/bml_multiply_ellblock_typed.c:246-442).
+//
+// Every 32x32 block x is split as hi = bf16(x), lo = bf16(x - hi), and
+// X^2 = sum_jb X[ib,jb] X[jb,kb] is formed as hi*hi + hi*lo + lo*hi with FP32
+// accumulation in tensor memory (lo*lo, about 2^-16 of the product, is
+// dropped).  The result is written back in the matrix precision; blocks are
+// kept as in the reference (kb == ib, or max |x| > threshold), the traces are
+// FP64 sums.
+//
+// Work: one CTA per SM, persistent over groups of four consecutive block rows
+// ib0..ib0+3, which share most of their block columns jb on a lattice.  For
+// the group, with M = 128 = 4 x 32 rows:
+//   D[kb] (128 x 32, FP32, in TMEM) += [X[ib0,jb]; ..; X[ib0+3,jb]] X[jb,kb]
+// over the union J of the rows' block columns (missing blocks are zero), for
+// every output block column kb; 16 output tiles of 32 TMEM columns are live
+// at once (a wave), so the group's outputs are made in waves.
+// Operands are staged into shared memory in the UMMA canonical K-major
+// no-swizzle layout (8-row x 16-byte core matrices).  A split kernel first
+// writes every block of X in that layout, as the left operand (rows x k) and
+// as the right operand (columns x k, the block transposed), so staging is a
+// plain 16-byte copy.  One thread issues the MMAs; completion is tracked by
+// tcgen05.commit on an mbarrier, with bounded waits.
+#include "device_util.cuh"
+#include "ellblock.h"
+
+#include <cuda_bf16.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+using namespace b200;
+
+namespace {
+
+constexpr int TB = 32;            // block size this path handles
+constexpr int TC_THREADS = 128;   // 4 warps; warp q owns TMEM lanes 32q..32q+31
+constexpr int TC_TILES = 16;      // live output tiles (16 x 32 = 512 TMEM columns)
+constexpr int TC_GROUP = 4;       // block rows per group (M = 128)
+constexpr int TC_KCAP = 4096;     // output block columns per group
+constexpr int TC_JCAP = 1024;     // union of block columns per group
+constexpr int IMG = TB * TB;      // bf16 elements per block image (2 KB)
+
+// bf16 image of a block in the K-major no-swizzle layout, as a left operand
+// (element (r, k) of the block) or a right operand (element (n, k) = block
+// (k, n)): 16-byte rows of 8 k, 8-row core matrices, row groups 128 B apart,
+// k-chunks of 8 (32 rows) 512 B apart.
+__device__ __forceinline__ int img_off(int row, int k)
+{
+    return (((k >> 3) * 4 + (row >> 3)) * 8 + (row & 7)) * 8 + (k & 7);
+}
+
+// Split every stored block of X into four images: left hi, left lo, right
+// hi, right lo, at img + slot*4*IMG.
+template <typename T>
+__global__ void tc_split_kernel(const T *pool, const int *nnzb, int NB, int MB, long long slot_elems,
+                                __nv_bfloat16 *img)
+{
+    for (long long s = blockIdx.x; s < (long long) NB * MB; s += gridDim.x)
+    {
+        const int ib = (int) (s / MB), jp = (int) (s % MB);
+        if (jp >= nnzb[ib])
+            continue;
+        const T *x = pool + s * slot_elems;
+        __nv_bfloat16 *o = img + s * 4 * IMG;
+        for (int e = threadIdx.x; e < IMG; e += blockDim.x)
+        {
+            const int r = e >> 5, c = e & 31;
+            const float v = (float) x[e];
+            const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+            const __nv_bfloat16 lo = __float2bfloat16_rn((float) ((double) x[e] - (double) __bfloat162float(hi)));
+            o[img_off(r, c)] = hi;           // left: row r, k = c
+            o[IMG + img_off(r, c)] = lo;
+            o[2 * IMG + img_off(c, r)] = hi; // right: n = c, k = r
+            o[3 * IMG + img_off(c, r)] = lo;
+        }
+    }
+}
+
+// --- tcgen05 / mbarrier primitives ---------------------------------------
+__device__ __forceinline__ unsigned su32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t smem_desc(unsigned addr, unsigned lbo, unsigned sbo)
+{
+    // start address, leading (k) and stride (row group) byte offsets in
+    // 16-byte units; version 1 (bits 46-47); no swizzle; base offset 0.
+    return (uint64_t) ((addr >> 4) & 0x3FFFu) | ((uint64_t) ((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t) ((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: D F32, A and B BF16, both K-major,
+// N = 32, M = 128.
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, unsigned accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                 ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u),
+                   "r"(0u), "r"(0u)
+                 : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init1(uint64_t *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(su32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `parity` of bar, at most about 2 s; false on timeout.
+__device__ bool mbar_wait2s(uint64_t *bar, unsigned parity)
+{
+    if (mbar_test(bar, parity))
+        return true;
+    const unsigned long long t0 = now_ns();
+    while (!mbar_test(bar, parity))
+        if (now_ns() - t0 > 2000000000ull)
+            return false;
+    return true;
+}
+
+__device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32])
+{
+    unsigned r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                   "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+                   "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+                   "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr)
+                 : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+        v[i] = __uint_as_float(r[i]);
+}
+
+// Shared memory of the X^2 kernel.
+struct TcSmem
+{
+    __nv_bfloat16 a[2][4 * IMG]; // left operand, hi and lo: 128 x 32 (8 KB each)
+    __nv_bfloat16 b[2][IMG];     // right operand, hi and lo: 32 x 32 (2 KB each)
+    uint64_t bar;
+    unsigned tmem;
+    int nJ, nK, npairs, ok;
+    int jb[TC_JCAP];             // union of the group's block columns
+    short jslot[TC_JCAP][TC_GROUP]; // position of X[ib0+q, jb] in row ib0+q, or -1
+    int jkey[2 * TC_JCAP];       // hash jb -> index in jb[]
+    int jval[2 * TC_JCAP];
+    int kkey[2 * TC_KCAP];       // hash kb -> output tile
+    int kval[2 * TC_KCAP];
+    int klist[TC_KCAP];          // kb of each output tile
+    int wstart[TC_KCAP / TC_TILES + 1]; // first pair of each wave (pairs sorted by wave)
+    unsigned char started[TC_TILES], touched[TC_TILES];
+};
+
+template <typename T> struct TcView
+{
+    const T *pool;
+    const int *indexb, *nnzb;
+    int NB, MB;
+    long long slot;
+};
+
+template <typename T> struct TcOut
+{
+    T *pool;
+    int *indexb, *nnzb;
+    int MB;
+    long long slot;
+};
+
+// Slot of key k in an open-addressing table of size 2*cap (cap a power of 2).
+__device__ __forceinline__ int tc_find(int *keys, int cap2, int k, bool &found)
+{
+    unsigned h = ((unsigned) k * 2654435761u) & (unsigned) (cap2 - 1);
+    for (int p = 0; p < cap2; ++p)
+    {
+        if (keys[h] == k)
+        {
+            found = true;
+            return (int) h;
+        }
+        if (keys[h] == B200_EMPTY_KEY)
+        {
+            found = false;
+            return (int) h;
+        }
+        h = (h + 1) & (unsigned) (cap2 - 1);
+    }
+    found = false;
+    return -1;
+}
+
+// flags: [0] row overflow, [1] widest kept row, [2] group over capacity,
+// [3] a tensor-core wait timed out
+template <typename T>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    tc_x2_kernel(TcView<T> X, TcOut<T> C, const __nv_bfloat16 *img, int2 *pairs_all, int pcap, double thr,
+                 double *dA, double *dC, int *flags)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int2 *pairs = pairs_all + (size_t) blockIdx.x * 2 * pcap; // unsorted, then sorted
+    int2 *sorted = pairs + pcap;
+    const int ngroups = (X.NB + TC_GROUP - 1) / TC_GROUP;
+
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(su32(&S.tmem))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0)
+        mbar_init1(&S.bar);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tbase = S.tmem;
+    unsigned phase = 0;
+    bool dead = false; // a wait timed out: stop issuing work
+
+    for (int grp = blockIdx.x; grp < ngroups && !dead; grp += gridDim.x)
+    {
+        const int ib0 = grp * TC_GROUP;
+        // ---- the group's block columns J, outputs K and product pairs ----
+        for (int s = tid; s < 2 * TC_JCAP; s += TC_THREADS)
+            S.jkey[s] = B200_EMPTY_KEY;
+        for (int s = tid; s < 2 * TC_KCAP; s += TC_THREADS)
+            S.kkey[s] = B200_EMPTY_KEY;
+        __syncthreads();
+        if (tid == 0)
+        {
+            int ok = 1;
+            int nJ = 0;
+            for (int q = 0; q < TC_GROUP && ok; ++q)
+            {
+                const int ib = ib0 + q;
+                if (ib >= X.NB)
+                    break;
+                for (int jp = 0; jp < X.nnzb[ib] && ok; ++jp)
+                {
+                    const int jb = X.indexb[(size_t) ib * X.MB + jp];
+                    if (jb < 0 || jb >= X.NB)
+                    {
+                        ok = 0;
+                        break;
+                    }
+                    bool f;
+                    const int h = tc_find(S.jkey, 2 * TC_JCAP, jb, f);
+                    if (h < 0 || (!f && nJ >= TC_JCAP))
+                    {
+                        ok = 0;
+                        break;
+                    }
+                    int idx;
+                    if (!f)
+                    {
+                        idx = nJ++;
+                        S.jkey[h] = jb;
+                        S.jval[h] = idx;
+                        S.jb[idx] = jb;
+                        for (int q2 = 0; q2 < TC_GROUP; ++q2)
+                            S.jslot[idx][q2] = -1;
+                    }
+                    else
+                        idx = S.jval[h];
+                    S.jslot[idx][q] = (short) jp;
+                }
+            }
+            int nK = 0, np = 0;
+            for (int j = 0; j < nJ && ok; ++j)
+            {
+                const int jb = S.jb[j];
+                for (int kp = 0; kp < X.nnzb[jb]; ++kp)
+                {
+                    const int kb = X.indexb[(size_t) jb * X.MB + kp];
+                    if (kb < 0 || kb >= X.NB)
+                    {
+                        ok = 0;
+                        break;
+                    }
+                    bool f;
+                    const int h = tc_find(S.kkey, 2 * TC_KCAP, kb, f);
+                    if (h < 0 || (!f && nK >= TC_KCAP) || np >= pcap)
+                    {
+                        ok = 0;
+                        break;
+                    }
+                    int t;
+                    if (!f)
+                    {
+                        t = nK++;
+                        S.kkey[h] = kb;
+                        S.kval[h] = t;
+                        S.klist[t] = kb;
+                    }
+                    else
+                        t = S.kval[h];
+                    pairs[np++] = make_int2(j, (t << 16) | kp);
+                }
+            }
+            // stable counting sort of the pairs by wave (tile / TC_TILES)
+            const int nW = (nK + TC_TILES - 1) / TC_TILES;
+            if (ok)
+            {
+                for (int w = 0; w <= nW; ++w)
+                    S.wstart[w] = 0;
+                for (int p = 0; p < np; ++p)
+                    S.wstart[((pairs[p].y >> 16) / TC_TILES) + 1]++;
+                for (int w = 0; w < nW; ++w)
+                    S.wstart[w + 1] += S.wstart[w];
+                for (int w = nW; w > 0; --w)
+                    S.wstart[w] = S.wstart[w - 1];
+                S.wstart[0] = 0;
+                // wstart[w + 1] runs from the start of wave w to its end,
+                // which is the start of wave w + 1
+                for (int p = 0; p < np; ++p)
+                {
+                    const int w = (pairs[p].y >> 16) / TC_TILES;
+                    sorted[S.wstart[w + 1]++] = pairs[p];
+                }
+            }
+            S.nJ = nJ;
+            S.nK = nK;
+            S.npairs = np;
+            S.ok = ok;
+            if (!ok)
+                atomicExch(&flags[2], 1);
+        }
+        __syncthreads();
+        if (!S.ok)
+            continue;
+        const int nK = S.nK;
+        const int nW = (nK + TC_TILES - 1) / TC_TILES;
+        const int myrow = ib0 + warp; // block row written by this warp
+        int kept = 0;
+        double trc = 0.0;
+
+        // ---- tr X of the group's rows (FP64, row order) ----
+        if (myrow < X.NB)
+        {
+            double s = 0.0;
+            for (int jp = 0; jp < X.nnzb[myrow]; ++jp)
+                if (X.indexb[(size_t) myrow * X.MB + jp] == myrow)
+                {
+                    const T *blk = X.pool + ((size_t) myrow * X.MB + jp) * X.slot;
+                    double v = (double) blk[lane * (TB + 1)];
+                    for (int o = 16; o; o >>= 1)
+                        v += __shfl_xor_sync(FULL, v, o);
+                    s += v;
+                }
+            if (lane == 0 && dA)
+                dA[myrow] = s;
+        }
+
+        // ---- waves of TC_TILES output tiles ----
+        for (int w = 0; w < nW && !dead; ++w)
+        {
+            const int t0 = w * TC_TILES;
+            const int nt = min(TC_TILES, nK - t0);
+            if (tid < TC_TILES)
+            {
+                S.started[tid] = 0;
+                S.touched[tid] = 0;
+            }
+            __syncthreads();
+            int curj = -1;
+            for (int p = S.wstart[w]; p < S.wstart[w + 1] && !dead; ++p)
+            {
+                const int2 pr = sorted[p];
+                const int j = pr.x, tile = (pr.y >> 16) - t0, kp = pr.y & 0xFFFF;
+                const int jb = S.jb[j];
+                if (j != curj)
+                {
+                    // left operand: X[ib0+q, jb] for q = 0..3 (zero when absent),
+                    // block q at row groups 4q..4q+3: chunk c of its image goes
+                    // to c*2048 + q*512 bytes of the tile
+                    for (int e = tid; e < 2 * 4 * 4 * 32; e += TC_THREADS)
+                    {
+                        const int part = e / 512;       // 0 hi, 1 lo
+                        const int rest = e % 512;
+                        const int q = rest / 128, c = (rest / 32) % 4, v = rest % 32; // 16-byte vectors
+                        const int jp = S.jslot[j][q];
+                        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+                        if (jp >= 0)
+                        {
+                            const uint4 *src = reinterpret_cast<const uint4 *>(
+                                img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG);
+                            val = src[c * 32 + v];
+                        }
+                        reinterpret_cast<uint4 *>(S.a[part])[c * 128 + q * 32 + v] = val;
+                    }
+                    curj = j;
+                }
+                // right operand: X[jb, kb] as (column, k)
+                for (int e = tid; e < 2 * 128; e += TC_THREADS)
+                {
+                    const int part = e / 128, v = e % 128;
+                    const uint4 *src = reinterpret_cast<const uint4 *>(
+                        img + (((size_t) jb * X.MB + kp) * 4 + 2 + part) * IMG);
+                    reinterpret_cast<uint4 *>(S.b[part])[v] = src[v];
+                }
+                proxy_fence();
+                __syncthreads();
+                if (tid == 0)
+                {
+                    tc_fence_after();
+                    const unsigned d = tbase + (unsigned) (tile * 32);
+                    const unsigned a0 = su32(S.a[0]), a1 = su32(S.a[1]);
+                    const unsigned b0 = su32(S.b[0]), b1 = su32(S.b[1]);
+                    unsigned acc = S.started[tile];
+#pragma unroll
+                    for (int ks = 0; ks < 2; ++ks)
+                    {
+                        // K = 16: two 8-wide k-chunks per step
+                        const uint64_t ah = smem_desc(a0 + ks * 2 * 2048, 2048, 128);
+                        const uint64_t al = smem_desc(a1 + ks * 2 * 2048, 2048, 128);
+                        const uint64_t bh = smem_desc(b0 + ks * 2 * 512, 512, 128);
+                        const uint64_t bl = smem_desc(b1 + ks * 2 * 512, 512, 128);
+                        umma_bf16(d, ah, bh, acc);
+                        umma_bf16(d, ah, bl, 1u);
+                        umma_bf16(d, al, bh, 1u);
+                        acc = 1u;
+                    }
+                    umma_commit(&S.bar);
+                    S.started[tile] = 1;
+                    unsigned char m = 0;
+                    for (int q = 0; q < TC_GROUP; ++q)
+                        if (S.jslot[j][q] >= 0)
+                            m |= (unsigned char) (1u << q);
+                    S.touched[tile] |= m;
+                }
+                // the operands are reused: wait for these MMAs (the block
+                // agrees on a timeout, so every thread leaves together)
+                const bool late = !mbar_wait2s(&S.bar, phase & 1);
+                ++phase;
+                tc_fence_after();
+                if (__syncthreads_or(late))
+                {
+                    if (tid == 0)
+                        atomicExch(&flags[3], 1);
+                    dead = true;
+                }
+            }
+            if (dead)
+                break;
+            // ---- epilogue: warp q reads block row ib0+q of every tile ----
+            for (int t = 0; t < nt; ++t)
+            {
+                float v[32];
+                tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32), v);
+                const int kb = S.klist[t0 + t];
+                if (myrow >= X.NB || !((S.touched[t] >> warp) & 1))
+                    continue;
+                float mx = 0.f, diag = 0.f;
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                {
+                    mx = fmaxf(mx, fabsf(v[c]));
+                    diag = c == lane ? v[c] : diag;
+                }
+                for (int o = 16; o; o >>= 1)
+                    mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+                const bool keep = kb == myrow || (double) mx > thr;
+                if (!keep)
+                    continue;
+                if (kb == myrow)
+                {
+                    double dd = (double) diag;
+                    for (int o = 16; o; o >>= 1)
+                        dd += __shfl_xor_sync(FULL, dd, o);
+                    trc += dd;
+                }
+                if (kept < C.MB)
+                {
+                    T *dst = C.pool + ((size_t) myrow * C.MB + kept) * C.slot + lane * TB;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c)
+                        dst[c] = (T) v[c];
+                    if (lane == 0)
+                        C.indexb[(size_t) myrow * C.MB + kept] = kb;
+                }
+                ++kept;
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (myrow < X.NB && lane == 0)
+        {
+            C.nnzb[myrow] = kept < C.MB ? kept : C.MB;
+            atomicMax(&flags[1], kept);
+            if (kept > C.MB)
+                atomicExch(&flags[0], 1);
+            if (dC)
+                dC[myrow] = trc;
+        }
+        __syncthreads();
+    }
+    // after a timeout, give the MMAs in flight one more bounded wait before
+    // their tensor memory is released
+    if (dead)
+        mbar_wait2s(&S.bar, (phase - 1) & 1);
+    // release the tensor memory (after every read of it)
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase) : "memory");
+}
+
+} // namespace
+
+// X2 = X*X on the tensor cores (BF16 hi/lo split, FP32 accumulation); X and
+// X2 must have blocks of 32 throughout.  Returns false with a status set
+// (UNSUPPORTED when the partition or a group's size is outside this path).
+bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, double threshold, double *trace)
+{
+    if (!X || !X2 || X == X2 || X->NB != X2->NB || X->matrix_precision != X2->matrix_precision)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "multiply_x2_tc: X and X2 must be distinct, of one partition and precision");
+        return false;
+    }
+    for (int ib = 0; ib < X->NB; ++ib)
+        if (X->bsize[ib] != TB || X2->bsize[ib] != TB)
+        {
+            b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply_x2_tc: block %d has size %d (32 needed)", ib,
+                           X->bsize[ib]);
+            return false;
+        }
+    if (X->MB > 32767)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply_x2_tc: MB=%d above 32767", X->MB);
+        return false;
+    }
+    B200Context *c = b200_ctx();
+    if (!c || !eb_to_device(X) || !eb_to_device(X2))
+        return false;
+    const int NB = X->NB, MB = X->MB;
+    const int pcap = 65536;
+    const int grid = c->sm_count;
+    const size_t n_img = (size_t) NB * MB * 4 * IMG;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t off_pairs = al(n_img * sizeof(__nv_bfloat16));
+    const size_t off_tr = al(off_pairs + (size_t) grid * 2 * pcap * sizeof(int2));
+    const size_t off_flags = al(off_tr + (size_t) 2 * NB * sizeof(double));
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_flags + 64));
+    if (!scr)
+        return false;
+    __nv_bfloat16 *img = reinterpret_cast<__nv_bfloat16 *>(scr);
+    int2 *pairs = reinterpret_cast<int2 *>(scr + off_pairs);
+    double *dA = reinterpret_cast<double *>(scr + off_tr);
+    double *dC = dA + NB;
+    int *flags = reinterpret_cast<int *>(scr + off_flags);
+    if (!CUDA_OK(cudaMemsetAsync(flags, 0, 64, c->stream)) ||
+        !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)))
+        return false;
+    const size_t smem = sizeof(TcSmem) + 1024;
+    const int sgrid = (int) min((long long) NB * MB, (long long) c->sm_count * 32);
+    if (X->matrix_precision == double_real)
+    {
+        tc_split_kernel<double><<<sgrid, 256, 0, c->stream>>>(static_cast<const double *>(X->d_pool), X->d_nnzb,
+                                                              NB, MB, X->slot_elems, img);
+        if (!LAUNCH_OK("tc_split_kernel"))
+            return false;
+        auto k = tc_x2_kernel<double>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, TC_THREADS, smem, c->stream>>>(
+            TcView<double>{static_cast<const double *>(X->d_pool), X->d_indexb, X->d_nnzb, NB, MB, X->slot_elems},
+            TcOut<double>{static_cast<double *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems},
+            img, pairs, pcap, threshold, dA, dC, flags);
+    }
+    else
+    {
+        tc_split_kernel<float><<<sgrid, 256, 0, c->stream>>>(static_cast<const float *>(X->d_pool), X->d_nnzb, NB,
+                                                             MB, X->slot_elems, img);
+        if (!LAUNCH_OK("tc_split_kernel"))
+            return false;
+        auto k = tc_x2_kernel<float>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, TC_THREADS, smem, c->stream>>>(
+            TcView<float>{static_cast<const float *>(X->d_pool), X->d_indexb, X->d_nnzb, NB, MB, X->slot_elems},
+            TcOut<float>{static_cast<float *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems},
+            img, pairs, pcap, threshold, dA, dC, flags);
+    }
+    if (!LAUNCH_OK("tc_x2_kernel"))
+        return false;
+    double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 256);
+    b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(dA, dC, NB, out);
+    if (!LAUNCH_OK("b200_sum_rows_kernel"))
+        return false;
+    unsigned char *pin = static_cast<unsigned char *>(c->pinned) + 8192;
+    if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 16, cudaMemcpyDeviceToHost, c->stream)) ||
+        !CUDA_OK(cudaMemcpyAsync(pin + 64, out, 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+        return false;
+    int hf[4];
+    memcpy(hf, pin, sizeof(hf));
+    X2->mirror = MIRROR_DEVICE_NEWER;
+    if (trace)
+        memcpy(trace, pin + 64, 2 * sizeof(double));
+    if (hf[3])
+    {
+        b200_set_error(BML_B200_ERR_TIMEOUT, "multiply_x2_tc: a tensor-core wait timed out");
+        return false;
+    }
+    if (hf[2])
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply_x2_tc: a group of block rows exceeds the kernel's capacity");
+        return false;
+    }
+    if (hf[0])
+    {
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW,
+                       "Number of non-zeroes blocks per row > MB, Increase MB (need %d, MB = %d)", hf[1], X2->MB);
+        return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int bml_b200_ellblock_multiply_x2_tc(bml_matrix_t *X, bml_matrix_t *X2, double threshold,
+                                                double *trace)
+{
+    if (bml_get_type(X) != ellblock || bml_get_type(X2) != ellblock)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ellblock_multiply_x2_tc: ELLBLOCK matrices expected");
+        return BML_B200_ERR_INVALID;
+    }
+    bml_b200_clear_error();
+    double tr[2] = {0.0, 0.0};
+    if (!eb_multiply_x2_tc(static_cast<bml_matrix_ellblock_t *>(X), static_cast<bml_matrix_ellblock_t *>(X2),
+                           threshold, tr))
+        return b200_get_error();
+    if (trace)
+    {
+        trace[0] = tr[0];
+        trace[1] = tr[1];
+    }
+    return BML_B200_OK;
+}
+
+extern "C" int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold, double occupation,
+                                           int maxiter, double tol, int stall, int nclose, double *info)
+{
+    double local[8] = {0, 4, 0, 0, 0, 0, 0, 0};
+    double *inf = info ? info : local;
+    for (int k = 0; k < 8; ++k)
+        inf[k] = local[k];
+    if (!H || !D || H == D || bml_get_type(H) != ellblock || bml_get_type(D) != ellblock ||
+        bml_get_precision(H) != bml_get_precision(D) || bml_get_N(H) != bml_get_N(D) || nclose < 0 ||
+        nclose > maxiter)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ellblock_sp2_mixed: H and D must be distinct ELLBLOCK matrices "
+                                             "of one precision and N, 0 <= nclose <= maxiter");
+        return BML_B200_ERR_INVALID;
+    }
+    bml_b200_clear_error();
+    bml_copy(H, D);
+    double *eb = static_cast<double *>(bml_gershgorin(H));
+    if (!eb || bml_b200_last_error())
+    {
+        free(eb);
+        return bml_b200_last_error();
+    }
+    bml_normalize(D, eb[0], eb[1]);
+    free(eb);
+    if (bml_b200_last_error())
+        return bml_b200_last_error();
+    bml_matrix_t *X2 = bml_zero_matrix(ellblock, bml_get_precision(D), bml_get_N(D), bml_get_M(D), sequential);
+    if (!X2)
+        return bml_b200_last_error();
+    int status = BML_B200_OK, rule = 3, it = 0, it_tc = 0, since = 0;
+    double best = HUGE_VAL, last = 0.0, x2s = 0.0, x2s_tc = 0.0;
+    for (; it < maxiter; ++it)
+    {
+        const bool closing = it >= maxiter - nclose;
+        double tr[2];
+        const auto t0 = std::chrono::steady_clock::now();
+        bool ok;
+        if (closing)
+            ok = eb_multiply_x2(static_cast<bml_matrix_ellblock_t *>(D), static_cast<bml_matrix_ellblock_t *>(X2),
+                                threshold, tr);
+        else
+            ok = eb_multiply_x2_tc(static_cast<bml_matrix_ellblock_t *>(D),
+                                   static_cast<bml_matrix_ellblock_t *>(X2), threshold, tr);
+        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        x2s += dt;
+        if (!closing)
+        {
+            x2s_tc += dt;
+            ++it_tc;
+        }
+        if (!ok)
+        {
+            status = b200_get_error();
+            rule = 4;
+            break;
+        }
+        const double t = tr[0], t2 = tr[1];
+        last = fabs(t - t2);
+        if (fabs(t2 - occupation) <= fabs(2.0 * t - t2 - occupation))
+            bml_copy(X2, D);
+        else
+            bml_add(D, X2, 2.0, -1.0, threshold);
+        if (bml_b200_last_error())
+        {
+            status = bml_b200_last_error();
+            rule = 4;
+            ++it;
+            break;
+        }
+        if (!closing && rule == 3)
+        {
+            // bulk stop rules: jump to the closing iterations
+            bool stop = last < tol;
+            if (!stop && stall > 0)
+            {
+                if (last < best)
+                {
+                    best = last;
+                    since = 0;
+                }
+                else if (++since >= stall)
+                    stop = true;
+            }
+            if (stop)
+            {
+                rule = last < tol ? 1 : 2;
+                const int remaining = maxiter - nclose - it - 1;
+                maxiter -= remaining; // the closing iterations follow now
+            }
+        }
+    }
+    bml_deallocate(&X2);
+    inf[0] = it;
+    inf[1] = rule;
+    inf[2] = status == BML_B200_OK ? bml_trace(D) : 0.0;
+    inf[3] = last;
+    inf[4] = 0;
+    inf[5] = x2s;
+    inf[6] = it_tc;
+    inf[7] = x2s_tc;
+    return status;
+}

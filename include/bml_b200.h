@@ -363,6 +363,25 @@ BML_B200_API int bml_b200_sp2(bml_matrix_t *H, bml_matrix_t *D, double threshold
 BML_B200_API int bml_b200_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold,
     double occupation, int maxiter, double tol, int stall, int nclose, double *info);
 
+/* ELLBLOCK X^2 on the tensor cores (no reference counterpart): each 32x32
+ * block x is split as hi = bf16(x), lo = bf16(x - hi) and the block products
+ * are formed as hi*hi + hi*lo + lo*hi on tcgen05 with FP32 accumulation, then
+ * written in X2's precision; blocks are kept as by bml_multiply_x2 (kb == ib
+ * or max |x| > threshold).  trace (may be NULL) receives {tr X, tr X2}.  Every
+ * block of X and X2 must be 32 x 32 (bml_set_block_sizes); otherwise
+ * UNSUPPORTED.  Blocks of a row come out in first-touch order over the four
+ * block rows the kernel handles together, not row by row. */
+BML_B200_API int bml_b200_ellblock_multiply_x2_tc(bml_matrix_t *X, bml_matrix_t *X2, double threshold,
+    double *trace);
+
+/* SP2 on ELLBLOCK matrices in mixed precision (no reference counterpart):
+ * bulk iterations use bml_b200_ellblock_multiply_x2_tc, the last nclose
+ * iterations the matrix-precision X^2 of bml_multiply_x2; adds, copies, the
+ * branch choice and the stop tests as bml_b200_sp2.  info as for
+ * bml_b200_sp2_mixed ([4] is 0). */
+BML_B200_API int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold,
+    double occupation, int maxiter, double tol, int stall, int nclose, double *info);
+
 /* Density-matrix response of SP2 (no reference counterpart): the gradient of
  * L = sum_ij D_ij V_ij with respect to the stored entries of H, where D is X
  * after `iters` iterations of bml_b200_sp2's loop from H (fixed count, no stop

@@ -1,0 +1,112 @@
+"""ELLBLOCK X^2 on the tensor cores (BF16 hi/lo split, FP32 accumulation)
+against the matrix-precision block product of bml_multiply_x2.
+
+Bounds: the split represents each entry to about 2^-17 of its size, and the
+products are summed in FP32, so entries of X^2 agree to 2e-5 of the largest
+entry and the traces to 2e-5 relative.  Blocks of 32 x 32 on a block lattice
+(entries N(0,1) exp(-d), neighbours within a radius), as in the mixed
+ELLBLOCK configuration."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import bml_b200 as B
+
+pytestmark = pytest.mark.gpu
+ELLBLOCK, DOUBLE, SINGLE = 3, 2, 1
+
+
+def block_lattice(L, radius, seed=0, bs=32):
+    """Dense symmetric matrix of L^3 blocks of bs x bs: block (a, b) nonzero
+    when the block sites are within `radius`, entries N(0,1) exp(-d)."""
+    rng = np.random.default_rng(seed)
+    nb = L ** 3
+    pos = np.array([(x, y, z) for z in range(L) for y in range(L) for x in range(L)])
+    N = nb * bs
+    H = np.zeros((N, N))
+    for a in range(nb):
+        for b in range(a, nb):
+            d = np.sqrt(((pos[a] - pos[b]) ** 2).sum())
+            if d <= radius:
+                blk = rng.standard_normal((bs, bs)) * np.exp(-d)
+                if a == b:
+                    blk = (blk + blk.T) / 2
+                H[a * bs:(a + 1) * bs, b * bs:(b + 1) * bs] = blk
+                H[b * bs:(b + 1) * bs, a * bs:(a + 1) * bs] = blk.T
+    return H
+
+
+def set_partition(nb, MB, bs=32):
+    arr = (C.c_int * nb)(*([bs] * nb))
+    B.lib.bml_b200_reset_block_sizes()
+    B.lib.bml_set_block_sizes(arr, nb, MB)
+
+
+def from_dense(D, prec=DOUBLE):
+    N = D.shape[0]
+    a = np.ascontiguousarray(D, dtype=np.float64 if prec == DOUBLE else np.float32)
+    h = B.lib.bml_import_from_dense(ELLBLOCK, prec, 0, N, N, a.ctypes.data_as(C.c_void_p), 0.0, 0)
+    B.check()
+    return h
+
+
+def to_dense(h, N, prec=DOUBLE):
+    p = B.lib.bml_export_to_dense(h, 0)
+    B.check()
+    d = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double if prec == DOUBLE else C.c_float)),
+                              shape=(N * N,)).copy()
+    B.lib.bml_free_memory(C.c_void_p(p))
+    return d.reshape(N, N).astype(np.float64)
+
+
+def free(h):
+    hh = C.c_void_p(h)
+    B.lib.bml_deallocate(C.byref(hh))
+
+
+@pytest.mark.parametrize("prec", [DOUBLE, SINGLE])
+@pytest.mark.parametrize("L,radius", [(3, 1.0), (4, 2.0)])
+def test_tc_x2_matches_block_product(prec, L, radius):
+    H = block_lattice(L, radius)
+    nb, N = L ** 3, H.shape[0]
+    set_partition(nb, nb)
+    try:
+        X = from_dense(H, prec)
+        Xe = B.lib.bml_zero_matrix(ELLBLOCK, prec, N, N, 0)
+        Xt = B.lib.bml_zero_matrix(ELLBLOCK, prec, N, N, 0)
+        B.check()
+        tre = B.lib.bml_multiply_x2(X, Xe, C.c_double(1e-6))
+        tre = np.ctypeslib.as_array(C.cast(tre, C.POINTER(C.c_double)), shape=(2,)).copy()
+        trt = (C.c_double * 2)()
+        st = B.lib.bml_b200_ellblock_multiply_x2_tc(X, Xt, 1e-6, trt)
+        assert st == B.OK, B.lib.bml_b200_error_string(st)
+        de, dt = to_dense(Xe, N, prec), to_dense(Xt, N, prec)
+        scale = np.abs(de).max()
+        assert np.abs(dt - de).max() <= 2e-5 * scale
+        assert trt[0] == pytest.approx(tre[0], rel=1e-6)
+        assert trt[1] == pytest.approx(tre[1], rel=2e-5)
+        # a second call on the same inputs gives the same result
+        st = B.lib.bml_b200_ellblock_multiply_x2_tc(X, Xt, 1e-6, trt)
+        assert st == B.OK
+        assert np.array_equal(to_dense(Xt, N, prec), dt)
+        for h in (X, Xe, Xt):
+            free(h)
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
+
+
+def test_tc_rejects_other_block_sizes():
+    set_partition(16, 16, bs=8)
+    try:
+        X = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, 128, 128, 0)
+        X2 = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, 128, 128, 0)
+        B.lib.bml_b200_set_verbose(0)
+        st = B.lib.bml_b200_ellblock_multiply_x2_tc(X, X2, 1e-6, None)
+        B.lib.bml_b200_set_verbose(1)
+        assert st == B.ERR_UNSUPPORTED
+        B.clear_error()
+        free(X)
+        free(X2)
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
