@@ -1597,3 +1597,131 @@ bool eb_multiply(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_matrix_
     eb_free(T0);
     return ok;
 }
+
+// ---------------------------------------------------------------------------
+// Synthetic ELLBLOCK Hamiltonian on a block lattice (no reference
+// counterpart): L^3 block sites (x fastest), block (a, b) present when the
+// sites are within `radius` (open boundaries), entries N(0,1) * exp(-d).
+// Symmetric: the block of (a, b), a < b, is drawn once in row a (row-major)
+// and transposed into row b; a diagonal block draws its upper triangle.
+// splitmix64 + Box-Muller as the ELLPACK generators.  The block partition
+// must already be L^3 blocks of bs (bml_set_block_sizes), MB at least the
+// number of neighbours.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Sm64
+{
+    uint64_t s;
+    uint64_t next()
+    {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return (double) (next() >> 11) * 0x1.0p-53; }
+    double normal()
+    {
+        const double u1 = 1.0 - uniform();
+        const double u2 = uniform();
+        return sqrt(-2.0 * log(u1)) * cos(6.283185307179586476925 * u2);
+    }
+};
+
+template <typename T> void fill_block_lattice(bml_matrix_ellblock_t *A, int L, double radius, uint64_t seed)
+{
+    const int bs = A->bsize[0];
+    const int R = (int) floor(radius);
+    Sm64 rng{seed};
+    T *pool = static_cast<T *>(A->h_pool);
+    for (int a = 0; a < A->NB; ++a)
+    {
+        const int ax = a % L, ay = (a / L) % L, az = a / (L * L);
+        int n = 0;
+        // neighbours in ascending index order: z, then y, then x
+        for (int dz = -R; dz <= R; ++dz)
+            for (int dy = -R; dy <= R; ++dy)
+                for (int dx = -R; dx <= R; ++dx)
+                {
+                    const int x = ax + dx, y = ay + dy, z = az + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= L || y >= L || z >= L)
+                        continue;
+                    const double d = sqrt((double) (dx * dx + dy * dy + dz * dz));
+                    if (d > radius)
+                        continue;
+                    const int b = (z * L + y) * L + x;
+                    T *blk = pool + ((size_t) a * A->MB + n) * A->slot_elems;
+                    if (b > a)
+                    {
+                        const double s = exp(-d);
+                        for (int e = 0; e < bs * bs; ++e)
+                            blk[e] = (T) (rng.normal() * s);
+                    }
+                    else if (b == a)
+                    {
+                        for (int r = 0; r < bs; ++r)
+                            for (int c = r; c < bs; ++c)
+                                blk[r * bs + c] = blk[c * bs + r] = (T) rng.normal();
+                    }
+                    else
+                    {
+                        // (b, a) was drawn in row b: find it and transpose
+                        int p = 0;
+                        while (A->indexb[(size_t) b * A->MB + p] != a)
+                            ++p;
+                        const T *src = pool + ((size_t) b * A->MB + p) * A->slot_elems;
+                        for (int r = 0; r < bs; ++r)
+                            for (int c = 0; c < bs; ++c)
+                                blk[r * bs + c] = src[c * bs + r];
+                    }
+                    A->indexb[(size_t) a * A->MB + n] = b;
+                    ++n;
+                }
+        A->nnzb[a] = n;
+    }
+}
+
+} // namespace
+
+extern "C" bml_matrix_t *bml_b200_gen_block_lattice(int L, double radius, int bs, unsigned long long seed,
+                                                    bml_matrix_precision_t prec)
+{
+    const int NB = L * L * L;
+    const int R = (int) floor(radius);
+    int span = 0;
+    for (int dz = -R; dz <= R; ++dz)
+        for (int dy = -R; dy <= R; ++dy)
+            for (int dx = -R; dx <= R; ++dx)
+                if (dx * dx + dy * dy + dz * dz <= radius * radius)
+                    ++span;
+    if (L <= 0 || bs <= 0 || bml_get_nb() != NB || bml_get_mb() < span)
+    {
+        b200_set_error(BML_B200_ERR_INVALID,
+                       "gen_block_lattice: set a partition of L^3 = %d blocks of %d with MB >= %d first", NB, bs,
+                       span);
+        return nullptr;
+    }
+    int *bsize = bml_get_block_sizes(NB * bs, NB * bs);
+    for (int ib = 0; ib < NB; ++ib)
+        if (bsize[ib] != bs)
+        {
+            b200_set_error(BML_B200_ERR_INVALID, "gen_block_lattice: block %d has size %d, not %d", ib, bsize[ib], bs);
+            return nullptr;
+        }
+    bml_matrix_ellblock_t *A = eb_alloc_blocks(prec, NB, bml_get_mb(), NB * bs, bsize, sequential);
+    if (!A)
+        return nullptr;
+    if (prec == double_real)
+        fill_block_lattice<double>(A, L, radius, seed);
+    else
+        fill_block_lattice<float>(A, L, radius, seed);
+    host_pointers(A);
+    eb_mark_host(A);
+    if (!eb_to_device(A))
+    {
+        eb_free(A);
+        return nullptr;
+    }
+    return A;
+}

@@ -407,6 +407,14 @@ BML_B200_API int bml_b200_gen_chain(int N, int M, unsigned long long seed,
 BML_B200_API int bml_b200_gen_lattice(int L, int radius, int N, int M,
     unsigned long long seed, double *value, int *index, int *nnz);
 
+/* ELLBLOCK Hamiltonian on a block lattice: L^3 block sites (x fastest),
+ * block (a, b) present when the sites are within `radius`, entries
+ * N(0,1) exp(-d), symmetric, seeded splitmix64 + Box-Muller.  The block
+ * partition must already be L^3 blocks of bs with MB at least the number of
+ * neighbours (bml_set_block_sizes).  Returns a new matrix or NULL. */
+BML_B200_API bml_matrix_t *bml_b200_gen_block_lattice(int L, double radius, int bs,
+    unsigned long long seed, bml_matrix_precision_t precision);
+
 #ifdef __cplusplus
 }
 #endif
