@@ -19,9 +19,11 @@
 // Operands are staged into shared memory in the UMMA canonical K-major
 // no-swizzle layout (8-row x 16-byte core matrices).  A split kernel first
 // writes every block of X in that layout, as the left operand (rows x k) and
-// as the right operand (columns x k, the block transposed), so staging is a
-// plain 16-byte copy.  One thread issues the MMAs; completion is tracked by
-// tcgen05.commit on an mbarrier, with bounded waits.
+// as the right operand (columns x k, the block transposed), one contiguous
+// 2 KB image each, so staging is one bulk copy (cp.async.bulk, completing on
+// an mbarrier) per block, issued by the lanes of a producer warp into a ring
+// of buffers.  One thread issues the MMAs and releases each buffer with
+// tcgen05.commit on its mbarrier; every wait is bounded.
 #include "device_util.cuh"
 #include "ellblock.h"
 
@@ -43,14 +45,23 @@ constexpr int TC_GROUP = 4;       // block rows per group (M = 128)
 constexpr int TC_KCAP = 4096;     // output block columns per group
 constexpr int TC_JCAP = 1024;     // union of block columns per group
 constexpr int IMG = TB * TB;      // bf16 elements per block image (2 KB)
+constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
+constexpr int TC_LCAP = 2048;     // product pairs per wave
+constexpr int TC_PCAP = 8192;     // product pairs per group
+constexpr int TC_ABUF = 4;        // left-operand buffers
+constexpr int TC_BBUF = 12;       // right-operand buffers (pipeline depth)
 
 // bf16 image of a block in the K-major no-swizzle layout, as a left operand
 // (element (r, k) of the block) or a right operand (element (n, k) = block
-// (k, n)): 16-byte rows of 8 k, 8-row core matrices, row groups 128 B apart,
-// k-chunks of 8 (32 rows) 512 B apart.
+// (k, n)): 16-byte rows of 8 k, 8-row core matrices of 128 bytes; the four
+// k-chunks of an 8-row group sit next to each other (LBO = 128 B) and the
+// row groups follow at SBO = 512 B, so each 32 x 32 block is one contiguous
+// 2 KB image and four blocks stack into the 128-row left operand.
+constexpr unsigned TC_LBO = 128, TC_SBO = 512;
+
 __device__ __forceinline__ int img_off(int row, int k)
 {
-    return (((k >> 3) * 4 + (row >> 3)) * 8 + (row & 7)) * 8 + (k & 7);
+    return (row >> 3) * 256 + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
 }
 
 // Split every stored block of X into four images: left hi, left lo, right
@@ -121,6 +132,21 @@ __device__ __forceinline__ void mbar_init1(uint64_t *bar)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+
+// Bulk copy global -> shared (16-byte aligned, a multiple of 16 bytes),
+// completing on bar.
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     su32(dst)),
+                 "l"(src), "r"(bytes), "r"(su32(bar))
+                 : "memory");
+}
+
 __device__ __forceinline__ bool mbar_test(uint64_t *bar, unsigned parity)
 {
     unsigned ok;
@@ -174,19 +200,28 @@ __device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32])
 // Shared memory of the X^2 kernel.
 struct TcSmem
 {
-    __nv_bfloat16 a[2][4 * IMG]; // left operand, hi and lo: 128 x 32 (8 KB each)
-    __nv_bfloat16 b[2][IMG];     // right operand, hi and lo: 32 x 32 (2 KB each)
-    uint64_t bar;
+    __nv_bfloat16 a[TC_ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
+    union
+    {
+        __nv_bfloat16 b[TC_BBUF][2][IMG]; // right operands, hi and lo: 32 x 32 (2 KB each)
+        float stage[TC_GROUP][TB][TB + 1]; // epilogue transpose (the ring is idle then)
+    };
+    uint64_t full_a[TC_ABUF], full_b[TC_BBUF]; // bulk copies landed
+    uint64_t empty_b[TC_BBUF];            // MMAs reading a B buffer (and all before) done
+    uint64_t done;                        // all MMAs of a wave done
     unsigned tmem;
-    int nJ, nK, npairs, ok;
+    int nJ, nK, npairs, ok, dead;
     int jb[TC_JCAP];             // union of the group's block columns
     short jslot[TC_JCAP][TC_GROUP]; // position of X[ib0+q, jb] in row ib0+q, or -1
-    int jkey[2 * TC_JCAP];       // hash jb -> index in jb[]
-    int jval[2 * TC_JCAP];
-    int kkey[2 * TC_KCAP];       // hash kb -> output tile
-    int kval[2 * TC_KCAP];
+    unsigned jbits[TC_NWCAP];    // the group's block columns jb (bitmap over NB)
+    int jpre[TC_NWCAP];          // J entries before each bitmap word: index = rank of jb
+    unsigned kbits[TC_NWCAP];    // output block columns of the group (bitmap over NB)
+    int kpre[TC_NWCAP];          // tiles before each bitmap word: tile = rank of kb
     int klist[TC_KCAP];          // kb of each output tile
-    int wstart[TC_KCAP / TC_TILES + 1]; // first pair of each wave (pairs sorted by wave)
+    int jcnt[TC_JCAP];           // pairs of the current wave per J entry, then their start
+    int list[TC_LCAP];           // pairs of the current wave: j << 20 | tile << 16 | kp
+    int jstart[TC_JCAP + 1];     // first pair of each J entry in ptile
+    unsigned short ptile[TC_PCAP]; // output tile of every pair (j, kp) of the group
     unsigned char started[TC_TILES], touched[TC_TILES];
 };
 
@@ -228,18 +263,57 @@ __device__ __forceinline__ int tc_find(int *keys, int cap2, int k, bool &found)
     return -1;
 }
 
+// Rank of the set bits of bits[0..nwords): pre[w] = set bits before word w,
+// list[rank] = bit position (up to cap entries), *total = bits set.  All
+// TC_THREADS threads; `scratch` holds one int per warp.
+__device__ void rank_bits(const unsigned *bits, int *pre, int *list, int cap, int nwords, int *scratch, int *total,
+                          int tid, int lane, int warp)
+{
+    const int per = (nwords + TC_THREADS - 1) / TC_THREADS;
+    const int w0 = min(tid * per, nwords), w1 = min(w0 + per, nwords);
+    int sum = 0;
+    for (int w = w0; w < w1; ++w)
+        sum += __popc(bits[w]);
+    int incl = sum;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const int y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o)
+            incl += y;
+    }
+    if (lane == 31)
+        scratch[warp] = incl;
+    __syncthreads();
+    int run = incl - sum;
+    for (int w = 0; w < warp; ++w)
+        run += scratch[w];
+    for (int w = w0; w < w1; ++w)
+    {
+        pre[w] = run;
+        unsigned b = bits[w];
+        while (b)
+        {
+            const int bt = __ffs(b) - 1;
+            b &= b - 1;
+            if (run < cap)
+                list[run] = (w << 5) + bt;
+            ++run;
+        }
+    }
+    if (tid == TC_THREADS - 1)
+        *total = run;
+}
+
 // flags: [0] row overflow, [1] widest kept row, [2] group over capacity,
 // [3] a tensor-core wait timed out
 template <typename T>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    tc_x2_kernel(TcView<T> X, TcOut<T> C, const __nv_bfloat16 *img, int2 *pairs_all, int pcap, double thr,
+    tc_x2_kernel(TcView<T> X, TcOut<T> C, const __nv_bfloat16 *img, const __nv_bfloat16 *zimg, double thr,
                  double *dA, double *dC, int *flags)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    int2 *pairs = pairs_all + (size_t) blockIdx.x * 2 * pcap; // unsorted, then sorted
-    int2 *sorted = pairs + pcap;
     const int ngroups = (X.NB + TC_GROUP - 1) / TC_GROUP;
 
     if (warp == 0)
@@ -249,128 +323,156 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0)
-        mbar_init1(&S.bar);
+    {
+        for (int i = 0; i < TC_ABUF; ++i)
+            mbar_init1(&S.full_a[i]);
+        for (int i = 0; i < TC_BBUF; ++i)
+        {
+            mbar_init1(&S.full_b[i]);
+            mbar_init1(&S.empty_b[i]);
+        }
+        mbar_init1(&S.done);
+        S.dead = 0;
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const unsigned tbase = S.tmem;
-    unsigned phase = 0;
     bool dead = false; // a wait timed out: stop issuing work
+    // pipeline counters, kept alike by the producer (thread 0) and the MMA
+    // issuer (thread 32): pairs and left operands issued so far, and the
+    // producer's view of completed MMA commits per right-operand buffer
+    unsigned gp = 0, ga = 0, nwaves = 0;
+    unsigned seen[TC_BBUF];
+    unsigned alast_b[TC_ABUF], alast_f[TC_ABUF];
+    for (int i = 0; i < TC_BBUF; ++i)
+        seen[i] = 0;
+    unsigned copied_a = 0; // left operands whose copies thread 0 issued
+    for (int i = 0; i < TC_ABUF; ++i)
+        alast_b[i] = alast_f[i] = 0;
 
     for (int grp = blockIdx.x; grp < ngroups && !dead; grp += gridDim.x)
     {
         const int ib0 = grp * TC_GROUP;
-        // ---- the group's block columns J, outputs K and product pairs ----
-        for (int s = tid; s < 2 * TC_JCAP; s += TC_THREADS)
-            S.jkey[s] = B200_EMPTY_KEY;
-        for (int s = tid; s < 2 * TC_KCAP; s += TC_THREADS)
-            S.kkey[s] = B200_EMPTY_KEY;
-        __syncthreads();
-        if (tid == 0)
+        // ---- the group's block columns J: a bitmap over NB, index = rank ----
+        const int nwords = (X.NB + 31) >> 5;
+        const int myrow = ib0 + warp; // block row of this warp (left operand q = warp)
+        for (int s2 = tid; s2 < nwords; s2 += TC_THREADS)
         {
-            int ok = 1;
-            int nJ = 0;
-            for (int q = 0; q < TC_GROUP && ok; ++q)
+            S.jbits[s2] = 0u;
+            S.kbits[s2] = 0u;
+        }
+        if (tid == 0)
+            S.ok = 1;
+        __syncthreads();
+        int bad = 0;
+        if (myrow < X.NB)
+            for (int jp = lane; jp < X.nnzb[myrow]; jp += 32)
             {
-                const int ib = ib0 + q;
-                if (ib >= X.NB)
-                    break;
-                for (int jp = 0; jp < X.nnzb[ib] && ok; ++jp)
-                {
-                    const int jb = X.indexb[(size_t) ib * X.MB + jp];
-                    if (jb < 0 || jb >= X.NB)
-                    {
-                        ok = 0;
-                        break;
-                    }
-                    bool f;
-                    const int h = tc_find(S.jkey, 2 * TC_JCAP, jb, f);
-                    if (h < 0 || (!f && nJ >= TC_JCAP))
-                    {
-                        ok = 0;
-                        break;
-                    }
-                    int idx;
-                    if (!f)
-                    {
-                        idx = nJ++;
-                        S.jkey[h] = jb;
-                        S.jval[h] = idx;
-                        S.jb[idx] = jb;
-                        for (int q2 = 0; q2 < TC_GROUP; ++q2)
-                            S.jslot[idx][q2] = -1;
-                    }
-                    else
-                        idx = S.jval[h];
-                    S.jslot[idx][q] = (short) jp;
-                }
+                const int jb = X.indexb[(size_t) myrow * X.MB + jp];
+                if (jb < 0 || jb >= X.NB)
+                    bad = 1;
+                else
+                    atomicOr(&S.jbits[jb >> 5], 1u << (jb & 31));
             }
-            int nK = 0, np = 0;
-            for (int j = 0; j < nJ && ok; ++j)
-            {
-                const int jb = S.jb[j];
-                for (int kp = 0; kp < X.nnzb[jb]; ++kp)
-                {
-                    const int kb = X.indexb[(size_t) jb * X.MB + kp];
-                    if (kb < 0 || kb >= X.NB)
-                    {
-                        ok = 0;
-                        break;
-                    }
-                    bool f;
-                    const int h = tc_find(S.kkey, 2 * TC_KCAP, kb, f);
-                    if (h < 0 || (!f && nK >= TC_KCAP) || np >= pcap)
-                    {
-                        ok = 0;
-                        break;
-                    }
-                    int t;
-                    if (!f)
-                    {
-                        t = nK++;
-                        S.kkey[h] = kb;
-                        S.kval[h] = t;
-                        S.klist[t] = kb;
-                    }
-                    else
-                        t = S.kval[h];
-                    pairs[np++] = make_int2(j, (t << 16) | kp);
-                }
-            }
-            // stable counting sort of the pairs by wave (tile / TC_TILES)
-            const int nW = (nK + TC_TILES - 1) / TC_TILES;
-            if (ok)
-            {
-                for (int w = 0; w <= nW; ++w)
-                    S.wstart[w] = 0;
-                for (int p = 0; p < np; ++p)
-                    S.wstart[((pairs[p].y >> 16) / TC_TILES) + 1]++;
-                for (int w = 0; w < nW; ++w)
-                    S.wstart[w + 1] += S.wstart[w];
-                for (int w = nW; w > 0; --w)
-                    S.wstart[w] = S.wstart[w - 1];
-                S.wstart[0] = 0;
-                // wstart[w + 1] runs from the start of wave w to its end,
-                // which is the start of wave w + 1
-                for (int p = 0; p < np; ++p)
-                {
-                    const int w = (pairs[p].y >> 16) / TC_TILES;
-                    sorted[S.wstart[w + 1]++] = pairs[p];
-                }
-            }
-            S.nJ = nJ;
-            S.nK = nK;
-            S.npairs = np;
-            S.ok = ok;
-            if (!ok)
+        if (__syncthreads_or(bad))
+        {
+            if (tid == 0)
                 atomicExch(&flags[2], 1);
+            continue;
+        }
+        rank_bits(S.jbits, S.jpre, S.jb, TC_JCAP, nwords, S.jcnt, &S.nJ, tid, lane, warp);
+        __syncthreads();
+        if (S.nJ > TC_JCAP)
+        {
+            if (tid == 0)
+                atomicExch(&flags[2], 1);
+            continue;
+        }
+        for (int j = tid; j < S.nJ; j += TC_THREADS)
+            for (int q = 0; q < TC_GROUP; ++q)
+                S.jslot[j][q] = -1;
+        __syncthreads();
+        if (myrow < X.NB)
+            for (int jp = lane; jp < X.nnzb[myrow]; jp += 32)
+            {
+                const int jb = X.indexb[(size_t) myrow * X.MB + jp];
+                const int j = S.jpre[jb >> 5] + __popc(S.jbits[jb >> 5] & ((1u << (jb & 31)) - 1u));
+                S.jslot[j][warp] = (short) jp;
+            }
+        __syncthreads();
+        const int nJ = S.nJ;
+        // ---- output block columns K: a bitmap over NB, tiles by rank ----
+        int badk = 0;
+        for (int j = warp; j < nJ && S.ok; j += TC_THREADS / 32)
+        {
+            const int jb = S.jb[j];
+            for (int kp = lane; kp < X.nnzb[jb]; kp += 32)
+            {
+                const int kb = X.indexb[(size_t) jb * X.MB + kp];
+                if (kb < 0 || kb >= X.NB)
+                    badk = 1;
+                else
+                    atomicOr(&S.kbits[kb >> 5], 1u << (kb & 31));
+            }
+        }
+        if (__syncthreads_or(badk))
+        {
+            if (tid == 0)
+                S.ok = 0;
+        }
+        __syncthreads();
+        rank_bits(S.kbits, S.kpre, S.klist, TC_KCAP, nwords, S.jcnt, &S.nK, tid, lane, warp);
+        __syncthreads();
+        if (tid == 0 && S.nK > TC_KCAP)
+            S.ok = 0;
+        __syncthreads();
+        if (warp == 0)
+        {
+            int run = 0;
+            for (int j0 = 0; j0 < nJ; j0 += 32)
+            {
+                const int j = j0 + lane;
+                const int n = j < nJ ? X.nnzb[S.jb[j]] : 0;
+                int incl = n;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o)
+                        incl += y;
+                }
+                if (j < nJ)
+                    S.jstart[j] = run + incl - n;
+                run += __shfl_sync(FULL, incl, 31);
+            }
+            if (lane == 0)
+            {
+                S.jstart[nJ] = run;
+                if (run > TC_PCAP)
+                    S.ok = 0;
+            }
         }
         __syncthreads();
         if (!S.ok)
+        {
+            if (tid == 0)
+                atomicExch(&flags[2], 1);
             continue;
+        }
+        // the output tile of every pair (j, kp), once per group
+        for (int j = warp; j < nJ; j += TC_THREADS / 32)
+        {
+            const int jb = S.jb[j];
+            for (int kp = lane; kp < X.nnzb[jb]; kp += 32)
+            {
+                const int kb = X.indexb[(size_t) jb * X.MB + kp];
+                S.ptile[S.jstart[j] + kp] =
+                    (unsigned short) (S.kpre[kb >> 5] + __popc(S.kbits[kb >> 5] & ((1u << (kb & 31)) - 1u)));
+            }
+        }
+        __syncthreads();
         const int nK = S.nK;
         const int nW = (nK + TC_TILES - 1) / TC_TILES;
-        const int myrow = ib0 + warp; // block row written by this warp
         int kept = 0;
         double trc = 0.0;
 
@@ -378,15 +480,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (myrow < X.NB)
         {
             double s = 0.0;
-            for (int jp = 0; jp < X.nnzb[myrow]; ++jp)
-                if (X.indexb[(size_t) myrow * X.MB + jp] == myrow)
+            for (int j0 = 0; j0 < X.nnzb[myrow]; j0 += 32)
+            {
+                const int jp = j0 + lane;
+                unsigned bal = __ballot_sync(FULL, jp < X.nnzb[myrow] && X.indexb[(size_t) myrow * X.MB + jp] == myrow);
+                while (bal)
                 {
-                    const T *blk = X.pool + ((size_t) myrow * X.MB + jp) * X.slot;
+                    const int d = j0 + __ffs(bal) - 1;
+                    bal &= bal - 1;
+                    const T *blk = X.pool + ((size_t) myrow * X.MB + d) * X.slot;
                     double v = (double) blk[lane * (TB + 1)];
                     for (int o = 16; o; o >>= 1)
                         v += __shfl_xor_sync(FULL, v, o);
                     s += v;
                 }
+            }
             if (lane == 0 && dA)
                 dA[myrow] = s;
         }
@@ -402,86 +510,206 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 S.touched[tid] = 0;
             }
             __syncthreads();
-            int curj = -1;
-            for (int p = S.wstart[w]; p < S.wstart[w + 1] && !dead; ++p)
+            // pairs (j, kb) of this wave, ordered by j then kp: count per j,
+            // prefix, write
+            for (int j = warp; j < nJ; j += TC_THREADS / 32)
             {
-                const int2 pr = sorted[p];
-                const int j = pr.x, tile = (pr.y >> 16) - t0, kp = pr.y & 0xFFFF;
-                const int jb = S.jb[j];
-                if (j != curj)
+                const int ps = S.jstart[j], pn = S.jstart[j + 1] - ps;
+                int cnt = 0;
+                for (int k0 = 0; k0 < pn; k0 += 32)
                 {
-                    // left operand: X[ib0+q, jb] for q = 0..3 (zero when absent),
-                    // block q at row groups 4q..4q+3: chunk c of its image goes
-                    // to c*2048 + q*512 bytes of the tile
-                    for (int e = tid; e < 2 * 4 * 4 * 32; e += TC_THREADS)
+                    const int kp = k0 + lane;
+                    bool in = false;
+                    if (kp < pn)
                     {
-                        const int part = e / 512;       // 0 hi, 1 lo
-                        const int rest = e % 512;
-                        const int q = rest / 128, c = (rest / 32) % 4, v = rest % 32; // 16-byte vectors
-                        const int jp = S.jslot[j][q];
-                        uint4 val = make_uint4(0u, 0u, 0u, 0u);
-                        if (jp >= 0)
-                        {
-                            const uint4 *src = reinterpret_cast<const uint4 *>(
-                                img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG);
-                            val = src[c * 32 + v];
-                        }
-                        reinterpret_cast<uint4 *>(S.a[part])[c * 128 + q * 32 + v] = val;
+                        const int t = S.ptile[ps + kp];
+                        in = t >= t0 && t < t0 + nt;
                     }
-                    curj = j;
+                    cnt += __popc(__ballot_sync(FULL, in));
                 }
-                // right operand: X[jb, kb] as (column, k)
-                for (int e = tid; e < 2 * 128; e += TC_THREADS)
+                if (lane == 0)
+                    S.jcnt[j] = cnt;
+            }
+            __syncthreads();
+            if (tid == 0)
+            {
+                int run = 0;
+                for (int j = 0; j < nJ; ++j)
                 {
-                    const int part = e / 128, v = e % 128;
-                    const uint4 *src = reinterpret_cast<const uint4 *>(
-                        img + (((size_t) jb * X.MB + kp) * 4 + 2 + part) * IMG);
-                    reinterpret_cast<uint4 *>(S.b[part])[v] = src[v];
+                    const int c = S.jcnt[j];
+                    S.jcnt[j] = run;
+                    run += c;
                 }
-                proxy_fence();
-                __syncthreads();
+                S.npairs = run;
+            }
+            __syncthreads();
+            const int p0 = 0, p1 = S.npairs;
+            if (p1 > TC_LCAP)
+            {
                 if (tid == 0)
+                    atomicExch(&flags[2], 1);
+                dead = true; // capacity, not a timeout: leave the group set
+                break;
+            }
+            for (int j = warp; j < nJ; j += TC_THREADS / 32)
+            {
+                const int ps = S.jstart[j], pn = S.jstart[j + 1] - ps;
+                int pos = S.jcnt[j];
+                for (int k0 = 0; k0 < pn; k0 += 32)
                 {
+                    const int kp = k0 + lane;
+                    bool in = false;
+                    int t = 0;
+                    if (kp < pn)
+                    {
+                        t = S.ptile[ps + kp];
+                        in = t >= t0 && t < t0 + nt;
+                    }
+                    const unsigned bal = __ballot_sync(FULL, in);
+                    if (in)
+                        S.list[pos + __popc(bal & lanemask_lt())] = (j << 20) | ((t - t0) << 16) | kp;
+                    pos += __popc(bal);
+                }
+            }
+            __syncthreads();
+            if (warp == 0)
+            {
+                // producer (warp 0): lane 0 waits on the ring and arms the
+                // barriers, the lanes issue one 2 KB bulk copy each
+                int curj = -1;
+                unsigned acur = 0;
+                for (int p = p0; p < p1; ++p)
+                {
+                    const int pv = S.list[p];
+                    const int j = pv >> 20, kp = pv & 0xFFFF;
+                    const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
+                    const bool switch_a = j != curj;
+                    const unsigned a = ga % TC_ABUF, fa = ga / TC_ABUF;
+                    int fail = 0;
+                    if (lane == 0)
+                    {
+                        if (f >= 1 && seen[b] < f)
+                        {
+                            if (!mbar_wait2s(&S.empty_b[b], (f - 1) & 1))
+                                fail = 1;
+                            seen[b] = f;
+                        }
+                        if (!fail && switch_a && fa >= 1)
+                        {
+                            // the last MMAs that read this buffer must be done
+                            const unsigned lb = alast_b[a], need = alast_f[a] + 1;
+                            if (seen[lb] < need)
+                            {
+                                if (!mbar_wait2s(&S.empty_b[lb], (need - 1) & 1))
+                                    fail = 1;
+                                seen[lb] = need;
+                            }
+                        }
+                        if (!fail)
+                        {
+                            if (switch_a)
+                                mbar_expect(&S.full_a[a], 2 * 4 * IMG * 2);
+                            mbar_expect(&S.full_b[b], 2 * IMG * 2);
+                        }
+                    }
+                    if (__shfl_sync(FULL, fail, 0))
+                    {
+                        if (lane == 0)
+                            S.dead = 1;
+                        break;
+                    }
+                    if (switch_a)
+                    {
+                        if (lane < 2 * TC_GROUP)
+                        {
+                            const int part = lane >> 2, q = lane & 3;
+                            const int jp = S.jslot[j][q];
+                            const __nv_bfloat16 *src =
+                                jp >= 0 ? img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG : zimg;
+                            bulk_copy(reinterpret_cast<unsigned char *>(S.a[a][part]) + q * 2048, src, IMG * 2,
+                                      &S.full_a[a]);
+                        }
+                        curj = j;
+                        acur = a;
+                        ++ga;
+                        copied_a = ga;
+                    }
+                    if (lane < 2)
+                        bulk_copy(S.b[b][lane], img + (((size_t) S.jb[j] * X.MB + kp) * 4 + 2 + lane) * IMG, IMG * 2,
+                                  &S.full_b[b]);
+                    alast_b[acur] = b;
+                    alast_f[acur] = f;
+                    ++gp;
+                }
+            }
+            else if (tid == 32)
+            {
+                // MMA issuer: the same sequence, consuming the ring
+                int curj = -1;
+                unsigned acur = 0;
+                for (int p = p0; p < p1 && !*reinterpret_cast<volatile int *>(&S.dead); ++p)
+                {
+                    const int pv = S.list[p];
+                    const int j = pv >> 20, tile = (pv >> 16) & 15;
+                    const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
+                    if (j != curj)
+                    {
+                        acur = ga % TC_ABUF;
+                        if (!mbar_wait2s(&S.full_a[acur], (ga / TC_ABUF) & 1))
+                        {
+                            S.dead = 1;
+                            break;
+                        }
+                        curj = j;
+                        ++ga;
+                    }
+                    if (!mbar_wait2s(&S.full_b[b], f & 1))
+                    {
+                        S.dead = 1;
+                        break;
+                    }
                     tc_fence_after();
                     const unsigned d = tbase + (unsigned) (tile * 32);
-                    const unsigned a0 = su32(S.a[0]), a1 = su32(S.a[1]);
-                    const unsigned b0 = su32(S.b[0]), b1 = su32(S.b[1]);
+                    const unsigned a0 = su32(S.a[acur][0]), a1 = su32(S.a[acur][1]);
+                    const unsigned b0 = su32(S.b[b][0]), b1 = su32(S.b[b][1]);
                     unsigned acc = S.started[tile];
 #pragma unroll
                     for (int ks = 0; ks < 2; ++ks)
                     {
                         // K = 16: two 8-wide k-chunks per step
-                        const uint64_t ah = smem_desc(a0 + ks * 2 * 2048, 2048, 128);
-                        const uint64_t al = smem_desc(a1 + ks * 2 * 2048, 2048, 128);
-                        const uint64_t bh = smem_desc(b0 + ks * 2 * 512, 512, 128);
-                        const uint64_t bl = smem_desc(b1 + ks * 2 * 512, 512, 128);
+                        const uint64_t ah = smem_desc(a0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
+                        const uint64_t al = smem_desc(a1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
+                        const uint64_t bh = smem_desc(b0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
+                        const uint64_t bl = smem_desc(b1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
                         umma_bf16(d, ah, bh, acc);
                         umma_bf16(d, ah, bl, 1u);
                         umma_bf16(d, al, bh, 1u);
                         acc = 1u;
                     }
-                    umma_commit(&S.bar);
+                    umma_commit(&S.empty_b[b]);
                     S.started[tile] = 1;
                     unsigned char m = 0;
                     for (int q = 0; q < TC_GROUP; ++q)
                         if (S.jslot[j][q] >= 0)
                             m |= (unsigned char) (1u << q);
                     S.touched[tile] |= m;
+                    ++gp;
                 }
-                // the operands are reused: wait for these MMAs (the block
-                // agrees on a timeout, so every thread leaves together)
-                const bool late = !mbar_wait2s(&S.bar, phase & 1);
-                ++phase;
-                tc_fence_after();
-                if (__syncthreads_or(late))
-                {
-                    if (tid == 0)
-                        atomicExch(&flags[3], 1);
-                    dead = true;
-                }
+                // every MMA of the wave (and before) done -> done barrier
+                umma_commit(&S.done);
             }
-            if (dead)
+            // the producer's and issuer's counters must stay alike: both
+            // walked every pair of the wave unless the wave died
+            const bool late = !mbar_wait2s(&S.done, nwaves & 1);
+            ++nwaves;
+            tc_fence_after();
+            if (__syncthreads_or(late || *reinterpret_cast<volatile int *>(&S.dead)))
+            {
+                if (tid == 0)
+                    atomicExch(&flags[3], 1);
+                dead = true;
                 break;
+            }
             // ---- epilogue: warp q reads block row ib0+q of every tile ----
             for (int t = 0; t < nt; ++t)
             {
@@ -511,15 +739,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 if (kept < C.MB)
                 {
-                    T *dst = C.pool + ((size_t) myrow * C.MB + kept) * C.slot + lane * TB;
+                    // lane = block row; through shared memory so that the
+                    // warp writes the row-major block in contiguous runs
 #pragma unroll
                     for (int c = 0; c < 32; ++c)
-                        dst[c] = (T) v[c];
+                        S.stage[warp][lane][c] = v[c];
+                    __syncwarp();
+                    T *dst = C.pool + ((size_t) myrow * C.MB + kept) * C.slot;
+#pragma unroll 4
+                    for (int r = 0; r < 32; ++r)
+                        dst[r * TB + lane] = (T) S.stage[warp][r][lane];
+                    __syncwarp();
                     if (lane == 0)
                         C.indexb[(size_t) myrow * C.MB + kept] = kb;
                 }
                 ++kept;
             }
+            // the transpose area is the copy ring: order these generic writes
+            // before the next wave's bulk copies
+            proxy_fence();
             tc_fence_before();
             __syncthreads();
         }
@@ -536,8 +774,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     // after a timeout, give the MMAs in flight one more bounded wait before
     // their tensor memory is released
-    if (dead)
-        mbar_wait2s(&S.bar, (phase - 1) & 1);
+    if (dead && tid == 32)
+    {
+        umma_commit(&S.done);
+        mbar_wait2s(&S.done, nwaves & 1);
+    }
+    if (dead && tid == 0)
+    {
+        // bulk copies still in flight land before the CTA leaves: the last
+        // fill of every buffer (bounded waits)
+        for (unsigned b = 0; b < TC_BBUF && b < gp; ++b)
+        {
+            const unsigned last = (gp - 1 - b) / TC_BBUF; // fill index of buffer (gp-1-b) % TC_BBUF
+            mbar_wait2s(&S.full_b[(gp - 1 - b) % TC_BBUF], last & 1);
+        }
+        for (unsigned a = 0; a < TC_ABUF && a < copied_a; ++a)
+            mbar_wait2s(&S.full_a[(copied_a - 1 - a) % TC_ABUF], ((copied_a - 1 - a) / TC_ABUF) & 1);
+    }
     // release the tensor memory (after every read of it)
     tc_fence_before();
     __syncthreads();
@@ -565,6 +818,11 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
                            X->bsize[ib]);
             return false;
         }
+    if (X->NB > TC_NWCAP * 32)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply_x2_tc: NB=%d above %d", X->NB, TC_NWCAP * 32);
+        return false;
+    }
     if (X->MB > 32767)
     {
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply_x2_tc: MB=%d above 32767", X->MB);
@@ -574,22 +832,22 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     if (!c || !eb_to_device(X) || !eb_to_device(X2))
         return false;
     const int NB = X->NB, MB = X->MB;
-    const int pcap = 65536;
     const int grid = c->sm_count;
     const size_t n_img = (size_t) NB * MB * 4 * IMG;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    const size_t off_pairs = al(n_img * sizeof(__nv_bfloat16));
-    const size_t off_tr = al(off_pairs + (size_t) grid * 2 * pcap * sizeof(int2));
+    const size_t off_tr = al(n_img * sizeof(__nv_bfloat16));
     const size_t off_flags = al(off_tr + (size_t) 2 * NB * sizeof(double));
-    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_flags + 64));
+    const size_t off_zero = al(off_flags + 64);
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_zero + IMG * sizeof(__nv_bfloat16)));
     if (!scr)
         return false;
     __nv_bfloat16 *img = reinterpret_cast<__nv_bfloat16 *>(scr);
-    int2 *pairs = reinterpret_cast<int2 *>(scr + off_pairs);
     double *dA = reinterpret_cast<double *>(scr + off_tr);
     double *dC = dA + NB;
     int *flags = reinterpret_cast<int *>(scr + off_flags);
+    __nv_bfloat16 *zimg = reinterpret_cast<__nv_bfloat16 *>(scr + off_zero);
     if (!CUDA_OK(cudaMemsetAsync(flags, 0, 64, c->stream)) ||
+        !CUDA_OK(cudaMemsetAsync(zimg, 0, IMG * sizeof(__nv_bfloat16), c->stream)) ||
         !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)))
         return false;
     const size_t smem = sizeof(TcSmem) + 1024;
@@ -606,7 +864,7 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
         k<<<grid, TC_THREADS, smem, c->stream>>>(
             TcView<double>{static_cast<const double *>(X->d_pool), X->d_indexb, X->d_nnzb, NB, MB, X->slot_elems},
             TcOut<double>{static_cast<double *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems},
-            img, pairs, pcap, threshold, dA, dC, flags);
+            img, zimg, threshold, dA, dC, flags);
     }
     else
     {
@@ -620,7 +878,7 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
         k<<<grid, TC_THREADS, smem, c->stream>>>(
             TcView<float>{static_cast<const float *>(X->d_pool), X->d_indexb, X->d_nnzb, NB, MB, X->slot_elems},
             TcOut<float>{static_cast<float *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems},
-            img, pairs, pcap, threshold, dA, dC, flags);
+            img, zimg, threshold, dA, dC, flags);
     }
     if (!LAUNCH_OK("tc_x2_kernel"))
         return false;
