@@ -642,8 +642,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     ++gp;
                 }
             }
-            else if (tid == 32)
+            else if (warp == 1)
             {
+              if (lane == 0)
+              {
                 // MMA issuer: the same sequence, consuming the ring
                 int curj = -1;
                 unsigned acur = 0;
@@ -697,6 +699,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 // every MMA of the wave (and before) done -> done barrier
                 umma_commit(&S.done);
+              }
+              // the other lanes wait here, not in a polling loop beside the
+              // issuing lane
+              __syncwarp();
             }
             // the producer's and issuer's counters must stay alike: both
             // walked every pair of the wave unless the wave died
