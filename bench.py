@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-tc", action="store_true",
+                    help="run the small tensor-core ELLBLOCK case for an ncu capture (10^3 block lattice)")
+    ap.add_argument("--no-ellblock", action="store_true", help="skip the ELLBLOCK tensor-core leg")
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: 30^3 lattice, 3 SP2 iterations then one X^2")
     return ap.parse_args()
@@ -220,6 +223,7 @@ def run_b200(args, rank, world, local):
     # per-X^2 roofline: one X^2 on the iterate of iteration SP2_ITERS-1
     rl = x2_roofline(B, H, info)
     mixed = mixed_leg(B, v, ix, nz, max(3, min(args.steps, 5)))
+    ellb = None if args.no_ellblock else ellblock_leg()
     res = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms, "higher_is_better": False,
@@ -236,6 +240,7 @@ def run_b200(args, rank, world, local):
         "sp2": {"iterations": info[0], "trace": info[2], "idempotency": info[3], "max_row_width": widths,
                 "x2_seconds_per_run": x2_seconds_per_run},
         "mixed": mixed,
+        "ellblock_tc": ellb,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res["cpu_baseline"] = cpu_baseline()
@@ -448,11 +453,99 @@ def run_profile_case():
                       "nnz_x2": B.lib.bml_b200_nnz(X2.h)}))
 
 
+class _StdoutToStderr:
+    """Route the process's stdout (fd 1) to stderr while the library prints
+    its partition messages (bml_set_block_sizes prints, as the reference
+    does), so that stdout keeps exactly one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        C.CDLL(None).fflush(None)
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
+def ellblock_case(L):
+    """H on the L^3 block lattice of 32x32 blocks (radius 2, N(0,1) exp(-d)
+    entries, seed 0) with MB = 257 (room for X^2's radius-4 block rows)."""
+    import bml_b200 as B
+    nb = L ** 3
+    arr = (C.c_int * nb)(*([32] * nb))
+    with _StdoutToStderr():
+        B.lib.bml_b200_reset_block_sizes()
+        B.lib.bml_set_block_sizes(arr, nb, 257)
+        H = B.lib.bml_b200_gen_block_lattice(L, 2.0, 32, SEED, 2)
+    B.check()
+    return H, nb * 32
+
+
+def run_profile_tc():
+    """Three tensor-core X^2 calls on the 10^3 block lattice (N = 32000)."""
+    import bml_b200 as B
+    H, n = ellblock_case(10)
+    X2 = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    tr = (C.c_double * 2)()
+    for _ in range(3):
+        B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, X2, 1e-6, tr))
+    print(json.dumps({"profile_case": "10^3 block lattice, tensor-core X^2", "trace": list(tr)}))
+
+
+def ellblock_leg(reps=3):
+    """The mixed ELLBLOCK configuration's product: X^2 of H on the 16^3 block
+    lattice (4096 block rows of 32, N = 131072, threshold 1e-6), on the
+    tensor cores (BF16 hi/lo split) against the FP64 block product, device
+    times by CUDA events and the tensor-core result's trace error."""
+    import bml_b200 as B
+    H, n = ellblock_case(16)
+    Xe = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    Xt = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    B.check()
+    tr = (C.c_double * 2)()
+
+    def timed(fn):
+        fn()
+        B.check(B.lib.bml_b200_synchronize())
+        B.check(B.lib.bml_b200_event_record(6))
+        for _ in range(reps):
+            fn()
+        B.check(B.lib.bml_b200_event_record(7))
+        return B.event_ms(6, 7) / 1e3 / reps
+
+    def exact():
+        p = B.lib.bml_multiply_x2(H, Xe, C.c_double(1e-6))
+        B.lib.bml_free_memory(C.c_void_p(p))
+        B.check()
+
+    te = timed(exact)
+    tt = timed(lambda: B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, Xt, 1e-6, tr)))
+    tre, trt = B.lib.bml_trace(Xe), B.lib.bml_trace(Xt)
+    nnz_h = B.lib.bml_b200_nnz(H)
+    res = {"workload": "X^2 of H, 16^3 block lattice, 4096 block rows of 32x32 (N=131072), radius 2, thr 1e-6",
+           "tc_s": tt, "fp64_s": te, "speedup": te / tt, "trace_rel_err": abs(trt - tre) / abs(tre),
+           "nnz_h": int(nnz_h), "nnz_x2": int(B.lib.bml_b200_nnz(Xt)),
+           "method": "tcgen05 kind::f16 BF16 hi*hi + hi*lo + lo*hi, FP32 accumulation in TMEM"}
+    for h in (H, Xe, Xt):
+        hh = C.c_void_p(h)
+        B.lib.bml_deallocate(C.byref(hh))
+    B.lib.bml_b200_reset_block_sizes()
+    return res
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.profile:
         run_profile_case()
+        return
+    if args.profile_tc:
+        run_profile_tc()
         return
     if args.impl == "reference":
         res = run_reference(args, rank, world)
