@@ -13,12 +13,13 @@ entries; the stop rule |tr X - tr X^2| < 1e-8 is not reached within them.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Under torchrun (N > 1) each rank runs an independent replica on its own GPU
-(the path does not shard across GPUs here); rank 0 prints one JSON line with
-the slowest rank's time.  `value` is seconds per SP2 run for the whole job
-(device time of K steps on every rank / (N*K) runs).  `e2e` is the same
-metric through the C ABI with host buffers: H uploaded from host arrays and
-the density matrix downloaded every step.  --impl reference runs the reference
+Under torchrun (N > 1) one solve is split over the ranks (bml_b200/sharded.py):
+each rank forms its block of rows of X^2, the partial traces are summed, and
+the new iterate's rows are all-gathered over NCCL after every iteration;
+rank 0 prints one JSON line with the slowest rank's time (strong scaling).
+`value` is seconds per SP2 solve.  `e2e` is the same metric through the C ABI
+with host buffers: H uploaded from host arrays and the density matrix
+downloaded every step.  --impl reference runs the reference
 bml CPU library (built from its sources into oracle/_ref) on the host cores
 with the same inputs and loop.
 """
@@ -161,7 +162,21 @@ def run_b200(args, rank, world, local):
     o_ix = torch.empty(N * M_X, dtype=torch.int32).pin_memory().numpy()
     o_nz = torch.empty(N, dtype=torch.int32).pin_memory().numpy()
 
+    sharded = None
+    if world > 1:
+        # One solve split over the ranks: each forms its rows of X^2, the
+        # traces are summed and the new iterate's rows all-gathered (NCCL).
+        from bml_b200.sharded import GpuOps, ShardedSP2
+        ops = GpuOps(B.lib, H.h, M_X, THRESHOLD, pg, torch)
+        sharded = ShardedSP2(ops, pg, rank, world)
+
     def step():
+        if sharded is not None:
+            t0 = time.perf_counter()
+            res = sharded.run(OCC, SP2_ITERS, 1e-8, 0)
+            info[0], info[1], info[2], info[3] = res["iterations"], res["rule"], res["trace"], res["idempotency"]
+            info[5] = time.perf_counter() - t0
+            return
         st = B.lib.bml_b200_sp2(H.h, D.h, THRESHOLD, OCC, SP2_ITERS, 1e-8, 0, info)
         B.check(st)
 
@@ -207,7 +222,7 @@ def run_b200(args, rank, world, local):
     barrier()
     ms = max_over_ranks(ms)
     sec_per_step = ms / 1e3 / args.steps
-    value = sec_per_step / world  # whole job: world replicas run concurrently
+    value = sec_per_step  # one solve, split over the ranks when world > 1
 
     # end-to-end through the C ABI with host buffers
     barrier()
@@ -217,24 +232,27 @@ def run_b200(args, rank, world, local):
                                              h_ix.ctypes.data_as(C.POINTER(C.c_int)),
                                              h_nz.ctypes.data_as(C.POINTER(C.c_int))))
         step()
-        B.check(B.lib.bml_b200_ellpack_download(D.h, o_v.ctypes.data_as(C.c_void_p),
+        B.check(B.lib.bml_b200_ellpack_download(ops.X if sharded is not None else D.h,
+                                               o_v.ctypes.data_as(C.c_void_p),
                                                o_ix.ctypes.data_as(C.POINTER(C.c_int)),
                                                o_nz.ctypes.data_as(C.POINTER(C.c_int))))
     e2e_steps = max(1, min(args.steps, 3))
     e2e = (time.perf_counter() - t0) / e2e_steps
-    e2e = max_over_ranks(e2e) / world
+    e2e = max_over_ranks(e2e)
 
     # per-X^2 roofline: one X^2 on the iterate of iteration SP2_ITERS-1
     rl = x2_roofline(B, H, info)
-    mixed = mixed_leg(B, v, ix, nz, max(3, min(args.steps, 5)))
-    ellb = None if args.no_ellblock else ellblock_leg()
+    # the single-GPU legs (mixed precision, ELLBLOCK tensor cores) run only
+    # without the sharded solve
+    mixed = mixed_leg(B, v, ix, nz, max(3, min(args.steps, 5))) if world == 1 else None
+    ellb = None if (args.no_ellblock or world > 1) else ellblock_leg()
     res = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded splitmix64 lattice Hamiltonian, generated on the host)",
         "config": {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
-                   "sp2_iterations": SP2_ITERS, "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "sp2_iterations": SP2_ITERS, "parallelism": ("rows sharded over %d GPUs (NCCL all-gather of the iterate)" % world) if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (iterates ~0.8-1.3 GB)"},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(v.nbytes + ix.nbytes + nz.nbytes),
                 "d2h_bytes_per_step": int(o_v.nbytes + o_ix.nbytes + o_nz.nbytes)},

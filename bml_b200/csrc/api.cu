@@ -620,6 +620,55 @@ int bml_b200_multiply_x2(bml_matrix_t *X, bml_matrix_t *X2, double threshold, do
 
 int bml_b200_last_required_M(void) { return g_required_M; }
 
+// Rows [r0, r1) of X^2 (row-sharded SP2): the other rows of X2 are left as
+// they are; the traces are those rows' partial sums.
+int bml_b200_multiply_x2_rows(bml_matrix_t *X, bml_matrix_t *X2, double threshold, int r0, int r1,
+                              double *trace)
+{
+    bml_matrix_ellpack_t *EX = as_ell(X, "multiply_x2_rows"), *E2 = as_ell(X2, "multiply_x2_rows");
+    if (!EX || !E2)
+        return b200_get_error();
+    if (EX == E2 || EX->N != E2->N || r0 < 0 || r1 > EX->N || r0 >= r1)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "multiply_x2_rows: rows [%d, %d) of N=%d", r0, r1, EX->N);
+        return BML_B200_ERR_INVALID;
+    }
+    if (!ell_to_device(EX) || !ell_to_device(E2))
+        return b200_get_error();
+    bml_matrix_ellpack_t A = ell_row_view(EX, r0, r1), C = ell_row_view(E2, r0, r1);
+    double tr[2] = {0.0, 0.0};
+    const bool ok = ell_multiply_AB(&A, EX, &C, threshold, tr, &g_required_M, 1);
+    ell_mark_device(E2);
+    if (trace)
+    {
+        trace[0] = tr[0];
+        trace[1] = tr[1];
+    }
+    return ok ? BML_B200_OK : b200_get_error();
+}
+
+// SP2 update of rows [r0, r1): X <- X2 (branch 0) or X <- 2X - X2 (branch 1,
+// thresholded as bml_add).
+int bml_b200_sp2_update_rows(bml_matrix_t *X, bml_matrix_t *X2, double threshold, int branch, int r0, int r1)
+{
+    bml_matrix_ellpack_t *EX = as_ell(X, "sp2_update_rows"), *E2 = as_ell(X2, "sp2_update_rows");
+    if (!EX || !E2)
+        return b200_get_error();
+    if (EX == E2 || EX->N != E2->N || r0 < 0 || r1 > EX->N || r0 >= r1 || (branch != 0 && branch != 1))
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "sp2_update_rows: rows [%d, %d) of N=%d, branch %d", r0, r1,
+                       EX->N, branch);
+        return BML_B200_ERR_INVALID;
+    }
+    if (!ell_to_device(EX) || !ell_to_device(E2))
+        return b200_get_error();
+    bml_b200_clear_error();
+    bml_matrix_ellpack_t A = ell_row_view(EX, r0, r1), B = ell_row_view(E2, r0, r1);
+    const bool ok = branch == 0 ? ell_copy(&B, &A) : ell_add(&A, &B, 2.0, -1.0, threshold);
+    ell_mark_device(EX);
+    return ok ? BML_B200_OK : b200_get_error();
+}
+
 void *bml_multiply_x2(bml_matrix_t *X, bml_matrix_t *X2, double threshold)
 {
     double *trace = static_cast<double *>(bml_allocate_memory(2 * sizeof(double)));

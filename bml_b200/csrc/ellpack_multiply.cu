@@ -2124,8 +2124,10 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
 
 } // namespace
 
+// x2_rows: A is a row view of B (rows of X^2): report overflow as X^2 does,
+// on the thresholded width only.
 bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C,
-                     double threshold, double *trace, int *required_M)
+                     double threshold, double *trace, int *required_M, int x2_rows)
 {
     if (!A || !B || !C)
     {
@@ -2156,7 +2158,7 @@ bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matri
     g.Bv = B->d_value; g.Bi = B->d_index; g.Bn = B->d_nnz; g.ldb = B->ld; g.NB = B->N;
     g.Cv = C->d_value; g.Ci = C->d_index; g.Cn = C->d_nnz; g.ldc = C->ld; g.Mc = C->M;
     g.thr = threshold;
-    g.check_pre = (A != B) ? 1 : 0;
+    g.check_pre = (A != B && !x2_rows) ? 1 : 0;
     // Column indices of B address columns of the product: at most max(B->N, C->N).
     const int ncols = B->N > C->N ? B->N : C->N;
     bool ok = A->matrix_precision == double_real

@@ -133,7 +133,10 @@ void b200_free_domain(bml_domain_t *D);
 // {sum of A's diagonal entries, sum of C's diagonal entries}.
 bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B,
                      bml_matrix_ellpack_t *C, double threshold, double *trace,
-                     int *required_M);
+                     int *required_M, int x2_rows = 0);
+// A view of rows [r0, r1) of A: the same storage, N = r1 - r0 (columns keep
+// their global numbering).  Operations on the view touch only those rows.
+bml_matrix_ellpack_t ell_row_view(const bml_matrix_ellpack_t *A, int r0, int r1);
 bool ell_add(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double alpha,
              double beta, double threshold);
 bool ell_add_identity(bml_matrix_ellpack_t *A, double beta, double threshold);

@@ -477,3 +477,17 @@ bml_matrix_ellpack_t *ell_constructor(int kind, bml_matrix_precision_t prec, int
     }
     return A;
 }
+
+bml_matrix_ellpack_t ell_row_view(const bml_matrix_ellpack_t *A, int r0, int r1)
+{
+    bml_matrix_ellpack_t V = *A;
+    const size_t sz = prec_size(A->matrix_precision);
+    V.N = r1 - r0;
+    V.d_value = static_cast<unsigned char *>(A->d_value) + (size_t) r0 * A->ld * sz;
+    V.d_index = A->d_index + (size_t) r0 * A->ld;
+    V.d_nnz = A->d_nnz + r0;
+    V.value = static_cast<unsigned char *>(A->value) + (size_t) r0 * A->M * sz;
+    V.index = A->index + (size_t) r0 * A->M;
+    V.nnz = A->nnz + r0;
+    return V;
+}

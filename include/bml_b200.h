@@ -272,6 +272,19 @@ BML_B200_API int bml_b200_multiply_x2(bml_matrix_t *X, bml_matrix_t *X2,
  * truncation to M (lets a caller size M exactly after ROW_OVERFLOW). */
 BML_B200_API int bml_b200_last_required_M(void);
 
+/* Row-sharded SP2 (no reference counterpart; the reference distributes rows
+ * over MPI ranks).  bml_b200_multiply_x2_rows forms rows [r0, r1) of X^2
+ * from all of X (X2's other rows are left as they are; overflow is reported
+ * on the thresholded width as for X^2) and returns those rows' partial
+ * traces.  bml_b200_sp2_update_rows applies the SP2 step to rows [r0, r1):
+ * X <- X2 (branch 0) or X <- 2X - X2 thresholded (branch 1).  A caller on
+ * several GPUs sums the partial traces over ranks, chooses the branch, then
+ * gathers every rank's rows of X before the next X^2. */
+BML_B200_API int bml_b200_multiply_x2_rows(bml_matrix_t *X, bml_matrix_t *X2, double threshold,
+    int r0, int r1, double *trace);
+BML_B200_API int bml_b200_sp2_update_rows(bml_matrix_t *X, bml_matrix_t *X2, double threshold,
+    int branch, int r0, int r1);
+
 /* Diagnostics of the last ELLPACK multiply: rows per kernel tier, in the
  * order A (one warp, 1024-slot table), W8, B1 (four warps, 2048 slots,
  * TMA-staged rows), W16 (8/16 warps per row, each warp owning a share of the
