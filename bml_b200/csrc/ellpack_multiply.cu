@@ -83,6 +83,9 @@ struct MulArgs
 #ifndef B200_C_BLOCKS
 #define B200_C_BLOCKS 8
 #endif
+#ifndef B200_DENSE_BITS
+#define B200_DENSE_BITS 1
+#endif
 constexpr int NTIERS = 7;
 constexpr int TIER_W8 = 1, TIER_B1 = 2, TIER_W16 = 3, TIER_K4 = 4, TIER_K8 = 5, TIER_C = NTIERS - 1;
 constexpr int BUCKET_TIERS_MASK = (1 << TIER_W8) | (1 << TIER_W16) | (1 << TIER_K4) | (1 << TIER_K8);
@@ -1664,10 +1667,13 @@ __global__ void __launch_bounds__(KW * 32, MINB)
 // -------------------------------------------------------------------------
 constexpr int C_W = 8;
 
+// use_bits: the row's touched columns are a bitmap in shared memory (ncols
+// bits) instead of the slab's marks, so a product reads the slab's
+// accumulator only when its column was already touched in this row.
 template <typename T>
 __global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs g, int smax, int ncols,
                                                         const int *rows, TierLists *tl,
-                                                        unsigned char *slabs)
+                                                        unsigned char *slabs, int use_bits)
 {
     constexpr int W = C_W;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -1679,6 +1685,7 @@ __global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs 
     int *stage = reinterpret_cast<int *>(smem) + wt * smax;
     int *cnt = reinterpret_cast<int *>(smem) + W * smax;
     TeamMisc *misc = reinterpret_cast<TeamMisc *>(cnt + 2 * W);
+    unsigned *bits = reinterpret_cast<unsigned *>(reinterpret_cast<unsigned char *>(misc) + 32);
 
     const size_t slab_bytes = (size_t) ncols * (sizeof(T) + 2 * sizeof(int));
     unsigned char *slab = slabs + (size_t) blockIdx.x * slab_bytes;
@@ -1704,8 +1711,12 @@ __global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs 
         if (!marks_clear)
         {
             // The slab is shared scratch: clear this block's marks once.
-            for (int s = tid; s < ncols; s += 256)
-                mark[s] = 0;
+            if (use_bits)
+                for (int s = tid; s < (ncols + 31) / 32; s += 256)
+                    bits[s] = 0u;
+            else
+                for (int s = tid; s < ncols; s += 256)
+                    mark[s] = 0;
             __syncthreads();
             marks_clear = true;
         }
@@ -1750,7 +1761,20 @@ __global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs 
                     {
                         k = birow[kp];
                         const T p = mul_rn(a, brow[kp]);
-                        if (mark[k] != i + 1)
+                        if (use_bits)
+                        {
+                            // only this lane sets this bit within the jp
+                            const unsigned m = 1u << (k & 31);
+                            if (!(bits[k >> 5] & m))
+                            {
+                                atomicOr(&bits[k >> 5], m);
+                                acc[k] = add_rn(T(0), p);
+                                ins = true;
+                            }
+                            else
+                                acc[k] = add_rn(acc[k], p);
+                        }
+                        else if (mark[k] != i + 1)
                         {
                             mark[k] = i + 1;
                             acc[k] = add_rn(T(0), p);
@@ -1793,7 +1817,10 @@ __global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs 
             {
                 k = order[q];
                 x = acc[k];
-                mark[k] = 0;
+                if (use_bits)
+                    atomicAnd(&bits[k >> 5], ~(1u << (k & 31)));
+                else
+                    mark[k] = 0;
                 if (k == i)
                 {
                     keep = true;
@@ -1919,7 +1946,11 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     const int N = g.NA;
     const int smaxC = b200_round_up(b200_ceil_div(g.ldb, C_W), 32);
     const size_t smemA = tierA_warp_bytes<T>() * A_WARPS;
-    const size_t smemC = (size_t) C_W * smaxC * sizeof(int) + 2 * C_W * sizeof(int) + 32;
+    const size_t smemC0 = (size_t) C_W * smaxC * sizeof(int) + 2 * C_W * sizeof(int) + 32;
+    // the touched-column bitmap, while it leaves 8 blocks per SM their share
+    const size_t bits_bytes = (size_t) (ncols + 31) / 32 * sizeof(unsigned);
+    const int use_bits = B200_DENSE_BITS && (smemC0 + bits_bytes) * C_BLOCKS_PER_SM <= 200 * 1024 ? 1 : 0;
+    const size_t smemC = smemC0 + (use_bits ? bits_bytes : 0);
     if (smemC > c->smem_optin)
     {
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "row width %d too large for the multiply kernels", g.ldb);
@@ -2073,7 +2104,7 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     if (!CUDA_OK(cudaFuncSetAttribute(dense_tier_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
         return false;
-    dense_tier_kernel<T><<<gridC, 256, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs);
+    dense_tier_kernel<T><<<gridC, 256, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
     if (!LAUNCH_OK("dense_tier_kernel"))
         return false;
 
