@@ -1665,13 +1665,16 @@ __global__ void __launch_bounds__(KW * 32, MINB)
 // order[ncols] (int, column ids in first-touch order).  Marks are cleared
 // column by column at the end of each row, as the reference clears ix[].
 // -------------------------------------------------------------------------
-constexpr int C_W = 8;
+#ifndef B200_C_W
+#define B200_C_W 8
+#endif
+constexpr int C_W = B200_C_W; // warps per row in the dense tier
 
 // use_bits: the row's touched columns are a bitmap in shared memory (ncols
 // bits) instead of the slab's marks, so a product reads the slab's
 // accumulator only when its column was already touched in this row.
 template <typename T>
-__global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs g, int smax, int ncols,
+__global__ void __launch_bounds__(C_W * 32, B200_C_BLOCKS) dense_tier_kernel(MulArgs g, int smax, int ncols,
                                                         const int *rows, TierLists *tl,
                                                         unsigned char *slabs, int use_bits)
 {
@@ -1712,10 +1715,10 @@ __global__ void __launch_bounds__(256, B200_C_BLOCKS) dense_tier_kernel(MulArgs 
         {
             // The slab is shared scratch: clear this block's marks once.
             if (use_bits)
-                for (int s = tid; s < (ncols + 31) / 32; s += 256)
+                for (int s = tid; s < (ncols + 31) / 32; s += C_W * 32)
                     bits[s] = 0u;
             else
-                for (int s = tid; s < ncols; s += 256)
+                for (int s = tid; s < ncols; s += C_W * 32)
                     mark[s] = 0;
             __syncthreads();
             marks_clear = true;
@@ -2104,7 +2107,7 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     if (!CUDA_OK(cudaFuncSetAttribute(dense_tier_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
         return false;
-    dense_tier_kernel<T><<<gridC, 256, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
+    dense_tier_kernel<T><<<gridC, C_W * 32, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
     if (!LAUNCH_OK("dense_tier_kernel"))
         return false;
 
