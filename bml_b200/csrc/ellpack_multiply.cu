@@ -74,14 +74,17 @@ struct MulArgs
 // tier is always in use); B200_C_BLOCKS: blocks per SM of the dense tier.
 // Measured on B200 over 4 FP64 SP2 iterations on the 40^3 lattice (N=64000,
 // radius 3): A + B1 + C 776 ms, A + K8 791 ms, A + B1 + K4 + K8 927 ms,
-// A + W8 + W16 + K4 + K8 994 ms.  The rows there reach 8000+ distinct
+// A + W8 + W16 + K4 + K8 994 ms (before the dense tier's bitmap and batched
+// loads, which took A + B1 + C to 576 ms with C at 6 blocks/SM and 3 chunks
+// of 32 products in flight per lane: 8 blocks 689 ms (32 registers, spills),
+// 5 blocks 580 ms, 3 or 4 chunks within 2%).  The rows there reach 8000+ distinct
 // columns before thresholding, where the dense tier's device-memory
 // accumulator still wins; the other tiers stay selectable at run time.
 #ifndef B200_X2_TIERS
 #define B200_X2_TIERS 0x05
 #endif
 #ifndef B200_C_BLOCKS
-#define B200_C_BLOCKS 8
+#define B200_C_BLOCKS 6
 #endif
 #ifndef B200_DENSE_BITS
 #define B200_DENSE_BITS 1
@@ -1669,6 +1672,10 @@ __global__ void __launch_bounds__(KW * 32, MINB)
 #define B200_C_W 8
 #endif
 constexpr int C_W = B200_C_W; // warps per row in the dense tier
+#ifndef B200_C_U
+#define B200_C_U 3
+#endif
+constexpr int C_U = B200_C_U; // chunks of 32 products a lane has in flight
 
 // use_bits: the row's touched columns are a bitmap in shared memory (ncols
 // bits) instead of the slab's marks, so a product reads the slab's
@@ -1755,42 +1762,80 @@ __global__ void __launch_bounds__(C_W * 32, B200_C_BLOCKS) dense_tier_kernel(Mul
                 const int S = b200_round_up(b200_ceil_div(nj, W), 32);
                 const int k0 = min(wt * S, nj), k1 = min(k0 + S, nj);
                 int local = 0;
-                for (int kb = k0; kb < k1; kb += 32)
+                if (use_bits)
                 {
-                    const int kp = kb + lane;
-                    bool ins = false;
-                    int k = 0;
-                    if (kp < k1)
+                    // C_U chunks of 32 at once: all loads of B's entries, then
+                    // the accumulators of columns already touched, then the
+                    // sums (the columns of one jp are distinct, so the
+                    // reordering changes no result)
+                    for (int kb = k0; kb < k1; kb += 32 * C_U)
                     {
-                        k = birow[kp];
-                        const T p = mul_rn(a, brow[kp]);
-                        if (use_bits)
+                        int kk[C_U];
+                        T bb[C_U], old[C_U];
+                        bool have[C_U], fresh[C_U];
+#pragma unroll
+                        for (int u = 0; u < C_U; ++u)
                         {
-                            // only this lane sets this bit within the jp
-                            const unsigned m = 1u << (k & 31);
-                            if (!(bits[k >> 5] & m))
+                            const int kp = kb + u * 32 + lane;
+                            have[u] = kp < k1;
+                            kk[u] = have[u] ? birow[kp] : 0;
+                            bb[u] = have[u] ? brow[kp] : T(0);
+                        }
+#pragma unroll
+                        for (int u = 0; u < C_U; ++u)
+                        {
+                            fresh[u] = false;
+                            old[u] = T(0);
+                            if (have[u])
                             {
-                                atomicOr(&bits[k >> 5], m);
+                                // only this lane sets this bit within the jp
+                                const unsigned m = 1u << (kk[u] & 31);
+                                fresh[u] = !(bits[kk[u] >> 5] & m);
+                                if (fresh[u])
+                                    atomicOr(&bits[kk[u] >> 5], m);
+                                else
+                                    old[u] = acc[kk[u]];
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < C_U; ++u)
+                            if (have[u])
+                                acc[kk[u]] = add_rn(fresh[u] ? T(0) : old[u], mul_rn(a, bb[u]));
+#pragma unroll
+                        for (int u = 0; u < C_U; ++u)
+                        {
+                            const bool ins = have[u] && fresh[u];
+                            const unsigned bal = __ballot_sync(FULL, ins);
+                            if (ins)
+                                stage[local + __popc(bal & lanemask_lt())] = kk[u];
+                            local += __popc(bal);
+                        }
+                    }
+                }
+                else
+                    for (int kb = k0; kb < k1; kb += 32)
+                    {
+                        const int kp = kb + lane;
+                        bool ins = false;
+                        int k = 0;
+                        if (kp < k1)
+                        {
+                            k = birow[kp];
+                            const T p = mul_rn(a, brow[kp]);
+                            if (mark[k] != i + 1)
+                            {
+                                mark[k] = i + 1;
                                 acc[k] = add_rn(T(0), p);
                                 ins = true;
                             }
                             else
                                 acc[k] = add_rn(acc[k], p);
                         }
-                        else if (mark[k] != i + 1)
-                        {
-                            mark[k] = i + 1;
-                            acc[k] = add_rn(T(0), p);
-                            ins = true;
-                        }
-                        else
-                            acc[k] = add_rn(acc[k], p);
+                        const unsigned bal = __ballot_sync(FULL, ins);
+                        if (ins)
+                            stage[local + __popc(bal & lanemask_lt())] = k;
+                        local += __popc(bal);
                     }
-                    const unsigned bal = __ballot_sync(FULL, ins);
-                    if (ins)
-                        stage[local + __popc(bal & lanemask_lt())] = k;
-                    local += __popc(bal);
-                }
                 if (lane == 0)
                     cnt[(step & 1) * W + wt] = local;
                 __syncthreads();
