@@ -1672,20 +1672,43 @@ __global__ void __launch_bounds__(KW * 32, MINB)
 #define B200_C_W 8
 #endif
 constexpr int C_W = B200_C_W; // warps per row in the dense tier
+// Two forms of the accumulation, chosen per call:
+//  - RED: acc[k] += p for a column already touched in this row is a
+//    reduction at L2 (red.global.add), so the lane does not wait for the old
+//    value.  Within one jp a column has one writer, and the block barrier
+//    between jp's orders the reductions of successive jp's, so each column
+//    is still summed in jp order.  The f64 reduction rounds to nearest even
+//    and keeps subnormals, so FP64 always takes this form; the f32 one
+//    flushes subnormals to zero, so FP32 takes it only when the caller allows
+//    that (mixed-precision SP2's FP32 iterations).
+//  - load/add/store, with C_U chunks of 32 products in flight per lane
+//    (exact FP32).
+// Blocks per SM and chunks per lane of each form (measured on B200 over 4
+// FP64 SP2 iterations on the 40^3 lattice: RED 8 blocks 407 ms with 1 or 2
+// chunks, 6 blocks 422 ms; load/store 6 blocks x 3 chunks 576 ms, 5 blocks
+// 580 ms, 8 blocks 689 ms (register spills)).
+#ifndef B200_C_BLOCKS_RED
+#define B200_C_BLOCKS_RED 8
+#endif
+#ifndef B200_C_U_RED
+#define B200_C_U_RED 1
+#endif
 #ifndef B200_C_U
 #define B200_C_U 3
 #endif
-constexpr int C_U = B200_C_U; // chunks of 32 products a lane has in flight
+template <bool RED> struct DenseCfg
+{
+    static constexpr int blocks = RED ? B200_C_BLOCKS_RED : B200_C_BLOCKS;
+    static constexpr int chunks = RED ? B200_C_U_RED : B200_C_U;
+};
 
-// use_bits: the row's touched columns are a bitmap in shared memory (ncols
-// bits) instead of the slab's marks, so a product reads the slab's
-// accumulator only when its column was already touched in this row.
-template <typename T>
-__global__ void __launch_bounds__(C_W * 32, B200_C_BLOCKS) dense_tier_kernel(MulArgs g, int smax, int ncols,
+template <typename T, bool RED>
+__global__ void __launch_bounds__(C_W * 32, DenseCfg<RED>::blocks) dense_tier_kernel(MulArgs g, int smax, int ncols,
                                                         const int *rows, TierLists *tl,
                                                         unsigned char *slabs, int use_bits)
 {
     constexpr int W = C_W;
+    constexpr int C_U = DenseCfg<RED>::chunks;
     extern __shared__ __align__(128) unsigned char smem[];
     if (g.flags->bad_input)
         return;
@@ -1793,14 +1816,22 @@ __global__ void __launch_bounds__(C_W * 32, B200_C_BLOCKS) dense_tier_kernel(Mul
                                 fresh[u] = !(bits[kk[u] >> 5] & m);
                                 if (fresh[u])
                                     atomicOr(&bits[kk[u] >> 5], m);
-                                else
+                                else if (!RED)
                                     old[u] = acc[kk[u]];
                             }
                         }
 #pragma unroll
                         for (int u = 0; u < C_U; ++u)
                             if (have[u])
-                                acc[kk[u]] = add_rn(fresh[u] ? T(0) : old[u], mul_rn(a, bb[u]));
+                            {
+                                const T p = mul_rn(a, bb[u]);
+                                if (fresh[u])
+                                    acc[kk[u]] = add_rn(T(0), p);
+                                else if (RED)
+                                    atomicAdd(acc + kk[u], p);
+                                else
+                                    acc[kk[u]] = add_rn(old[u], p);
+                            }
 #pragma unroll
                         for (int u = 0; u < C_U; ++u)
                         {
@@ -1828,6 +1859,8 @@ __global__ void __launch_bounds__(C_W * 32, B200_C_BLOCKS) dense_tier_kernel(Mul
                                 acc[k] = add_rn(T(0), p);
                                 ins = true;
                             }
+                            else if (RED)
+                                atomicAdd(acc + k, p);
                             else
                                 acc[k] = add_rn(acc[k], p);
                         }
@@ -1974,7 +2007,10 @@ bool launch_wide(B200Context *c, const MulArgs &g, const BucketArgs &ba, const i
     return LAUNCH_OK("wide_kernel");
 }
 
-constexpr int C_BLOCKS_PER_SM = B200_C_BLOCKS;
+// FP32 multiplies may use the flushing f32 reduction in the dense tier
+// (set by mixed-precision SP2 around its FP32 iterations; off by default,
+// which keeps FP32 products bit-exact).
+bool g_f32_reduce = false;
 
 // Distinct-column counts of the last multiply, reused as the next call's
 // tier estimate when the row count matches (SP2 multiplies the same-size
@@ -1995,16 +2031,18 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     const int smaxC = b200_round_up(b200_ceil_div(g.ldb, C_W), 32);
     const size_t smemA = tierA_warp_bytes<T>() * A_WARPS;
     const size_t smemC0 = (size_t) C_W * smaxC * sizeof(int) + 2 * C_W * sizeof(int) + 32;
-    // the touched-column bitmap, while it leaves 8 blocks per SM their share
+    const bool red = sizeof(T) == 8 || g_f32_reduce;
+    const int blocks_c = red ? DenseCfg<true>::blocks : DenseCfg<false>::blocks;
+    // the touched-column bitmap, while it leaves each block its share
     const size_t bits_bytes = (size_t) (ncols + 31) / 32 * sizeof(unsigned);
-    const int use_bits = B200_DENSE_BITS && (smemC0 + bits_bytes) * C_BLOCKS_PER_SM <= 200 * 1024 ? 1 : 0;
+    const int use_bits = B200_DENSE_BITS && (smemC0 + bits_bytes) * blocks_c <= 200 * 1024 ? 1 : 0;
     const size_t smemC = smemC0 + (use_bits ? bits_bytes : 0);
     if (smemC > c->smem_optin)
     {
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "row width %d too large for the multiply kernels", g.ldb);
         return false;
     }
-    const int gridC = c->sm_count * C_BLOCKS_PER_SM;
+    const int gridC = c->sm_count * blocks_c;
     const size_t slab_bytes = (size_t) ncols * (sizeof(T) + 2 * sizeof(int));
 
     if (g_hint_n != N)
@@ -2149,10 +2187,10 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
         if (!launch_window<T, K8_CFG>(c, gridK8, g, ba, list(TIER_K8), tl, TIER_K8, next_on(TIER_K8),
                                       list(next_on(TIER_K8)), keyg, gvals))
             return false;
-    if (!CUDA_OK(cudaFuncSetAttribute(dense_tier_kernel<T>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
+    auto dense = red ? dense_tier_kernel<T, true> : dense_tier_kernel<T, false>;
+    if (!CUDA_OK(cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
         return false;
-    dense_tier_kernel<T><<<gridC, C_W * 32, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
+    dense<<<gridC, C_W * 32, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
     if (!LAUNCH_OK("dense_tier_kernel"))
         return false;
 
@@ -2202,6 +2240,11 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
 }
 
 } // namespace
+
+void ell_set_f32_reduce(bool on)
+{
+    g_f32_reduce = on;
+}
 
 // x2_rows: A is a row view of B (rows of X^2): report overflow as X^2 does,
 // on the thresholded width only.

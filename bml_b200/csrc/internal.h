@@ -131,6 +131,9 @@ void b200_free_domain(bml_domain_t *D);
 // C <- A*B (A==B allowed) thresholded with the diagonal kept, in the
 // reference's first-touch column order.  trace (nullable) receives
 // {sum of A's diagonal entries, sum of C's diagonal entries}.
+// FP32 products may use the dense tier's f32 reduction at L2, which
+// flushes subnormal sums to zero (used by mixed-precision SP2; off by default).
+void ell_set_f32_reduce(bool on);
 bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B,
                      bml_matrix_ellpack_t *C, double threshold, double *trace,
                      int *required_M, int x2_rows = 0);

@@ -170,7 +170,11 @@ extern "C" int bml_b200_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double thres
         status = bml_b200_last_error();
         goto done;
     }
+    // the FP32 products may take the dense tier's f32 reduction (subnormal
+    // sums flush to zero, below the FP32 iterations' rounding anyway)
+    ell_set_f32_reduce(true);
     status = sp2_iterate(X, X2, threshold, occupation, maxiter - nclose, tol, stall, s, &stopped);
+    ell_set_f32_reduce(false);
     inf[6] = s.it;
     inf[7] = s.x2_seconds;
     if (status != BML_B200_OK)
