@@ -1668,10 +1668,6 @@ __global__ void __launch_bounds__(KW * 32, MINB)
 // order[ncols] (int, column ids in first-touch order).  Marks are cleared
 // column by column at the end of each row, as the reference clears ix[].
 // -------------------------------------------------------------------------
-#ifndef B200_C_W
-#define B200_C_W 8
-#endif
-constexpr int C_W = B200_C_W; // warps per row in the dense tier
 // Two forms of the accumulation, chosen per call:
 //  - RED: acc[k] += p for a column already touched in this row is a
 //    reduction at L2 (red.global.add), so the lane does not wait for the old
@@ -1681,33 +1677,41 @@ constexpr int C_W = B200_C_W; // warps per row in the dense tier
 //    and keeps subnormals, so FP64 always takes this form; the f32 one
 //    flushes subnormals to zero, so FP32 takes it only when the caller allows
 //    that (mixed-precision SP2's FP32 iterations).
-//  - load/add/store, with C_U chunks of 32 products in flight per lane
-//    (exact FP32).
-// Blocks per SM and chunks per lane of each form (measured on B200 over 4
-// FP64 SP2 iterations on the 40^3 lattice: RED 8 blocks 407 ms with 1 or 2
-// chunks, 6 blocks 422 ms; load/store 6 blocks x 3 chunks 576 ms, 5 blocks
-// 580 ms, 8 blocks 689 ms (register spills)).
+//  - load/add/store (exact FP32).
+// Warps per row, blocks per SM and chunks of 32 products in flight per lane
+// of each form, measured on B200 over 4 FP64 SP2 iterations on the 40^3
+// lattice: RED 4 warps x 10 blocks x 3 chunks 377 ms (x 8-12 blocks, 2-4
+// chunks: 377-398 ms; 8 warps x 8 blocks 407 ms; 16 warps x 4 blocks
+// 655 ms); load/store 8 warps x 6 blocks x 3 chunks 576 ms (5 blocks 580 ms,
+// 8 blocks 689 ms with register spills).
+#ifndef B200_C_W_RED
+#define B200_C_W_RED 4
+#endif
 #ifndef B200_C_BLOCKS_RED
-#define B200_C_BLOCKS_RED 8
+#define B200_C_BLOCKS_RED 10
 #endif
 #ifndef B200_C_U_RED
-#define B200_C_U_RED 1
+#define B200_C_U_RED 3
+#endif
+#ifndef B200_C_W
+#define B200_C_W 8
 #endif
 #ifndef B200_C_U
 #define B200_C_U 3
 #endif
 template <bool RED> struct DenseCfg
 {
+    static constexpr int warps = RED ? B200_C_W_RED : B200_C_W;
     static constexpr int blocks = RED ? B200_C_BLOCKS_RED : B200_C_BLOCKS;
     static constexpr int chunks = RED ? B200_C_U_RED : B200_C_U;
 };
 
 template <typename T, bool RED>
-__global__ void __launch_bounds__(C_W * 32, DenseCfg<RED>::blocks) dense_tier_kernel(MulArgs g, int smax, int ncols,
+__global__ void __launch_bounds__(DenseCfg<RED>::warps * 32, DenseCfg<RED>::blocks) dense_tier_kernel(MulArgs g, int smax, int ncols,
                                                         const int *rows, TierLists *tl,
                                                         unsigned char *slabs, int use_bits)
 {
-    constexpr int W = C_W;
+    constexpr int W = DenseCfg<RED>::warps;
     constexpr int C_U = DenseCfg<RED>::chunks;
     extern __shared__ __align__(128) unsigned char smem[];
     if (g.flags->bad_input)
@@ -1745,10 +1749,10 @@ __global__ void __launch_bounds__(C_W * 32, DenseCfg<RED>::blocks) dense_tier_ke
         {
             // The slab is shared scratch: clear this block's marks once.
             if (use_bits)
-                for (int s = tid; s < (ncols + 31) / 32; s += C_W * 32)
+                for (int s = tid; s < (ncols + 31) / 32; s += W * 32)
                     bits[s] = 0u;
             else
-                for (int s = tid; s < ncols; s += C_W * 32)
+                for (int s = tid; s < ncols; s += W * 32)
                     mark[s] = 0;
             __syncthreads();
             marks_clear = true;
@@ -2028,11 +2032,13 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     if (!c)
         return false;
     const int N = g.NA;
-    const int smaxC = b200_round_up(b200_ceil_div(g.ldb, C_W), 32);
+
     const size_t smemA = tierA_warp_bytes<T>() * A_WARPS;
-    const size_t smemC0 = (size_t) C_W * smaxC * sizeof(int) + 2 * C_W * sizeof(int) + 32;
     const bool red = sizeof(T) == 8 || g_f32_reduce;
+    const int warps_c = red ? DenseCfg<true>::warps : DenseCfg<false>::warps;
     const int blocks_c = red ? DenseCfg<true>::blocks : DenseCfg<false>::blocks;
+    const int smaxC = b200_round_up(b200_ceil_div(g.ldb, warps_c), 32);
+    const size_t smemC0 = (size_t) warps_c * smaxC * sizeof(int) + 2 * warps_c * sizeof(int) + 32;
     // the touched-column bitmap, while it leaves each block its share
     const size_t bits_bytes = (size_t) (ncols + 31) / 32 * sizeof(unsigned);
     const int use_bits = B200_DENSE_BITS && (smemC0 + bits_bytes) * blocks_c <= 200 * 1024 ? 1 : 0;
@@ -2190,7 +2196,7 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     auto dense = red ? dense_tier_kernel<T, true> : dense_tier_kernel<T, false>;
     if (!CUDA_OK(cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
         return false;
-    dense<<<gridC, C_W * 32, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
+    dense<<<gridC, warps_c * 32, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
     if (!LAUNCH_OK("dense_tier_kernel"))
         return false;
 
