@@ -71,15 +71,13 @@ struct MulArgs
 
 // Tiers in routing order: A, W8, B1, W16, K4, K8, C (dense).
 // B200_X2_TIERS: bit t set = tier t in use (rows skip unused tiers; the dense
-// tier is always in use); B200_C_BLOCKS: blocks per SM of the dense tier.
+// tier is always in use).
 // Measured on B200 over 4 FP64 SP2 iterations on the 40^3 lattice (N=64000,
-// radius 3): A + B1 + C 776 ms, A + K8 791 ms, A + B1 + K4 + K8 927 ms,
-// A + W8 + W16 + K4 + K8 994 ms (before the dense tier's bitmap and batched
-// loads, which took A + B1 + C to 576 ms with C at 6 blocks/SM and 3 chunks
-// of 32 products in flight per lane: 8 blocks 689 ms (32 registers, spills),
-// 5 blocks 580 ms, 3 or 4 chunks within 2%).  The rows there reach 8000+ distinct
-// columns before thresholding, where the dense tier's device-memory
-// accumulator still wins; the other tiers stay selectable at run time.
+// radius 3), with the dense tier's first form: A + B1 + C 776 ms, A + K8
+// 791 ms, A + B1 + K4 + K8 927 ms, A + W8 + W16 + K4 + K8 994 ms; the dense
+// tier's later forms (below) took A + B1 + C to 376 ms.  The rows there reach
+// 8000+ distinct columns before thresholding, where the dense tier's
+// device-memory accumulator wins; the other tiers stay selectable at run time.
 #ifndef B200_X2_TIERS
 #define B200_X2_TIERS 0x05
 #endif
