@@ -44,9 +44,9 @@ THRESHOLD = 1e-5
 OCC = N / 2.0
 SP2_ITERS = 4
 # DRAM bytes per product term of the dense X^2 tier, from one ncu capture of
-# the 30^3 lattice case (bench.py --profile): 136.26 GB read + 22.29 GB
+# the 30^3 lattice case (bench.py --profile): 122.82 GB read + 11.77 GB
 # written for 18,570,945,128 products.
-DRAM_BYTES_PER_PRODUCT = (136.262850e9 + 22.292815e9) / 18570945128
+DRAM_BYTES_PER_PRODUCT = (122.821243e9 + 11.769428e9) / 18570945128
 METRIC = "s per SP2 solve & X² HBM GB/s, ELLPACK N=64K: FP64 vs mixed at ≤1e-6 err"
 WORKLOAD = ("SP2 on the 40^3 lattice Hamiltonian (N=64000, radius 3, M=%d, thr 1e-5, occ N/2, FP64), "
             "first %d iterations from X0 (the full solve fills in to dense)" % (M_X, SP2_ITERS))
@@ -368,7 +368,7 @@ def x2_roofline(B, H, info):
     return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "peak_source": src, "traffic": DRAM_BYTES_PER_PRODUCT * P,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dense tier on the 30^3 "
-                              "case (158.6 GB for 18.57 G products, profiles/x2_dense_tier_lattice30.md), "
+                              "case (134.6 GB for 18.57 G products, profiles/x2_dense_tier_lattice30.md), "
                               "scaled by this call's products",
             "kernel": "one ELLPACK X^2 call (tier kernels together) on the SP2 iterate of iteration %d"
                       % (SP2_ITERS - 1),

@@ -1939,6 +1939,272 @@ __global__ void __launch_bounds__(DenseCfg<RED>::warps * 32, DenseCfg<RED>::bloc
     }
 }
 
+// -------------------------------------------------------------------------
+// Tier C, staged form (the reduction form with B's rows in shared memory):
+// B's rows stream through a ring of STAGES units of at most CHUNK entries,
+// copied by TMA bulk copies (cp.async.bulk) up to STAGES - 1 units ahead, as
+// in the team tiers; the accumulator is the per-block slab with the
+// shared-memory touched bitmap and L2 reductions.  The product loop then
+// reads B from shared memory, so no lane waits on a global load.  The
+// first-touch list is built per unit (units follow B's row order).
+// Shared memory: mbar[STAGES] | sv[STAGES][CHUNK] | sk[STAGES][CHUNK] |
+//                stg[W][SPW] (int) | cnt[2][W] | misc | bits[ncols/32]
+// -------------------------------------------------------------------------
+template <typename T, int W, int STAGES, int CHUNK> struct StagedCfg
+{
+    static constexpr int NT = W * 32;
+    static constexpr int SPW = ((CHUNK + W - 1) / W + 31) / 32 * 32;
+    static constexpr size_t off_sv = 128;
+    static constexpr size_t off_sk = off_sv + size_t(STAGES) * CHUNK * sizeof(T);
+    static constexpr size_t off_stg = off_sk + size_t(STAGES) * CHUNK * sizeof(int);
+    static constexpr size_t off_cnt = off_stg + size_t(W) * SPW * sizeof(int);
+    static constexpr size_t off_misc = off_cnt + 2 * W * sizeof(int);
+    static constexpr size_t off_bits = (off_misc + sizeof(TeamMisc) + 15) / 16 * 16;
+    static size_t bytes(int ncols) { return off_bits + (size_t) (ncols + 31) / 32 * sizeof(unsigned); }
+};
+
+template <typename T, int W, int STAGES, int CHUNK, int MINB>
+__global__ void __launch_bounds__(W * 32, MINB) dense_staged_kernel(MulArgs g, int ncols, const int *rows,
+                                                                   TierLists *tl, unsigned char *slabs)
+{
+    using Cfg = StagedCfg<T, W, STAGES, CHUNK>;
+    constexpr int NT = Cfg::NT, SPW = Cfg::SPW;
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (g.flags->bad_input)
+        return;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);
+    T *sv = reinterpret_cast<T *>(smem + Cfg::off_sv);
+    int *sk = reinterpret_cast<int *>(smem + Cfg::off_sk);
+    int *cnt = reinterpret_cast<int *>(smem + Cfg::off_cnt);
+    TeamMisc *misc = reinterpret_cast<TeamMisc *>(smem + Cfg::off_misc);
+    unsigned *bits = reinterpret_cast<unsigned *>(smem + Cfg::off_bits);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int *stg = reinterpret_cast<int *>(smem + Cfg::off_stg) + warp * SPW;
+
+    const size_t slab_bytes = (size_t) ncols * (sizeof(T) + 2 * sizeof(int));
+    T *acc = reinterpret_cast<T *>(slabs + (size_t) blockIdx.x * slab_bytes);
+    int *order = reinterpret_cast<int *>(acc + ncols) + ncols;
+
+    const int nrows = tl->count[NTIERS - 1];
+    const T *Av = static_cast<const T *>(g.Av);
+    const T *Bv = static_cast<const T *>(g.Bv);
+    T *Cv = static_cast<T *>(g.Cv);
+    const T thr = (T) g.thr;
+    int *tflag = &g.flags->timeout;
+
+    // Column ids in the ring start as 0, so a unit whose copy never landed
+    // (a timed-out wait, reported to the host) still names a valid column.
+    for (int s = tid; s < STAGES * CHUNK; s += NT)
+        sk[s] = 0;
+    for (int s = tid; s < (ncols + 31) / 32; s += NT)
+        bits[s] = 0u;
+    if (tid == 0)
+    {
+        for (int s = 0; s < STAGES; ++s)
+            mbar_init(&mbar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    unsigned ucount = 0; // units consumed by this block (uniform)
+    for (;;)
+    {
+        if (tid == 0)
+            misc->row = atomicAdd(&tl->cursor[NTIERS - 1], 1);
+        __syncthreads();
+        const int pos = misc->row;
+        if (pos >= nrows || *reinterpret_cast<volatile int *>(tflag))
+            break;
+        const int i = rows[pos];
+        if (tid == 0)
+            misc->diag = 0.0;
+        const int ni = g.An[i];
+        const T *arow = Av + (size_t) i * g.lda;
+        const int *airow = g.Ai + (size_t) i * g.lda;
+
+        // Producer (thread 0): the next unit to copy is chunk pc of the B row
+        // named at position pj.  Every thread counts the units it consumes.
+        int pj = 0, pc = 0, pnj = 0;
+        unsigned issued = 0;
+        auto prod_skip = [&]() {
+            while (pj < ni)
+            {
+                pnj = g.Bn[airow[pj]];
+                if (pc * CHUNK < pnj)
+                    return;
+                ++pj;
+                pc = 0;
+            }
+        };
+        auto issue = [&]() {
+            const int s = (ucount + issued) % STAGES;
+            const int j = airow[pj];
+            const int off = pc * CHUNK;
+            const int n = min(CHUNK, pnj - off);
+            const unsigned bv = (unsigned) ((n * sizeof(T) + 15) & ~size_t(15));
+            const unsigned bk = (unsigned) ((n * sizeof(int) + 15) & ~size_t(15));
+            mbar_expect_tx(&mbar[s], bv + bk);
+            bulk_g2s(sv + (size_t) s * CHUNK, Bv + (size_t) j * g.ldb + off, bv, &mbar[s]);
+            bulk_g2s(sk + (size_t) s * CHUNK, g.Bi + (size_t) j * g.ldb + off, bk, &mbar[s]);
+            ++pc;
+            ++issued;
+            prod_skip();
+        };
+        if (tid == 0)
+        {
+            prod_skip();
+            while (issued < STAGES && pj < ni)
+                issue();
+        }
+
+        int distinct = 0;
+        T dA = T(0);
+        unsigned consumed = 0;
+        for (int jp0 = 0; jp0 < ni; jp0 += 32)
+        {
+            const int q = jp0 + lane;
+            T av = T(0);
+            int aj = 0, nj_l = 0;
+            if (q < ni)
+            {
+                av = arow[q];
+                aj = airow[q];
+                nj_l = g.Bn[aj];
+            }
+            const int cnt_here = min(32, ni - jp0);
+            for (int t = 0; t < cnt_here; ++t)
+            {
+                const T a = __shfl_sync(FULL, av, t);
+                const int j = __shfl_sync(FULL, aj, t);
+                const int nj = __shfl_sync(FULL, nj_l, t);
+                if (j == i)
+                    dA = add_rn(dA, a);
+                for (int off = 0; off < nj; off += CHUNK)
+                {
+                    const unsigned u = ucount + consumed;
+                    const int s = u % STAGES;
+                    const int n = min(CHUNK, nj - off);
+                    mbar_wait_bounded(&mbar[s], (u / STAGES) & 1, tflag);
+                    const T *uv = sv + (size_t) s * CHUNK;
+                    const int *uk = sk + (size_t) s * CHUNK;
+                    const int S = b200_round_up(b200_ceil_div(n, W), 32);
+                    const int k0 = min(warp * S, n), k1 = min(k0 + S, n);
+                    int local = 0;
+                    for (int kb = k0; kb < k1; kb += 32)
+                    {
+                        const int kp = kb + lane;
+                        bool ins = false;
+                        int k = 0;
+                        if (kp < k1)
+                        {
+                            k = uk[kp];
+                            const T p = mul_rn(a, uv[kp]);
+                            // only this lane sets this bit within the unit
+                            const unsigned m = 1u << (k & 31);
+                            if (!(bits[k >> 5] & m))
+                            {
+                                atomicOr(&bits[k >> 5], m);
+                                acc[k] = add_rn(T(0), p);
+                                ins = true;
+                            }
+                            else
+                                atomicAdd(acc + k, p);
+                        }
+                        const unsigned bal = __ballot_sync(FULL, ins);
+                        if (ins)
+                            stg[local + __popc(bal & lanemask_lt())] = k;
+                        local += __popc(bal);
+                    }
+                    if (lane == 0)
+                        cnt[(u & 1) * W + warp] = local;
+                    __syncthreads();
+                    ++consumed;
+                    int pre = 0, tot = 0;
+#pragma unroll
+                    for (int w = 0; w < W; ++w)
+                    {
+                        const int cw = cnt[(u & 1) * W + w];
+                        pre += (w < warp) ? cw : 0;
+                        tot += cw;
+                    }
+                    for (int r = lane; r < local; r += 32)
+                        order[distinct + pre + r] = stg[r];
+                    __syncwarp();
+                    distinct += tot;
+                    // the stage just consumed is free: refill it
+                    if (tid == 0 && pj < ni)
+                        issue();
+                }
+            }
+        }
+        ucount += consumed;
+        __syncthreads();
+
+        // Compaction in first-touch order: keep k == i or |x| > threshold.
+        int ll = 0, round = 0;
+        for (int c0 = 0; c0 < distinct; c0 += NT, ++round)
+        {
+            const int q = c0 + warp * 32 + lane;
+            bool keep = false;
+            int k = 0;
+            T x = T(0);
+            if (q < distinct)
+            {
+                k = order[q];
+                x = acc[k];
+                atomicAnd(&bits[k >> 5], ~(1u << (k & 31)));
+                if (k == i)
+                {
+                    keep = true;
+                    misc->diag = (double) x;
+                }
+                else
+                    keep = fabs(x) > thr;
+            }
+            const unsigned bal = __ballot_sync(FULL, keep);
+            if (lane == 0)
+                cnt[(round & 1) * W + warp] = __popc(bal);
+            __syncthreads();
+            int pre = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < W; ++w)
+            {
+                const int cw = cnt[(round & 1) * W + w];
+                pre += (w < warp) ? cw : 0;
+                tot += cw;
+            }
+            const int p = ll + pre + __popc(bal & lanemask_lt());
+            if (keep && p < g.Mc)
+            {
+                Cv[(size_t) i * g.ldc + p] = x;
+                g.Ci[(size_t) i * g.ldc + p] = k;
+            }
+            ll += tot;
+        }
+        __syncthreads();
+        if (tid == 0)
+            finish_row<T>(g, i, ll, distinct, dA, misc->diag);
+    }
+}
+
+// Staged dense tier: warps per row, ring stages, entries per unit, min blocks/SM
+#ifndef B200_C_STAGED
+#define B200_C_STAGED 1
+#endif
+#ifndef B200_CS_W
+#define B200_CS_W 4
+#endif
+#ifndef B200_CS_STAGES
+#define B200_CS_STAGES 2
+#endif
+#ifndef B200_CS_CHUNK
+#define B200_CS_CHUNK 1024
+#endif
+#ifndef B200_CS_MINB
+#define B200_CS_MINB 6
+#endif
+constexpr int CS_W = B200_CS_W, CS_STAGES = B200_CS_STAGES, CS_CHUNK = B200_CS_CHUNK, CS_MINB = B200_CS_MINB;
+
 // Team tier B1: (W, LOGTS, STAGES, CHUNK, min blocks per SM)
 #define B1_CFG 4, 11, 3, 256, 4
 
@@ -2046,8 +2312,24 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "row width %d too large for the multiply kernels", g.ldb);
         return false;
     }
-    const int gridC = c->sm_count * blocks_c;
+    int gridC = c->sm_count * blocks_c;
     const size_t slab_bytes = (size_t) ncols * (sizeof(T) + 2 * sizeof(int));
+    // the staged form of the reduction kernel, while its shared memory fits
+    using SCfg = StagedCfg<T, CS_W, CS_STAGES, CS_CHUNK>;
+    auto staged_k = dense_staged_kernel<T, CS_W, CS_STAGES, CS_CHUNK, CS_MINB>;
+    const size_t smemS = SCfg::bytes(ncols);
+    bool staged = B200_C_STAGED && red && smemS <= c->smem_optin;
+    if (staged)
+    {
+        if (!CUDA_OK(cudaFuncSetAttribute(staged_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemS)))
+            return false;
+        int occS = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occS, staged_k, CS_W * 32, smemS);
+        if (occS > 0)
+            gridC = c->sm_count * occS;
+        else
+            staged = false;
+    }
 
     if (g_hint_n != N)
     {
@@ -2191,12 +2473,21 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
         if (!launch_window<T, K8_CFG>(c, gridK8, g, ba, list(TIER_K8), tl, TIER_K8, next_on(TIER_K8),
                                       list(next_on(TIER_K8)), keyg, gvals))
             return false;
-    auto dense = red ? dense_tier_kernel<T, true> : dense_tier_kernel<T, false>;
-    if (!CUDA_OK(cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
-        return false;
-    dense<<<gridC, warps_c * 32, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
-    if (!LAUNCH_OK("dense_tier_kernel"))
-        return false;
+    if (staged)
+    {
+        staged_k<<<gridC, CS_W * 32, smemS, c->stream>>>(g, ncols, list(TIER_C), tl, slabs);
+        if (!LAUNCH_OK("dense_staged_kernel"))
+            return false;
+    }
+    else
+    {
+        auto dense = red ? dense_tier_kernel<T, true> : dense_tier_kernel<T, false>;
+        if (!CUDA_OK(cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemC)))
+            return false;
+        dense<<<gridC, warps_c * 32, smemC, c->stream>>>(g, smaxC, ncols, list(TIER_C), tl, slabs, use_bits);
+        if (!LAUNCH_OK("dense_tier_kernel"))
+            return false;
+    }
 
     if (trace)
     {
