@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-ellblock", action="store_true", help="skip the ELLBLOCK tensor-core leg")
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: 30^3 lattice, 3 SP2 iterations then one X^2")
+    ap.add_argument("--profile-ops", action="store_true",
+                    help="case for ncu of the one-pass ELLPACK operations (add, threshold, copy, scale, "
+                         "trace, Gershgorin, transpose) on the 30^3 lattice's SP2 iterate X and X^2")
     return ap.parse_args()
 
 
@@ -478,6 +481,50 @@ def run_profile_case():
                       "nnz_x2": B.lib.bml_b200_nnz(X2.h)}))
 
 
+def run_profile_ops():
+    """The one-pass ELLPACK operations, each launched once, on matrices larger
+    than L2: X = the SP2 iterate after 3 iterations on the 30^3 lattice
+    (N = 27000, threshold 1e-5, as in --profile) and X2 = X^2.  The SP2 start
+    and iterations launch gershgorin, scale, copy (3), add (1) and diag (1)
+    kernels first; the operations below follow, in the order written.
+    Prints the entry counts from which each operation's compulsory bytes
+    follow."""
+    import bml_b200 as B
+    Lp, Mp = 30, M_X
+    Np = Lp ** 3
+    v, ix, nz = B.gen_lattice(Lp, RADIUS, Np, M_H, SEED)
+    H = B.Ellpack.from_arrays(v, ix, nz, Np, M_H)
+    X = B.Ellpack(Np, Mp)
+    info = (C.c_double * 6)()
+    B.check(B.lib.bml_b200_sp2(H.h, X.h, THRESHOLD, Np / 2.0, 3, 1e-8, 0, info))
+    X2 = B.Ellpack(Np, Mp)
+    tr = (C.c_double * 2)()
+    B.check(B.lib.bml_b200_multiply_x2(X.h, X2.h, THRESHOLD, tr))
+    nnz = lambda m: int(B.lib.bml_b200_nnz(m.h))
+    n_x, n_x2 = nnz(X), nnz(X2)
+    # the operations, in launch order
+    S = B.Ellpack(Np, Mp)
+    B.lib.bml_copy(X.h, S.h)                       # copy_kernel: X -> S
+    B.lib.bml_add(S.h, X2.h, 2.0, -1.0, THRESHOLD)  # add_kernel: S = 2 S - X2
+    n_add = nnz(S)
+    T = B.Ellpack(Np, Mp)
+    B.lib.bml_copy(X2.h, T.h)                      # copy_kernel: X2 -> T
+    B.lib.bml_threshold(T.h, 1e-4)                 # threshold_kernel, in place
+    n_thr = nnz(T)
+    alpha = C.c_double(0.5)
+    B.lib.bml_scale_inplace(C.byref(alpha), X2.h)  # scale_kernel on X2
+    trace = B.lib.bml_trace(X2.h)                  # diag_kernel
+    eb = B.lib.bml_gershgorin(X2.h)                # gershgorin_kernel
+    B.lib.bml_free_memory(eb)
+    Xt = B.lib.bml_transpose_new(X2.h)             # transpose_scatter_kernel + row_sort_kernel
+    B.check()
+    hh = C.c_void_p(Xt)
+    B.lib.bml_deallocate(C.byref(hh))
+    print(json.dumps({"profile_case": "one-pass ELLPACK operations on the 30^3 lattice's SP2 iterate X and X^2",
+                      "N": Np, "M": Mp, "nnz_x": n_x, "nnz_x2": n_x2, "nnz_add": n_add, "nnz_threshold": n_thr,
+                      "trace": trace}))
+
+
 class _StdoutToStderr:
     """Route the process's stdout (fd 1) to stderr while the library prints
     its partition messages (bml_set_block_sizes prints, as the reference
@@ -571,6 +618,9 @@ def main():
         return
     if args.profile_tc:
         run_profile_tc()
+        return
+    if args.profile_ops:
+        run_profile_ops()
         return
     if args.impl == "reference":
         res = run_reference(args, rank, world)

@@ -74,12 +74,14 @@ struct MulArgs
 // tier is always in use).
 // Measured on B200 over 4 FP64 SP2 iterations on the 40^3 lattice (N=64000,
 // radius 3), with the dense tier's first form: A + B1 + C 776 ms, A + K8
-// 791 ms, A + B1 + K4 + K8 927 ms, A + W8 + W16 + K4 + K8 994 ms; the dense
-// tier's later forms (below) took A + B1 + C to 376 ms.  The rows there reach
-// 8000+ distinct columns before thresholding, where the dense tier's
-// device-memory accumulator wins; the other tiers stay selectable at run time.
+// 791 ms, A + B1 + K4 + K8 927 ms, A + W8 + W16 + K4 + K8 994 ms.  The dense
+// tier's later forms (below) took A + B1 + C to 358 ms and A + C to 348 ms:
+// the staged dense tier is now faster than B1 on B1's rows too.  The rows
+// there reach 8000+ distinct columns before thresholding, where the dense
+// tier's device-memory accumulator wins; the other tiers stay selectable at
+// run time.
 #ifndef B200_X2_TIERS
-#define B200_X2_TIERS 0x05
+#define B200_X2_TIERS 0x01
 #endif
 #ifndef B200_C_BLOCKS
 #define B200_C_BLOCKS 6

@@ -289,16 +289,27 @@ __global__ void threshold_kernel(const T *Av, const int *Ai, const int *An, int 
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
     {
         const int n = An[i];
+        const T *av = Av + (size_t) i * lda;
+        const int *ai = Ai + (size_t) i * lda;
+        // the next 32 entries are loaded before this chunk's are written
+        // (in place, writes land below the chunk being read)
+        T xn = T(0);
+        int kn = 0;
+        if (lane < n)
+        {
+            xn = av[lane];
+            kn = ai[lane];
+        }
         int ll = 0;
         for (int c0 = 0; c0 < n; c0 += 32)
         {
             const int q = c0 + lane;
-            T x = T(0);
-            int k = 0;
-            if (q < n)
+            const T x = xn;
+            const int k = kn;
+            if (q + 32 < n)
             {
-                x = Av[(size_t) i * lda + q];
-                k = Ai[(size_t) i * lda + q];
+                xn = av[q + 32];
+                kn = ai[q + 32];
             }
             const bool keep = q < n && fabs(x) > thr_t;
             const unsigned bal = __ballot_sync(FULL, keep);
@@ -315,6 +326,29 @@ __global__ void threshold_kernel(const T *Av, const int *Ai, const int *An, int 
     }
 }
 
+// One warp moves n 4-byte words from src to dst (both 16-byte aligned; rows
+// start on 32-entry boundaries): 16-byte vectors, four in flight per lane,
+// then the words past the last whole vector.
+__device__ __forceinline__ void warp_copy_words(unsigned *dst, const unsigned *src, int n, int lane)
+{
+    const int nv = n >> 2;
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+    int v = lane;
+    for (; v + 96 < nv; v += 128)
+    {
+        const uint4 a = s4[v], b = s4[v + 32], c = s4[v + 64], d = s4[v + 96];
+        d4[v] = a;
+        d4[v + 32] = b;
+        d4[v + 64] = c;
+        d4[v + 96] = d;
+    }
+    for (; v < nv; v += 32)
+        d4[v] = s4[v];
+    for (int w = (nv << 2) + lane; w < n; w += 32)
+        dst[w] = src[w];
+}
+
 // scale: B = s*A over the stored entries (the reference scales the padded
 // N*M array with BLAS ?scal, bml_scale_ellpack_typed.c:85,119; entries past
 // nnz are never read).  One warp per row.
@@ -322,19 +356,49 @@ template <typename T>
 __global__ void scale_kernel(const T *Av, const int *Ai, const int *An, int lda, T *Bv, int *Bi,
                              int *Bn, int ldb, int N, T s, int copy_structure)
 {
+    constexpr int E = 16 / sizeof(T); // entries per 16-byte vector
+    struct alignas(16) Vec
+    {
+        T v[E];
+    };
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
     {
         const int n = An[i];
-        for (int p = lane; p < n; p += 32)
+        const Vec *a = reinterpret_cast<const Vec *>(Av + (size_t) i * lda);
+        Vec *b = reinterpret_cast<Vec *>(Bv + (size_t) i * ldb);
+        const int nv = n / E;
+        int v = lane;
+        for (; v + 32 < nv; v += 64)
         {
-            Bv[(size_t) i * ldb + p] = mul_rn(s, Av[(size_t) i * lda + p]);
-            if (copy_structure)
-                Bi[(size_t) i * ldb + p] = Ai[(size_t) i * lda + p];
+            Vec x = a[v], y = a[v + 32];
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+            {
+                x.v[e] = mul_rn(s, x.v[e]);
+                y.v[e] = mul_rn(s, y.v[e]);
+            }
+            b[v] = x;
+            b[v + 32] = y;
         }
-        if (copy_structure && lane == 0)
-            Bn[i] = n;
+        for (; v < nv; v += 32)
+        {
+            Vec x = a[v];
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                x.v[e] = mul_rn(s, x.v[e]);
+            b[v] = x;
+        }
+        for (int p = nv * E + lane; p < n; p += 32)
+            Bv[(size_t) i * ldb + p] = mul_rn(s, Av[(size_t) i * lda + p]);
+        if (copy_structure)
+        {
+            warp_copy_words(reinterpret_cast<unsigned *>(Bi + (size_t) i * ldb),
+                            reinterpret_cast<const unsigned *>(Ai + (size_t) i * lda), n, lane);
+            if (lane == 0)
+                Bn[i] = n;
+        }
     }
 }
 
@@ -349,11 +413,11 @@ __global__ void copy_kernel(const T *Av, const int *Ai, const int *An, int lda, 
     {
         const int n = An[i];
         const int m = min(n, Mb);
-        for (int p = lane; p < m; p += 32)
-        {
-            Bv[(size_t) i * ldb + p] = Av[(size_t) i * lda + p];
-            Bi[(size_t) i * ldb + p] = Ai[(size_t) i * lda + p];
-        }
+        warp_copy_words(reinterpret_cast<unsigned *>(Bv + (size_t) i * ldb),
+                        reinterpret_cast<const unsigned *>(Av + (size_t) i * lda),
+                        m * (int) (sizeof(T) / 4), lane);
+        warp_copy_words(reinterpret_cast<unsigned *>(Bi + (size_t) i * ldb),
+                        reinterpret_cast<const unsigned *>(Ai + (size_t) i * lda), m, lane);
         if (lane == 0)
         {
             Bn[i] = m;
@@ -439,40 +503,71 @@ __global__ void trace_mult_kernel(const T *Av, const int *Ai, const int *An, int
 // `radius += (double) |a|` into a variable of the matrix precision; dvalue =
 // the last diagonal entry; hi = dvalue + radius, lo = dvalue - radius in the
 // matrix precision.
+// One lane per row, so each row's sum runs in row order in one thread; the
+// warp stages its 32 rows through shared memory 32 entries at a time, each
+// row's entries read by one coalesced load.
+constexpr int GER_WARPS = 4;
+
 template <typename T>
-__global__ void gershgorin_kernel(const T *Av, const int *Ai, const int *An, int ld, int N,
-                                  double *hi, double *lo)
+__global__ void __launch_bounds__(GER_WARPS * 32) gershgorin_kernel(const T *Av, const int *Ai,
+                                                                    const int *An, int ld, int N,
+                                                                    double *hi, double *lo)
 {
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    __shared__ T tv[GER_WARPS][32][33];
+    __shared__ unsigned char tdg[GER_WARPS][32][33]; // entry is on the diagonal
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int groups = (N + 31) / 32;
+    for (int gi = blockIdx.x * GER_WARPS + w; gi < groups; gi += gridDim.x * GER_WARPS)
     {
-        const int n = An[i];
-        // The sum runs in row order, so one lane walks the row; the row is
-        // read in 32-wide chunks so the loads stay coalesced.
+        const int i = gi * 32 + lane; // this lane's row
+        const int n = i < N ? An[i] : 0;
+        int nmax = n;
+#pragma unroll
+        for (int o = 16; o; o >>= 1)
+            nmax = max(nmax, __shfl_xor_sync(FULL, nmax, o));
         T radius = T(0), dvalue = T(0);
-        for (int c0 = 0; c0 < n; c0 += 32)
+        for (int c0 = 0; c0 < nmax; c0 += 32)
         {
-            const int q = c0 + lane;
-            T v = T(0);
-            int k = -1;
-            if (q < n)
+            // row r of the group: its entries c0 .. c0 + 31, lane = entry;
+            // 16 rows' loads are issued before any is stored
+            for (int r0 = 0; r0 < 32; r0 += 16)
             {
-                v = Av[(size_t) i * ld + q];
-                k = Ai[(size_t) i * ld + q];
+                T v[16];
+                int k[16];
+#pragma unroll
+                for (int r = 0; r < 16; ++r)
+                {
+                    const int row = gi * 32 + r0 + r;
+                    const int nr = __shfl_sync(FULL, n, r0 + r);
+                    const int q = c0 + lane;
+                    v[r] = T(0);
+                    k[r] = -1;
+                    if (row < N && q < nr)
+                    {
+                        v[r] = Av[(size_t) row * ld + q];
+                        k[r] = Ai[(size_t) row * ld + q];
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < 16; ++r)
+                {
+                    tv[w][r0 + r][lane] = v[r];
+                    tdg[w][r0 + r][lane] = k[r] == gi * 32 + r0 + r;
+                }
             }
+            __syncwarp();
             const int m = min(32, n - c0);
             for (int t = 0; t < m; ++t)
             {
-                const T vt = __shfl_sync(FULL, v, t);
-                const int kt = __shfl_sync(FULL, k, t);
-                if (kt == i)
+                const T vt = tv[w][lane][t];
+                if (tdg[w][lane][t])
                     dvalue = vt;
                 else
                     radius = (T) __dadd_rn((double) radius, (double) fabs(vt));
             }
+            __syncwarp();
         }
-        if (lane == 0)
+        if (i < N)
         {
             hi[i] = (double) add_rn(dvalue, radius);
             lo[i] = (double) add_rn(dvalue, (T) -radius);
@@ -972,12 +1067,12 @@ bool ell_gershgorin(bml_matrix_ellpack_t *A, double *bounds)
     if (!hi)
         return false;
     double *lo = hi + A->N;
-    const int grid = rows_grid(c, A->N, 8);
+    const int grid = max(1, min(b200_ceil_div(A->N, 32 * GER_WARPS), c->sm_count * 8));
     if (A->matrix_precision == double_real)
-        gershgorin_kernel<double><<<grid, 256, 0, c->stream>>>(
+        gershgorin_kernel<double><<<grid, GER_WARPS * 32, 0, c->stream>>>(
             static_cast<const double *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->N, hi, lo);
     else
-        gershgorin_kernel<float><<<grid, 256, 0, c->stream>>>(
+        gershgorin_kernel<float><<<grid, GER_WARPS * 32, 0, c->stream>>>(
             static_cast<const float *>(A->d_value), A->d_index, A->d_nnz, A->ld, A->N, hi, lo);
     double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 3072);
     // emax starts at DBL_MIN and emin at DBL_MAX, as in the reference (:88-89).

@@ -295,7 +295,7 @@ BML_B200_API int bml_b200_last_tier_counts(int *counts, int n);
 
 /* Selects the multiply tiers later ELLPACK multiplies may use: bit t enables
  * tier t in the order of bml_b200_last_tier_counts; the dense tier C is
- * always enabled; 0 restores the default.  Any choice gives the same result
+ * always enabled; 0 restores the default (A and C).  Any choice gives the same result
  * (the tiers differ only in speed), and rows a tier cannot hold move on to the
  * next enabled one.  Also discards the per-row width estimates kept from the
  * last multiply.  Returns the previous mask.  No reference counterpart. */
