@@ -135,3 +135,43 @@ def test_rows_handed_on_from_a_full_warp(oracle_mod, tier):
     assert tr[1] == pytest.approx(tr_ref[1], rel=1e-12)
     # the rows entered the tier and were handed on to the dense tier
     assert counts[B.X2_TIERS.index(tier)] > 0 and counts[B.X2_TIERS.index("C")] > 0, counts
+
+
+def _wide_random_rows(N, lo, hi, empty, seed):
+    """Rows of lo..hi random distinct columns in random order (the diagonal
+    among them), values U(-1, 1)/32, and the listed rows empty: rows of B
+    wider than the dense tier's 1024-entry staging unit, so one jp spans
+    several units, and jps that reference an empty row."""
+    rng = np.random.default_rng(seed)
+    M = hi
+    v = np.zeros(N * M)
+    ix = np.zeros(N * M, np.int32)
+    nz = np.zeros(N, np.int32)
+    for i in range(N):
+        if i in empty:
+            continue
+        w = int(rng.integers(lo, hi + 1))
+        cols = rng.choice(np.delete(np.arange(N), i), size=w - 1, replace=False)
+        cols = np.insert(cols, int(rng.integers(0, w)), i)
+        v[i * M:i * M + w] = rng.uniform(-1, 1, w) / 32
+        ix[i * M:i * M + w] = cols
+        nz[i] = w
+    return v, ix, nz, M
+
+
+@pytest.mark.parametrize("prec", [DOUBLE, SINGLE])
+def test_dense_tier_multi_unit_rows(oracle_mod, prec):
+    O = oracle_mod
+    N = 1100
+    v, ix, nz, M = _wide_random_rows(N, 1025, 1090, {3, 17, 600}, 11)
+    if prec == SINGLE:
+        v = v.astype(np.float32)
+    M2 = N
+    ref, tr_ref = _reference_x2(O, v, ix, nz, N, M, 1e-6, M2, prec=prec)
+    runs = _gpu_x2((v, ix, nz), N, M, M2, 1e-6, prec=prec)
+    for got, tr, counts in runs:
+        assert O.same_rows_exact(got, ref, M2, M2), "rows differ from the reference"
+        tol = 1e-12 if prec == DOUBLE else 1e-5
+        assert tr[0] == pytest.approx(tr_ref[0], rel=tol)
+        assert tr[1] == pytest.approx(tr_ref[1], rel=tol)
+        assert counts[B.X2_TIERS.index("C")] > 0, counts
