@@ -1113,14 +1113,27 @@ int bml_b200_ellpack_upload(bml_matrix_t *A, const void *value, const int *index
         return BML_B200_ERR_INVALID;
     }
     const size_t sz = prec_size(E->matrix_precision);
+    // Only the columns up to the widest row travel (entries past a row's nnz
+    // are never read).
+    int w = 0;
+    for (int i = 0; i < E->N; ++i)
+    {
+        if (nnz[i] < 0 || nnz[i] > E->M)
+        {
+            b200_set_error(BML_B200_ERR_INVALID, "ellpack_upload: nnz[%d] = %d outside [0, M=%d]", i, nnz[i],
+                           E->M);
+            return BML_B200_ERR_INVALID;
+        }
+        w = nnz[i] > w ? nnz[i] : w;
+    }
     // Write straight to the device; the host mirror becomes stale.
     B200Context *c = b200_ctx();
     if (!c)
         return b200_get_error();
-    if (!CUDA_OK(cudaMemcpy2DAsync(E->d_value, E->ld * sz, value, E->M * sz, E->M * sz, E->N,
-                                   cudaMemcpyHostToDevice, c->stream)) ||
-        !CUDA_OK(cudaMemcpy2DAsync(E->d_index, E->ld * sizeof(int), index, E->M * sizeof(int),
-                                   E->M * sizeof(int), E->N, cudaMemcpyHostToDevice, c->stream)) ||
+    if ((w > 0 && (!CUDA_OK(cudaMemcpy2DAsync(E->d_value, E->ld * sz, value, E->M * sz, w * sz, E->N,
+                                              cudaMemcpyHostToDevice, c->stream)) ||
+                   !CUDA_OK(cudaMemcpy2DAsync(E->d_index, E->ld * sizeof(int), index, E->M * sizeof(int),
+                                              w * sizeof(int), E->N, cudaMemcpyHostToDevice, c->stream)))) ||
         !CUDA_OK(cudaMemcpyAsync(E->d_nnz, nnz, (size_t) E->N * sizeof(int), cudaMemcpyHostToDevice,
                                  c->stream)) ||
         !b200_sync())
@@ -1143,13 +1156,22 @@ int bml_b200_ellpack_download(bml_matrix_t *A, void *value, int *index, int *nnz
     if (!c || !ell_to_device(E))
         return b200_get_error();
     const size_t sz = prec_size(E->matrix_precision);
-    if (!CUDA_OK(cudaMemcpy2DAsync(value, E->M * sz, E->d_value, E->ld * sz, E->M * sz, E->N,
-                                   cudaMemcpyDeviceToHost, c->stream)) ||
-        !CUDA_OK(cudaMemcpy2DAsync(index, E->M * sizeof(int), E->d_index, E->ld * sizeof(int),
-                                   E->M * sizeof(int), E->N, cudaMemcpyDeviceToHost, c->stream)) ||
-        !CUDA_OK(cudaMemcpyAsync(nnz, E->d_nnz, (size_t) E->N * sizeof(int), cudaMemcpyDeviceToHost,
+    // Row lengths first; then only the columns up to the widest row travel
+    // (entries past a row's nnz are left as the caller had them).
+    if (!CUDA_OK(cudaMemcpyAsync(nnz, E->d_nnz, (size_t) E->N * sizeof(int), cudaMemcpyDeviceToHost,
                                  c->stream)) ||
         !b200_sync())
+        return b200_get_error();
+    int w = 0;
+    for (int i = 0; i < E->N; ++i)
+        w = nnz[i] > w ? nnz[i] : w;
+    w = w < E->M ? w : E->M;
+    if (w > 0 &&
+        (!CUDA_OK(cudaMemcpy2DAsync(value, E->M * sz, E->d_value, E->ld * sz, w * sz, E->N,
+                                    cudaMemcpyDeviceToHost, c->stream)) ||
+         !CUDA_OK(cudaMemcpy2DAsync(index, E->M * sizeof(int), E->d_index, E->ld * sizeof(int),
+                                    w * sizeof(int), E->N, cudaMemcpyDeviceToHost, c->stream)) ||
+         !b200_sync()))
         return b200_get_error();
     return BML_B200_OK;
 }

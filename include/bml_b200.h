@@ -302,7 +302,10 @@ BML_B200_API int bml_b200_last_tier_counts(int *counts, int n);
 BML_B200_API int bml_b200_set_x2_tiers(int mask);
 
 /* Raw ELLPACK transfer between the device matrix and caller host arrays laid
- * out like the reference (row-major value[N*M], index[N*M], nnz[N]). */
+ * out like the reference (row-major value[N*M], index[N*M], nnz[N]).  Only
+ * the columns up to the widest row are transferred: entries past a row's nnz
+ * are neither read from the device nor written to the caller's arrays.
+ * Upload rejects an nnz outside [0, M] (BML_B200_ERR_INVALID). */
 BML_B200_API int bml_b200_ellpack_upload(bml_matrix_t *A, const void *value,
     const int *index, const int *nnz);
 BML_B200_API int bml_b200_ellpack_download(bml_matrix_t *A, void *value, int *index,
