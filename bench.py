@@ -453,7 +453,7 @@ def run_reference(args, rank, world):
               "bml ELLPACK OpenMP CPU path on %d threads" % (steps, warm, SP2_ITERS, threads))
     return {"impl": "reference", "metric": METRIC, "value": dt, "unit": "s", "n_gpus": world,
             "steps": steps, "warmup": warm, "ms_per_step": dt * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded splitmix64 lattice Hamiltonian)",
             "config": {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
                        "sp2_iterations": SP2_ITERS},
