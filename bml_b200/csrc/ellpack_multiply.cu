@@ -506,11 +506,13 @@ __global__ void __launch_bounds__(W * 32, MINB) team_kernel(MulArgs g, const int
     unsigned ucount = 0; // units consumed by this block (uniform)
     for (;;)
     {
+        // one thread decides (a flag read by every thread could change
+        // between their reads and split the block at the barrier)
         if (tid == 0)
-            misc->row = atomicAdd(&tl->cursor[tier], 1);
+            misc->row = *reinterpret_cast<volatile int *>(tflag) ? nrows : atomicAdd(&tl->cursor[tier], 1);
         __syncthreads();
         const int pos = misc->row;
-        if (pos >= nrows || *reinterpret_cast<volatile int *>(tflag))
+        if (pos >= nrows)
             break;
         const int i = rows[pos];
         for (int s = tid; s < TS; s += NT)
@@ -2011,11 +2013,13 @@ __global__ void __launch_bounds__(W * 32, MINB) dense_staged_kernel(MulArgs g, i
     unsigned ucount = 0; // units consumed by this block (uniform)
     for (;;)
     {
+        // one thread decides (a flag read by every thread could change
+        // between their reads and split the block at the barrier)
         if (tid == 0)
-            misc->row = atomicAdd(&tl->cursor[NTIERS - 1], 1);
+            misc->row = *reinterpret_cast<volatile int *>(tflag) ? nrows : atomicAdd(&tl->cursor[NTIERS - 1], 1);
         __syncthreads();
         const int pos = misc->row;
-        if (pos >= nrows || *reinterpret_cast<volatile int *>(tflag))
+        if (pos >= nrows)
             break;
         const int i = rows[pos];
         if (tid == 0)
