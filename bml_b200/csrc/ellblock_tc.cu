@@ -21,9 +21,13 @@
 // writes every block of X in that layout, as the left operand (rows x k) and
 // as the right operand (columns x k, the block transposed), one contiguous
 // 2 KB image each, so staging is one bulk copy (cp.async.bulk, completing on
-// an mbarrier) per block, issued by the lanes of a producer warp into a ring
-// of buffers.  One thread issues the MMAs and releases each buffer with
-// tcgen05.commit on its mbarrier; every wait is bounded.
+// an mbarrier) per block, issued by one producer thread into rings of left
+// and right operand buffers.  One thread issues the MMAs and releases each
+// buffer with tcgen05.commit on its "empty" mbarrier.  Everything either
+// thread needs per pair is precomputed by the whole CTA when the wave's pair
+// list is built (the new-left-operand flag, the rows each tile touches), so
+// their loops hold only the waits, the copies and the MMAs.  Every wait is
+// bounded.
 #include "device_util.cuh"
 #include "ellblock.h"
 
@@ -48,8 +52,14 @@ constexpr int IMG = TB * TB;      // bf16 elements per block image (2 KB)
 constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
 constexpr int TC_LCAP = 2048;     // product pairs per wave
 constexpr int TC_PCAP = 8192;     // product pairs per group
-constexpr int TC_ABUF = 4;        // left-operand buffers
-constexpr int TC_BBUF = 12;       // right-operand buffers (pipeline depth)
+#ifndef B200_TC_ABUF
+#define B200_TC_ABUF 6
+#endif
+#ifndef B200_TC_BBUF
+#define B200_TC_BBUF 12
+#endif
+constexpr int TC_ABUF = B200_TC_ABUF; // left-operand buffers
+constexpr int TC_BBUF = B200_TC_BBUF; // right-operand buffers (pipeline depth)
 
 // bf16 image of a block in the K-major no-swizzle layout, as a left operand
 // (element (r, k) of the block) or a right operand (element (n, k) = block
@@ -200,7 +210,17 @@ __device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32])
 // Shared memory of the X^2 kernel.
 struct TcSmem
 {
-    __nv_bfloat16 a[TC_ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
+    union
+    {
+        __nv_bfloat16 a[TC_ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
+        struct
+        {
+            unsigned jbits[TC_NWCAP]; // the group's block columns jb (bitmap over NB)
+            int jpre[TC_NWCAP];       // J entries before each bitmap word: index = rank of jb
+            unsigned kbits[TC_NWCAP]; // output block columns of the group (bitmap over NB)
+            int kpre[TC_NWCAP];       // tiles before each bitmap word: tile = rank of kb
+        } su; // the group's set-up, while the left-operand ring is idle
+    };
     union
     {
         __nv_bfloat16 b[TC_BBUF][2][IMG]; // right operands, hi and lo: 32 x 32 (2 KB each)
@@ -208,21 +228,19 @@ struct TcSmem
     };
     uint64_t full_a[TC_ABUF], full_b[TC_BBUF]; // bulk copies landed
     uint64_t empty_b[TC_BBUF];            // MMAs reading a B buffer (and all before) done
+    uint64_t empty_a[TC_ABUF];            // MMAs reading an A buffer's fill (and all before) done
     uint64_t done;                        // all MMAs of a wave done
     unsigned tmem;
     int nJ, nK, npairs, ok, dead;
     int jb[TC_JCAP];             // union of the group's block columns
     short jslot[TC_JCAP][TC_GROUP]; // position of X[ib0+q, jb] in row ib0+q, or -1
-    unsigned jbits[TC_NWCAP];    // the group's block columns jb (bitmap over NB)
-    int jpre[TC_NWCAP];          // J entries before each bitmap word: index = rank of jb
-    unsigned kbits[TC_NWCAP];    // output block columns of the group (bitmap over NB)
-    int kpre[TC_NWCAP];          // tiles before each bitmap word: tile = rank of kb
     int klist[TC_KCAP];          // kb of each output tile
     int jcnt[TC_JCAP];           // pairs of the current wave per J entry, then their start
     int list[TC_LCAP];           // pairs of the current wave: j << 20 | tile << 16 | kp
     int jstart[TC_JCAP + 1];     // first pair of each J entry in ptile
     unsigned short ptile[TC_PCAP]; // output tile of every pair (j, kp) of the group
-    unsigned char started[TC_TILES], touched[TC_TILES];
+    unsigned char jmask[TC_JCAP];  // rows q of the group holding X[ib0+q, jb]
+    int touched[TC_TILES];         // rows q of the group with a product in the tile
 };
 
 template <typename T> struct TcView
@@ -325,7 +343,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (tid == 0)
     {
         for (int i = 0; i < TC_ABUF; ++i)
+        {
             mbar_init1(&S.full_a[i]);
+            mbar_init1(&S.empty_a[i]);
+        }
         for (int i = 0; i < TC_BBUF; ++i)
         {
             mbar_init1(&S.full_b[i]);
@@ -340,16 +361,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const unsigned tbase = S.tmem;
     bool dead = false; // a wait timed out: stop issuing work
     // pipeline counters, kept alike by the producer (thread 0) and the MMA
-    // issuer (thread 32): pairs and left operands issued so far, and the
-    // producer's view of completed MMA commits per right-operand buffer
+    // issuer (thread 32): pairs and left operands issued so far
     unsigned gp = 0, ga = 0, nwaves = 0;
-    unsigned seen[TC_BBUF];
-    unsigned alast_b[TC_ABUF], alast_f[TC_ABUF];
-    for (int i = 0; i < TC_BBUF; ++i)
-        seen[i] = 0;
     unsigned copied_a = 0; // left operands whose copies thread 0 issued
-    for (int i = 0; i < TC_ABUF; ++i)
-        alast_b[i] = alast_f[i] = 0;
 
     for (int grp = blockIdx.x; grp < ngroups && !dead; grp += gridDim.x)
     {
@@ -359,8 +373,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int myrow = ib0 + warp; // block row of this warp (left operand q = warp)
         for (int s2 = tid; s2 < nwords; s2 += TC_THREADS)
         {
-            S.jbits[s2] = 0u;
-            S.kbits[s2] = 0u;
+            S.su.jbits[s2] = 0u;
+            S.su.kbits[s2] = 0u;
         }
         if (tid == 0)
             S.ok = 1;
@@ -373,7 +387,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (jb < 0 || jb >= X.NB)
                     bad = 1;
                 else
-                    atomicOr(&S.jbits[jb >> 5], 1u << (jb & 31));
+                    atomicOr(&S.su.jbits[jb >> 5], 1u << (jb & 31));
             }
         if (__syncthreads_or(bad))
         {
@@ -381,7 +395,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 atomicExch(&flags[2], 1);
             continue;
         }
-        rank_bits(S.jbits, S.jpre, S.jb, TC_JCAP, nwords, S.jcnt, &S.nJ, tid, lane, warp);
+        rank_bits(S.su.jbits, S.su.jpre, S.jb, TC_JCAP, nwords, S.jcnt, &S.nJ, tid, lane, warp);
         __syncthreads();
         if (S.nJ > TC_JCAP)
         {
@@ -397,9 +411,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int jp = lane; jp < X.nnzb[myrow]; jp += 32)
             {
                 const int jb = X.indexb[(size_t) myrow * X.MB + jp];
-                const int j = S.jpre[jb >> 5] + __popc(S.jbits[jb >> 5] & ((1u << (jb & 31)) - 1u));
+                const int j = S.su.jpre[jb >> 5] + __popc(S.su.jbits[jb >> 5] & ((1u << (jb & 31)) - 1u));
                 S.jslot[j][warp] = (short) jp;
             }
+        __syncthreads();
+        for (int j = tid; j < S.nJ; j += TC_THREADS)
+        {
+            unsigned char m = 0;
+            for (int q = 0; q < TC_GROUP; ++q)
+                if (S.jslot[j][q] >= 0)
+                    m |= (unsigned char) (1u << q);
+            S.jmask[j] = m;
+        }
         __syncthreads();
         const int nJ = S.nJ;
         // ---- output block columns K: a bitmap over NB, tiles by rank ----
@@ -413,7 +436,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (kb < 0 || kb >= X.NB)
                     badk = 1;
                 else
-                    atomicOr(&S.kbits[kb >> 5], 1u << (kb & 31));
+                    atomicOr(&S.su.kbits[kb >> 5], 1u << (kb & 31));
             }
         }
         if (__syncthreads_or(badk))
@@ -422,7 +445,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 S.ok = 0;
         }
         __syncthreads();
-        rank_bits(S.kbits, S.kpre, S.klist, TC_KCAP, nwords, S.jcnt, &S.nK, tid, lane, warp);
+        rank_bits(S.su.kbits, S.su.kpre, S.klist, TC_KCAP, nwords, S.jcnt, &S.nK, tid, lane, warp);
         __syncthreads();
         if (tid == 0 && S.nK > TC_KCAP)
             S.ok = 0;
@@ -467,9 +490,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             {
                 const int kb = X.indexb[(size_t) jb * X.MB + kp];
                 S.ptile[S.jstart[j] + kp] =
-                    (unsigned short) (S.kpre[kb >> 5] + __popc(S.kbits[kb >> 5] & ((1u << (kb & 31)) - 1u)));
+                    (unsigned short) (S.su.kpre[kb >> 5] + __popc(S.su.kbits[kb >> 5] & ((1u << (kb & 31)) - 1u)));
             }
         }
+        // the set-up area is the left-operand ring: order its generic
+        // accesses before the bulk copies that refill it
+        proxy_fence();
         __syncthreads();
         const int nK = S.nK;
         const int nW = (nK + TC_TILES - 1) / TC_TILES;
@@ -505,10 +531,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int t0 = w * TC_TILES;
             const int nt = min(TC_TILES, nK - t0);
             if (tid < TC_TILES)
-            {
-                S.started[tid] = 0;
                 S.touched[tid] = 0;
-            }
             __syncthreads();
             // pairs (j, kb) of this wave, ordered by j then kp: count per j,
             // prefix, write
@@ -565,104 +588,86 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         t = S.ptile[ps + kp];
                         in = t >= t0 && t < t0 + nt;
                     }
-                    const unsigned bal = __ballot_sync(FULL, in);
+                        const unsigned bal = __ballot_sync(FULL, in);
                     if (in)
-                        S.list[pos + __popc(bal & lanemask_lt())] = (j << 20) | ((t - t0) << 16) | kp;
+                    {
+                        const int at = pos + __popc(bal & lanemask_lt());
+                        // bit 30: the first pair of this j in the wave (a new left operand)
+                        S.list[at] = (at == S.jcnt[j] ? 1 << 30 : 0) | (j << 20) | ((t - t0) << 16) | kp;
+                        atomicOr(&S.touched[t - t0], (int) S.jmask[j]);
+                    }
                     pos += __popc(bal);
                 }
             }
             __syncthreads();
-            if (warp == 0)
+            if (tid == 0)
             {
-                // producer (warp 0): lane 0 waits on the ring and arms the
-                // barriers, the lanes issue one 2 KB bulk copy each
-                int curj = -1;
-                unsigned acur = 0;
+                // producer (thread 0): for each pair, its right operand into
+                // the next B buffer and, on a new j, the group's left operand
+                // into the next A buffer, each once the MMAs that read the
+                // buffer's previous fill are done
                 for (int p = p0; p < p1; ++p)
                 {
                     const int pv = S.list[p];
-                    const int j = pv >> 20, kp = pv & 0xFFFF;
+                    const int j = (pv >> 20) & 1023, kp = pv & 0xFFFF;
                     const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
-                    const bool switch_a = j != curj;
-                    const unsigned a = ga % TC_ABUF, fa = ga / TC_ABUF;
-                    int fail = 0;
-                    if (lane == 0)
+                    if (pv >> 30)
                     {
-                        if (f >= 1 && seen[b] < f)
+                        const unsigned a = ga % TC_ABUF, fa = ga / TC_ABUF;
+                        if (fa >= 1 && !mbar_wait2s(&S.empty_a[a], (fa - 1) & 1))
                         {
-                            if (!mbar_wait2s(&S.empty_b[b], (f - 1) & 1))
-                                fail = 1;
-                            seen[b] = f;
+                            S.dead = 1;
+                            break;
                         }
-                        if (!fail && switch_a && fa >= 1)
+                        mbar_expect(&S.full_a[a], 2 * 4 * IMG * 2);
+#pragma unroll
+                        for (int q = 0; q < TC_GROUP; ++q)
                         {
-                            // the last MMAs that read this buffer must be done
-                            const unsigned lb = alast_b[a], need = alast_f[a] + 1;
-                            if (seen[lb] < need)
+                            const int jp = S.jslot[j][q];
+#pragma unroll
+                            for (int part = 0; part < 2; ++part)
                             {
-                                if (!mbar_wait2s(&S.empty_b[lb], (need - 1) & 1))
-                                    fail = 1;
-                                seen[lb] = need;
+                                const __nv_bfloat16 *src =
+                                    jp >= 0 ? img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG : zimg;
+                                bulk_copy(reinterpret_cast<unsigned char *>(S.a[a][part]) + q * 2048, src, IMG * 2,
+                                          &S.full_a[a]);
                             }
                         }
-                        if (!fail)
-                        {
-                            if (switch_a)
-                                mbar_expect(&S.full_a[a], 2 * 4 * IMG * 2);
-                            mbar_expect(&S.full_b[b], 2 * IMG * 2);
-                        }
-                    }
-                    if (__shfl_sync(FULL, fail, 0))
-                    {
-                        if (lane == 0)
-                            S.dead = 1;
-                        break;
-                    }
-                    if (switch_a)
-                    {
-                        if (lane < 2 * TC_GROUP)
-                        {
-                            const int part = lane >> 2, q = lane & 3;
-                            const int jp = S.jslot[j][q];
-                            const __nv_bfloat16 *src =
-                                jp >= 0 ? img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG : zimg;
-                            bulk_copy(reinterpret_cast<unsigned char *>(S.a[a][part]) + q * 2048, src, IMG * 2,
-                                      &S.full_a[a]);
-                        }
-                        curj = j;
-                        acur = a;
                         ++ga;
                         copied_a = ga;
                     }
-                    if (lane < 2)
-                        bulk_copy(S.b[b][lane], img + (((size_t) S.jb[j] * X.MB + kp) * 4 + 2 + lane) * IMG, IMG * 2,
-                                  &S.full_b[b]);
-                    alast_b[acur] = b;
-                    alast_f[acur] = f;
+                    if (f >= 1 && !mbar_wait2s(&S.empty_b[b], (f - 1) & 1))
+                    {
+                        S.dead = 1;
+                        break;
+                    }
+                    mbar_expect(&S.full_b[b], 2 * IMG * 2);
+                    const __nv_bfloat16 *bsrc = img + ((size_t) S.jb[j] * X.MB + kp) * 4 * IMG;
+                    bulk_copy(S.b[b][0], bsrc + 2 * IMG, IMG * 2, &S.full_b[b]);
+                    bulk_copy(S.b[b][1], bsrc + 3 * IMG, IMG * 2, &S.full_b[b]);
                     ++gp;
                 }
             }
-            else if (warp == 1)
+            else if (tid == 32)
             {
-              if (lane == 0)
-              {
-                // MMA issuer: the same sequence, consuming the ring
-                int curj = -1;
-                unsigned acur = 0;
-                for (int p = p0; p < p1 && !*reinterpret_cast<volatile int *>(&S.dead); ++p)
+                // MMA issuer (thread 32): the same sequence, consuming the
+                // ring; the first MMA into a tile in this wave overwrites it
+                unsigned started = 0, acur = 0;
+                for (int p = p0; p < p1; ++p)
                 {
                     const int pv = S.list[p];
-                    const int j = pv >> 20, tile = (pv >> 16) & 15;
+                    const int tile = (pv >> 16) & 15;
                     const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
-                    if (j != curj)
+                    if (pv >> 30)
                     {
+                        if (p > p0)
+                            umma_commit(&S.empty_a[acur]); // the previous left operand is done with
                         acur = ga % TC_ABUF;
                         if (!mbar_wait2s(&S.full_a[acur], (ga / TC_ABUF) & 1))
                         {
                             S.dead = 1;
                             break;
                         }
-                        curj = j;
                         ++ga;
                     }
                     if (!mbar_wait2s(&S.full_b[b], f & 1))
@@ -674,7 +679,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const unsigned d = tbase + (unsigned) (tile * 32);
                     const unsigned a0 = su32(S.a[acur][0]), a1 = su32(S.a[acur][1]);
                     const unsigned b0 = su32(S.b[b][0]), b1 = su32(S.b[b][1]);
-                    unsigned acc = S.started[tile];
+                    unsigned acc = (started >> tile) & 1u;
+                    started |= 1u << tile;
 #pragma unroll
                     for (int ks = 0; ks < 2; ++ks)
                     {
@@ -689,21 +695,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         acc = 1u;
                     }
                     umma_commit(&S.empty_b[b]);
-                    S.started[tile] = 1;
-                    unsigned char m = 0;
-                    for (int q = 0; q < TC_GROUP; ++q)
-                        if (S.jslot[j][q] >= 0)
-                            m |= (unsigned char) (1u << q);
-                    S.touched[tile] |= m;
                     ++gp;
                 }
-                // every MMA of the wave (and before) done -> done barrier
+                // the wave's last left operand, then every MMA of the wave
+                // (and before) done -> done barrier
+                if (p1 > p0)
+                    umma_commit(&S.empty_a[acur]);
                 umma_commit(&S.done);
-              }
-              // the other lanes wait here, not in a polling loop beside the
-              // issuing lane
-              __syncwarp();
             }
+            // the other lanes of warps 0 and 1 wait here, not in a polling
+            // loop beside their working lane
+            __syncwarp();
             // the producer's and issuer's counters must stay alike: both
             // walked every pair of the wave unless the wave died
             const bool late = !mbar_wait2s(&S.done, nwaves & 1);
