@@ -53,6 +53,28 @@ def test_multiply_AB_bit_exact(oracle_mod):
         O.ref_free(RC)
 
 
+@pytest.mark.parametrize("alpha,beta,thr", [(1.2, 0.8, 0.0), (1.0, -1.0, 1e-4)])
+def test_multiply_general_bit_exact(oracle_mod, alpha, beta, thr):
+    """C <- alpha*A*B + beta*C, the reference's bml_multiply (the reference
+    test multiply_matrix_typed.c uses alpha 1.2, beta 0.8): a product into a
+    temporary, then the add."""
+    O = oracle_mod
+    v1, ix1, nz1, N, M = lattice(seed=0)
+    v2, ix2, nz2, _, _ = lattice(seed=7)
+    v3, ix3, nz3, _, _ = lattice(seed=11)
+    Mc = 1024
+    pad = lambda a: np.pad(a.reshape(N, M), ((0, 0), (0, Mc - M))).reshape(-1)
+    RA, GA = both(O, v1, ix1, nz1, N, M)
+    RB, GB = both(O, v2, ix2, nz2, N, M)
+    RC, GC = both(O, pad(v3), pad(ix3), nz3, N, Mc)
+    O.ref().bml_multiply(RA, RB, RC, alpha, beta, thr)
+    B.lib.bml_multiply(GA.h, GB.h, GC.h, alpha, beta, thr)
+    B.check()
+    assert_same(O, RC, GC, Mc)
+    for R in (RA, RB, RC):
+        O.ref_free(R)
+
+
 @pytest.mark.parametrize("alpha,beta,thr", [(2.0, -1.0, 1e-5), (1.0, 1.0, 0.0), (0.0, 0.5, 1e-3),
                                             (1.2, 0.0, 1e-2), (-0.7, 0.3, 0.0)])
 def test_add_bit_exact(oracle_mod, alpha, beta, thr):
