@@ -92,21 +92,25 @@ inline int rows_grid(B200Context *c, int N, int rows_per_block)
 // place only after it has been read.
 // Shared memory per team: keys[TS] pos[TS] xa[ldA](T) ka[ldA] newpos[ldB] cnt.
 // ---------------------------------------------------------------------------
+constexpr int ADD_U = 8; // entries per thread in flight in the add's loads
+
 template <typename T, int W>
 __global__ void __launch_bounds__(W * 32) add_kernel(T *Av, int *Ai, int *An, int lda, int Ma,
                                                    const T *Bv, const int *Bi, const int *Bn,
                                                    int ldb, int N, double alpha, double beta,
                                                    double thr, int logts, int *overflow)
 {
+    constexpr int NT = W * 32;
     extern __shared__ __align__(128) unsigned char smem[];
     const int TS = 1 << logts;
     const unsigned mask = TS - 1;
-    T *xa = reinterpret_cast<T *>(smem);
-    int *ka = reinterpret_cast<int *>(xa + lda);
+    T *xa = reinterpret_cast<T *>(smem);    // A's entries, then x = alpha*a (+ beta*b)
+    T *newx = xa + lda;                      // B's new entries: x = beta*b, by warp segment
+    int *ka = reinterpret_cast<int *>(newx + ldb);
     int *keys = ka + lda;
     int *pos = keys + TS;
-    int *newb = pos + TS;   // B positions of new columns, in B order
-    int *cnt = newb + ldb;  // [2][W]
+    int *newk = pos + TS;
+    int *cnt = newk + ldb; // [W]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
     const T thr_t = (T) thr;
     const bool use_a = alpha > 0.0 || alpha < 0.0;
@@ -114,100 +118,157 @@ __global__ void __launch_bounds__(W * 32) add_kernel(T *Av, int *Ai, int *An, in
 
     for (int i = blockIdx.x; i < N; i += gridDim.x)
     {
-        for (int s = tid; s < TS; s += W * 32)
+        for (int s = tid; s < TS; s += NT)
             keys[s] = B200_EMPTY_KEY;
         __syncthreads();
         const int na = use_a ? An[i] : 0;
         const int nb = use_b ? Bn[i] : 0;
-        // stage A's row: x = 0 + alpha*a
-        for (int p = tid; p < na; p += W * 32)
+        // A's row into shared memory: x = 0 + alpha*a, column -> position
+        // (ADD_U entries per thread loaded before any is stored)
+        for (int p0 = 0; p0 < na; p0 += NT * ADD_U)
         {
-            const int k = Ai[(size_t) i * lda + p];
-            ka[p] = k;
-            xa[p] = axpy_d(T(0), alpha, Av[(size_t) i * lda + p]);
-            hash_put(keys, pos, mask, k, p);
+            int kk[ADD_U];
+            T aa[ADD_U];
+#pragma unroll
+            for (int u = 0; u < ADD_U; ++u)
+            {
+                const int p = p0 + u * NT + tid;
+                kk[u] = p < na ? Ai[(size_t) i * lda + p] : 0;
+                aa[u] = p < na ? Av[(size_t) i * lda + p] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < ADD_U; ++u)
+            {
+                const int p = p0 + u * NT + tid;
+                if (p < na)
+                {
+                    ka[p] = kk[u];
+                    xa[p] = axpy_d(T(0), alpha, aa[u]);
+                    hash_put(keys, pos, mask, kk[u], p);
+                }
+            }
         }
         __syncthreads();
-        // B's contributions: existing columns update xa, new ones are listed
-        // in B order (warp-contiguous chunks + cross-warp prefix).
+        // B's row, one contiguous segment per warp: a column of A's row takes
+        // x + beta*b (one writer: B's columns are distinct); a new column is
+        // listed at its segment's start, in B order
+        const int seg = b200_round_up(b200_ceil_div(max(nb, 1), W), 32);
+        const int s0 = min(warp * seg, nb), s1 = min(s0 + seg, nb);
+        int local = 0;
+        for (int q0 = s0; q0 < s1; q0 += 32 * ADD_U)
+        {
+            int kk[ADD_U];
+            T bb[ADD_U];
+#pragma unroll
+            for (int u = 0; u < ADD_U; ++u)
+            {
+                const int q = q0 + u * 32 + lane;
+                kk[u] = q < s1 ? Bi[(size_t) i * ldb + q] : 0;
+                bb[u] = q < s1 ? Bv[(size_t) i * ldb + q] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < ADD_U; ++u)
+            {
+                const int q = q0 + u * 32 + lane;
+                bool isnew = false;
+                if (q < s1)
+                {
+                    const int p = hash_get(keys, pos, mask, kk[u]);
+                    if (p >= 0)
+                        xa[p] = axpy_d(xa[p], beta, bb[u]);
+                    else
+                        isnew = true;
+                }
+                const unsigned bal = __ballot_sync(FULL, isnew);
+                if (isnew)
+                {
+                    const int at = s0 + local + __popc(bal & lanemask_lt());
+                    newk[at] = kk[u];
+                    newx[at] = axpy_d(T(0), beta, bb[u]);
+                }
+                local += __popc(bal);
+            }
+        }
+        if (lane == 0)
+            cnt[warp] = local;
+        __syncthreads();
+        int npre[W];
         int nnew = 0;
-        for (int c0 = 0; c0 < nb; c0 += W * 32)
+#pragma unroll
+        for (int w = 0; w < W; ++w)
         {
-            const int q = c0 + warp * 32 + lane;
-            bool isnew = false;
-            if (q < nb)
-            {
-                const int k = Bi[(size_t) i * ldb + q];
-                const int p = hash_get(keys, pos, mask, k);
-                if (p >= 0)
-                    xa[p] = axpy_d(xa[p], beta, Bv[(size_t) i * ldb + q]);
-                else
-                    isnew = true;
-            }
-            const unsigned bal = __ballot_sync(FULL, isnew);
-            if (lane == 0)
-                cnt[((c0 / (W * 32)) & 1) * W + warp] = __popc(bal);
-            __syncthreads();
-            int pre = 0, tot = 0;
-            for (int w = 0; w < W; ++w)
-            {
-                const int cw = cnt[((c0 / (W * 32)) & 1) * W + w];
-                pre += w < warp ? cw : 0;
-                tot += cw;
-            }
-            if (isnew)
-                newb[nnew + pre + __popc(bal & lanemask_lt())] = q;
-            nnew += tot;
+            npre[w] = nnew;
+            nnew += cnt[w];
         }
-        __syncthreads();
-        // compaction: A's entries then the new B entries
+        // the sum's entries: A's, then the new ones; e -> (column, value)
+        auto entry = [&](int e, int &k, T &x) {
+            if (e < na)
+            {
+                k = ka[e];
+                x = xa[e];
+                return;
+            }
+            const int r = e - na;
+            int w = 0, base = 0;
+#pragma unroll
+            for (int v = 1; v < W; ++v)
+                if (r >= npre[v])
+                {
+                    w = v;
+                    base = npre[v];
+                }
+            const int at = w * seg + (r - base);
+            k = newk[at];
+            x = newx[at];
+        };
         const int total = na + nnew;
-        int ll = 0;
-        int round = 0;
-        for (int c0 = 0; c0 < total; c0 += W * 32, ++round)
+        const int seg3 = b200_round_up(b200_ceil_div(max(total, 1), W), 32);
+        const int e0 = min(warp * seg3, total), e1 = min(e0 + seg3, total);
+        int kept = 0;
+        for (int c0 = e0; c0 < e1; c0 += 32)
         {
-            const int q = c0 + warp * 32 + lane;
-            T x = T(0);
+            const int e = c0 + lane;
             int k = 0;
-            if (q < na)
-            {
-                x = xa[q];
-                k = ka[q];
-            }
-            else if (q < total)
-            {
-                const int bq = newb[q - na];
-                k = Bi[(size_t) i * ldb + bq];
-                x = axpy_d(T(0), beta, Bv[(size_t) i * ldb + bq]);
-            }
-            const bool keep = q < total && fabs(x) > thr_t;
+            T x = T(0);
+            if (e < e1)
+                entry(e, k, x);
+            kept += __popc(__ballot_sync(FULL, e < e1 && fabs(x) > thr_t));
+        }
+        __syncthreads(); // every thread has read cnt
+        if (lane == 0)
+            cnt[warp] = kept;
+        __syncthreads();
+        int ll = 0, total_kept = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+        {
+            ll += w < warp ? cnt[w] : 0;
+            total_kept += cnt[w];
+        }
+        for (int c0 = e0; c0 < e1; c0 += 32)
+        {
+            const int e = c0 + lane;
+            int k = 0;
+            T x = T(0);
+            if (e < e1)
+                entry(e, k, x);
+            const bool keep = e < e1 && fabs(x) > thr_t;
             const unsigned bal = __ballot_sync(FULL, keep);
-            if (lane == 0)
-                cnt[(round & 1) * W + warp] = __popc(bal);
-            __syncthreads();
-            int pre = 0, tot = 0;
-            for (int w = 0; w < W; ++w)
-            {
-                const int cw = cnt[(round & 1) * W + w];
-                pre += w < warp ? cw : 0;
-                tot += cw;
-            }
-            const int p = ll + pre + __popc(bal & lanemask_lt());
+            const int p = ll + __popc(bal & lanemask_lt());
             if (keep && p < Ma)
             {
                 Av[(size_t) i * lda + p] = x;
                 Ai[(size_t) i * lda + p] = k;
             }
-            ll += tot;
+            ll += __popc(bal);
         }
-        __syncthreads();
         if (tid == 0)
         {
-            An[i] = min(ll, Ma);
-            if (ll > Ma)
+            An[i] = min(total_kept, Ma);
+            if (total_kept > Ma)
                 atomicExch(overflow, 1);
         }
-        __syncthreads();
+        __syncthreads(); // before the next row reuses the shared arrays
     }
 }
 
@@ -719,25 +780,28 @@ bool ell_add(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double alpha, dou
     int *ovf = zeroed_flag(c);
     if (!ovf)
         return false;
-    const int need = 2 * (A->M + B->M);
+    // the hash holds A's row at most half full
+    const int need = 2 * A->M;
     int logts = 5;
     while ((1 << logts) < need)
         ++logts;
     const size_t sz = prec_size(A->matrix_precision);
-    const size_t smem = (size_t) A->ld * (sz + 4) + ((size_t) 2 << logts) * 4 + (size_t) B->ld * 4 +
-                        2 * 8 * 4 + 64;
+    // xa[lda] newx[ldb] (matrix precision) | ka[lda] keys[TS] pos[TS] newk[ldb] cnt[8]
+    const size_t smem = (size_t) (A->ld + B->ld) * (sz + 4) + ((size_t) 2 << logts) * 4 + 8 * 4 + 64;
     if (smem > c->smem_optin)
     {
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "add: rows of width %d/%d exceed shared memory",
                        A->M, B->M);
         return false;
     }
-    const int grid = min(A->N, c->sm_count * 8);
     if (A->matrix_precision == double_real)
     {
         auto k = add_kernel<double, 8>;
         if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
             return false;
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem);
+        const int grid = min(A->N, c->sm_count * (occ > 0 ? occ : 1));
         k<<<grid, 256, smem, c->stream>>>(static_cast<double *>(A->d_value), A->d_index, A->d_nnz,
                                           A->ld, A->M, static_cast<const double *>(B->d_value),
                                           B->d_index, B->d_nnz, B->ld, A->N, alpha, beta,
@@ -748,6 +812,9 @@ bool ell_add(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double alpha, dou
         auto k = add_kernel<float, 8>;
         if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
             return false;
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem);
+        const int grid = min(A->N, c->sm_count * (occ > 0 ? occ : 1));
         k<<<grid, 256, smem, c->stream>>>(static_cast<float *>(A->d_value), A->d_index, A->d_nnz,
                                           A->ld, A->M, static_cast<const float *>(B->d_value),
                                           B->d_index, B->d_nnz, B->ld, A->N, alpha, beta,
