@@ -642,9 +642,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         break;
                     }
                     mbar_expect(&S.full_b[b], 2 * IMG * 2);
+                    // the right hi and lo images are adjacent in both places:
+                    // one 4 KB copy
                     const __nv_bfloat16 *bsrc = img + ((size_t) S.jb[j] * X.MB + kp) * 4 * IMG;
-                    bulk_copy(S.b[b][0], bsrc + 2 * IMG, IMG * 2, &S.full_b[b]);
-                    bulk_copy(S.b[b][1], bsrc + 3 * IMG, IMG * 2, &S.full_b[b]);
+                    bulk_copy(S.b[b][0], bsrc + 2 * IMG, 2 * IMG * 2, &S.full_b[b]);
                     ++gp;
                 }
             }
