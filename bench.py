@@ -373,8 +373,8 @@ def x2_roofline(B, H, info):
     return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "peak_source": src, "traffic": DRAM_BYTES_PER_PRODUCT * P,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dense tier on the 30^3 "
-                              "case (134.6 GB for 18.57 G products, profiles/x2_dense_tier_lattice30.md), "
-                              "scaled by this call's products",
+                              "case (bench.py --profile: 134.6 GB for 18.57 G products), scaled by this "
+                              "call's products",
             "kernel": "one ELLPACK X^2 call (tier kernels together) on the SP2 iterate of iteration %d"
                       % (SP2_ITERS - 1),
             "x2_seconds": t, "nnz_x": int(nnz_x), "nnz_x2": int(nnz_x2), "products": P,
