@@ -574,7 +574,7 @@ def run_profile_tc():
 def ellblock_leg(reps=3):
     """The mixed ELLBLOCK configuration's product: X^2 of H on the 16^3 block
     lattice (4096 block rows of 32, N = 131072, threshold 1e-6), on the
-    tensor cores (BF16 hi/lo split) against the FP64 block product, device
+    tensor cores (scaled FP16 hi/lo split) against the FP64 block product, device
     times by CUDA events and the tensor-core result's trace error."""
     import bml_b200 as B
     H, n = ellblock_case(16)
@@ -604,7 +604,7 @@ def ellblock_leg(reps=3):
     res = {"workload": "X^2 of H, 16^3 block lattice, 4096 block rows of 32x32 (N=131072), radius 2, thr 1e-6",
            "tc_s": tt, "fp64_s": te, "speedup": te / tt, "trace_rel_err": abs(trt - tre) / abs(tre),
            "nnz_h": int(nnz_h), "nnz_x2": int(B.lib.bml_b200_nnz(Xt)),
-           "method": "tcgen05 kind::f16 BF16 hi*hi + hi*lo + lo*hi, FP32 accumulation in TMEM"}
+           "method": "tcgen05 kind::f16, FP16 hi*hi + hi*lo + lo*hi of X scaled by 2^s, FP32 accumulation in TMEM"}
     for h in (H, Xe, Xt):
         hh = C.c_void_p(h)
         B.lib.bml_deallocate(C.byref(hh))

@@ -1,13 +1,16 @@
-// ELLBLOCK X^2 on the tcgen05 tensor cores, BF16 with a hi/lo split (mixed
+// ELLBLOCK X^2 on the tcgen05 tensor cores, FP16 with a hi/lo split (mixed
 // precision; no reference counterpart: the reference multiplies blocks in the
 // matrix precision, ellblock/bml_multiply_ellblock_typed.c:246-442).
 //
-// Every 32x32 block x is split as hi = bf16(x), lo = bf16(x - hi), and
-// X^2 = sum_jb X[ib,jb] X[jb,kb] is formed as hi*hi + hi*lo + lo*hi with FP32
-// accumulation in tensor memory (lo*lo, about 2^-16 of the product, is
-// dropped).  The result is written back in the matrix precision; blocks are
-// kept as in the reference (kb == ib, or max |x| > threshold), the traces are
-// FP64 sums.
+// X is scaled by a power of two 2^s (its largest entry near 2^14) and every
+// 32x32 block x is split as hi = fp16(2^s x), lo = fp16(2^s x - hi); X^2 =
+// sum_jb X[ib,jb] X[jb,kb] is formed as hi*hi + hi*lo + lo*hi with FP32
+// accumulation in tensor memory and scaled back by 2^-2s (lo*lo, about 2^-22
+// of the product, is dropped).  The accuracy is then set by the tensor
+// cores' FP32 accumulation: one X^2 of the 16^3 block lattice has its trace
+// within 7e-6, with BF16 operands (8-bit significands) and FP16 alike.  The
+// result is written back in the matrix precision; blocks are kept as in the
+// reference (kb == ib, or max |x| > threshold), the traces are FP64 sums.
 //
 // Work: one CTA per SM, persistent over groups of four consecutive block rows
 // ib0..ib0+3, which share most of their block columns jb on a lattice.  For
@@ -32,6 +35,7 @@
 #include "ellblock.h"
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <chrono>
 #include <cmath>
@@ -48,7 +52,7 @@ constexpr int TC_TILES = 16;      // live output tiles (16 x 32 = 512 TMEM colum
 constexpr int TC_GROUP = 4;       // block rows per group (M = 128)
 constexpr int TC_KCAP = 4096;     // output block columns per group
 constexpr int TC_JCAP = 1024;     // union of block columns per group
-constexpr int IMG = TB * TB;      // bf16 elements per block image (2 KB)
+constexpr int IMG = TB * TB;      // 16-bit elements per block image (2 KB)
 constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
 constexpr int TC_LCAP = 2048;     // product pairs per wave
 constexpr int TC_PCAP = 8192;     // product pairs per group
@@ -59,9 +63,37 @@ constexpr int TC_PCAP = 8192;     // product pairs per group
 #define B200_TC_BBUF 12
 #endif
 constexpr int TC_ABUF = B200_TC_ABUF; // left-operand buffers
+// Operand type of the split: FP16 (11-bit significands: hi and lo carry
+// about 22 bits, the dropped lo*lo about 2^-22 of a product) with the whole
+// matrix scaled by 2^s so that its largest entry is near 2^14 (entries down
+// to about 2^-24 of it keep a normal lo); or BF16 (8-bit significands, no
+// scaling needed, about 2^-16 per product).
+#ifndef B200_TC_F16
+#define B200_TC_F16 1
+#endif
+#if B200_TC_F16
+typedef __half tc_t;
+__device__ __forceinline__ tc_t tc_from_double(double x) { return __double2half(x); }
+__device__ __forceinline__ double tc_to_double(tc_t h) { return (double) __half2float(h); }
+#else
+typedef __nv_bfloat16 tc_t;
+__device__ __forceinline__ tc_t tc_from_double(double x) { return __float2bfloat16_rn((float) x); }
+__device__ __forceinline__ double tc_to_double(tc_t h) { return (double) __bfloat162float(h); }
+#endif
+
+// Exponent s of the split's scale 2^s, from the bits of max |x| (as float):
+// the largest entry lands near 2^14; 0 for an all-zero matrix (BF16: 0).
+__device__ __forceinline__ int tc_scale_exp(unsigned maxbits)
+{
+    if (!B200_TC_F16 || maxbits == 0u)
+        return 0;
+    int e = 0;
+    frexpf(__uint_as_float(maxbits), &e); // max |x| in [2^(e-1), 2^e)
+    return min(max(14 - e, -100), 100);
+}
 constexpr int TC_BBUF = B200_TC_BBUF; // right-operand buffers (pipeline depth)
 
-// bf16 image of a block in the K-major no-swizzle layout, as a left operand
+// 16-bit image of a block in the K-major no-swizzle layout, as a left operand
 // (element (r, k) of the block) or a right operand (element (n, k) = block
 // (k, n)): 16-byte rows of 8 k, 8-row core matrices of 128 bytes; the four
 // k-chunks of an 8-row group sit next to each other (LBO = 128 B) and the
@@ -74,25 +106,48 @@ __device__ __forceinline__ int img_off(int row, int k)
     return (row >> 3) * 256 + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
 }
 
-// Split every stored block of X into four images: left hi, left lo, right
-// hi, right lo, at img + slot*4*IMG.
+// max |x| over the stored blocks of X, as float bits (non-negative floats
+// order like their bits), into *maxbits.
 template <typename T>
-__global__ void tc_split_kernel(const T *pool, const int *nnzb, int NB, int MB, long long slot_elems,
-                                __nv_bfloat16 *img)
+__global__ void tc_maxabs_kernel(const T *pool, const int *nnzb, int NB, int MB, long long slot_elems,
+                                 unsigned *maxbits)
 {
+    float m = 0.f;
     for (long long s = blockIdx.x; s < (long long) NB * MB; s += gridDim.x)
     {
         const int ib = (int) (s / MB), jp = (int) (s % MB);
         if (jp >= nnzb[ib])
             continue;
         const T *x = pool + s * slot_elems;
-        __nv_bfloat16 *o = img + s * 4 * IMG;
+        for (int e = threadIdx.x; e < IMG; e += blockDim.x)
+            m = fmaxf(m, fabsf((float) x[e]));
+    }
+    for (int o = 16; o; o >>= 1)
+        m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(maxbits, __float_as_uint(m));
+}
+
+// Split every stored block of X, scaled by 2^s, into four images: left hi,
+// left lo, right hi, right lo, at img + slot*4*IMG.
+template <typename T>
+__global__ void tc_split_kernel(const T *pool, const int *nnzb, int NB, int MB, long long slot_elems,
+                                const unsigned *maxbits, tc_t *img)
+{
+    const double scale = ldexp(1.0, tc_scale_exp(*maxbits));
+    for (long long s = blockIdx.x; s < (long long) NB * MB; s += gridDim.x)
+    {
+        const int ib = (int) (s / MB), jp = (int) (s % MB);
+        if (jp >= nnzb[ib])
+            continue;
+        const T *x = pool + s * slot_elems;
+        tc_t *o = img + s * 4 * IMG;
         for (int e = threadIdx.x; e < IMG; e += blockDim.x)
         {
             const int r = e >> 5, c = e & 31;
-            const float v = (float) x[e];
-            const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-            const __nv_bfloat16 lo = __float2bfloat16_rn((float) ((double) x[e] - (double) __bfloat162float(hi)));
+            const double v = (double) x[e] * scale; // a power of two: exact
+            const tc_t hi = tc_from_double(v);
+            const tc_t lo = tc_from_double(v - tc_to_double(hi));
             o[img_off(r, c)] = hi;           // left: row r, k = c
             o[IMG + img_off(r, c)] = lo;
             o[2 * IMG + img_off(c, r)] = hi; // right: n = c, k = r
@@ -112,11 +167,13 @@ __device__ __forceinline__ uint64_t smem_desc(unsigned addr, unsigned lbo, unsig
            ((uint64_t) ((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// kind::f16 instruction descriptor: D F32, A and B BF16, both K-major,
-// N = 32, M = 128.
-constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// kind::f16 instruction descriptor: D F32, A and B both FP16 (type 0) or
+// both BF16 (type 1), both K-major, N = 32, M = 128.
+constexpr uint32_t TC_AB_TYPE = B200_TC_F16 ? 0u : 1u;
+constexpr uint32_t TC_IDESC =
+    (1u << 4) | (TC_AB_TYPE << 7) | (TC_AB_TYPE << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ void umma_bf16(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, unsigned accumulate)
+__device__ __forceinline__ void umma_f16(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, unsigned accumulate)
 {
     asm volatile("{\n\t.reg .pred p;\n\t"
                  "setp.ne.b32 p, %4, 0;\n\t"
@@ -212,7 +269,7 @@ struct TcSmem
 {
     union
     {
-        __nv_bfloat16 a[TC_ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
+        tc_t a[TC_ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
         struct
         {
             unsigned jbits[TC_NWCAP]; // the group's block columns jb (bitmap over NB)
@@ -223,7 +280,7 @@ struct TcSmem
     };
     union
     {
-        __nv_bfloat16 b[TC_BBUF][2][IMG]; // right operands, hi and lo: 32 x 32 (2 KB each)
+        tc_t b[TC_BBUF][2][IMG]; // right operands, hi and lo: 32 x 32 (2 KB each)
         float stage[TC_GROUP][TB][TB + 1]; // epilogue transpose (the ring is idle then)
     };
     uint64_t full_a[TC_ABUF], full_b[TC_BBUF]; // bulk copies landed
@@ -326,7 +383,7 @@ __device__ void rank_bits(const unsigned *bits, int *pre, int *list, int cap, in
 // [3] a tensor-core wait timed out
 template <typename T>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    tc_x2_kernel(TcView<T> X, TcOut<T> C, const __nv_bfloat16 *img, const __nv_bfloat16 *zimg, double thr,
+    tc_x2_kernel(TcView<T> X, TcOut<T> C, const tc_t *img, const tc_t *zimg, double thr,
                  double *dA, double *dC, int *flags)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -359,6 +416,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     const unsigned tbase = S.tmem;
+    const float unscale = ldexpf(1.0f, -2 * tc_scale_exp((unsigned) flags[8]));
     bool dead = false; // a wait timed out: stop issuing work
     // pipeline counters, kept alike by the producer (thread 0) and the MMA
     // issuer (thread 32): pairs and left operands issued so far
@@ -627,7 +685,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
                             for (int part = 0; part < 2; ++part)
                             {
-                                const __nv_bfloat16 *src =
+                                const tc_t *src =
                                     jp >= 0 ? img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG : zimg;
                                 bulk_copy(reinterpret_cast<unsigned char *>(S.a[a][part]) + q * 2048, src, IMG * 2,
                                           &S.full_a[a]);
@@ -644,7 +702,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     mbar_expect(&S.full_b[b], 2 * IMG * 2);
                     // the right hi and lo images are adjacent in both places:
                     // one 4 KB copy
-                    const __nv_bfloat16 *bsrc = img + ((size_t) S.jb[j] * X.MB + kp) * 4 * IMG;
+                    const tc_t *bsrc = img + ((size_t) S.jb[j] * X.MB + kp) * 4 * IMG;
                     bulk_copy(S.b[b][0], bsrc + 2 * IMG, 2 * IMG * 2, &S.full_b[b]);
                     ++gp;
                 }
@@ -690,9 +748,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         const uint64_t al = smem_desc(a1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
                         const uint64_t bh = smem_desc(b0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
                         const uint64_t bl = smem_desc(b1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
-                        umma_bf16(d, ah, bh, acc);
-                        umma_bf16(d, ah, bl, 1u);
-                        umma_bf16(d, al, bh, 1u);
+                        umma_f16(d, ah, bh, acc);
+                        umma_f16(d, ah, bl, 1u);
+                        umma_f16(d, al, bh, 1u);
                         acc = 1u;
                     }
                     umma_commit(&S.empty_b[b]);
@@ -724,6 +782,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             {
                 float v[32];
                 tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32), v);
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                    v[c] *= unscale; // undo the split's 2^s on both factors
                 const int kb = S.klist[t0 + t];
                 if (myrow >= X.NB || !((S.touched[t] >> warp) & 1))
                     continue;
@@ -810,7 +871,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 } // namespace
 
-// X2 = X*X on the tensor cores (BF16 hi/lo split, FP32 accumulation); X and
+// X2 = X*X on the tensor cores (FP16 hi/lo split, FP32 accumulation); X and
 // X2 must have blocks of 32 throughout.  Returns false with a status set
 // (UNSUPPORTED when the partition or a group's size is outside this path).
 bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, double threshold, double *trace)
@@ -844,27 +905,32 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     const int grid = c->sm_count;
     const size_t n_img = (size_t) NB * MB * 4 * IMG;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    const size_t off_tr = al(n_img * sizeof(__nv_bfloat16));
+    const size_t off_tr = al(n_img * sizeof(tc_t));
     const size_t off_flags = al(off_tr + (size_t) 2 * NB * sizeof(double));
     const size_t off_zero = al(off_flags + 64);
-    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_zero + IMG * sizeof(__nv_bfloat16)));
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_zero + IMG * sizeof(tc_t)));
     if (!scr)
         return false;
-    __nv_bfloat16 *img = reinterpret_cast<__nv_bfloat16 *>(scr);
+    tc_t *img = reinterpret_cast<tc_t *>(scr);
     double *dA = reinterpret_cast<double *>(scr + off_tr);
     double *dC = dA + NB;
     int *flags = reinterpret_cast<int *>(scr + off_flags);
-    __nv_bfloat16 *zimg = reinterpret_cast<__nv_bfloat16 *>(scr + off_zero);
+    unsigned *maxbits = reinterpret_cast<unsigned *>(flags + 8); // max |x| of X, for the split's scale
+    tc_t *zimg = reinterpret_cast<tc_t *>(scr + off_zero);
     if (!CUDA_OK(cudaMemsetAsync(flags, 0, 64, c->stream)) ||
-        !CUDA_OK(cudaMemsetAsync(zimg, 0, IMG * sizeof(__nv_bfloat16), c->stream)) ||
+        !CUDA_OK(cudaMemsetAsync(zimg, 0, IMG * sizeof(tc_t), c->stream)) ||
         !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)))
         return false;
     const size_t smem = sizeof(TcSmem) + 1024;
     const int sgrid = (int) min((long long) NB * MB, (long long) c->sm_count * 32);
     if (X->matrix_precision == double_real)
     {
+        tc_maxabs_kernel<double><<<sgrid, 256, 0, c->stream>>>(static_cast<const double *>(X->d_pool),
+                                                               X->d_nnzb, NB, MB, X->slot_elems, maxbits);
+        if (!LAUNCH_OK("tc_maxabs_kernel"))
+            return false;
         tc_split_kernel<double><<<sgrid, 256, 0, c->stream>>>(static_cast<const double *>(X->d_pool), X->d_nnzb,
-                                                              NB, MB, X->slot_elems, img);
+                                                              NB, MB, X->slot_elems, maxbits, img);
         if (!LAUNCH_OK("tc_split_kernel"))
             return false;
         auto k = tc_x2_kernel<double>;
@@ -877,8 +943,12 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     }
     else
     {
+        tc_maxabs_kernel<float><<<sgrid, 256, 0, c->stream>>>(static_cast<const float *>(X->d_pool), X->d_nnzb,
+                                                              NB, MB, X->slot_elems, maxbits);
+        if (!LAUNCH_OK("tc_maxabs_kernel"))
+            return false;
         tc_split_kernel<float><<<sgrid, 256, 0, c->stream>>>(static_cast<const float *>(X->d_pool), X->d_nnzb, NB,
-                                                             MB, X->slot_elems, img);
+                                                             MB, X->slot_elems, maxbits, img);
         if (!LAUNCH_OK("tc_split_kernel"))
             return false;
         auto k = tc_x2_kernel<float>;

@@ -379,10 +379,11 @@ BML_B200_API int bml_b200_sp2(bml_matrix_t *H, bml_matrix_t *D, double threshold
 BML_B200_API int bml_b200_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold,
     double occupation, int maxiter, double tol, int stall, int nclose, double *info);
 
-/* ELLBLOCK X^2 on the tensor cores (no reference counterpart): each 32x32
- * block x is split as hi = bf16(x), lo = bf16(x - hi) and the block products
- * are formed as hi*hi + hi*lo + lo*hi on tcgen05 with FP32 accumulation, then
- * written in X2's precision; blocks are kept as by bml_multiply_x2 (kb == ib
+/* ELLBLOCK X^2 on the tensor cores (no reference counterpart): X is scaled
+ * by a power of two, each 32x32 block x is split as hi = fp16(x), lo =
+ * fp16(x - hi), and the block products are formed as hi*hi + hi*lo + lo*hi
+ * on tcgen05 with FP32 accumulation, scaled back and written in X2's
+ * precision; blocks are kept as by bml_multiply_x2 (kb == ib
  * or max |x| > threshold).  trace (may be NULL) receives {tr X, tr X2}.  Every
  * block of X and X2 must be 32 x 32 (bml_set_block_sizes); otherwise
  * UNSUPPORTED.  Blocks of a row come out in first-touch order over the four

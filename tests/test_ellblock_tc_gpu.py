@@ -1,4 +1,4 @@
-"""ELLBLOCK X^2 on the tensor cores (BF16 hi/lo split, FP32 accumulation)
+"""ELLBLOCK X^2 on the tensor cores (scaled FP16 hi/lo split, FP32 accumulation)
 against the matrix-precision block product of bml_multiply_x2.
 
 Bounds: the split represents each entry to about 2^-17 of its size, and the
@@ -108,5 +108,43 @@ def test_tc_rejects_other_block_sizes():
         B.clear_error()
         free(X)
         free(X2)
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
+
+
+def test_ellblock_sp2_mixed_against_fp64():
+    """bml_b200_ellblock_sp2_mixed: bulk SP2 iterations on the tensor-core X^2,
+    the last two on the matrix-precision block product, against the same
+    solve with every iteration exact (nclose = maxiter).  On the 4^3 block
+    lattice (N = 2048, radius 2) the iterates stay within the group limits
+    of the tensor-core path for all ten iterations.  Tolerances: trace,
+    band energy tr(DH) and ||D - D_exact||_F / ||D_exact||_F within 1e-4
+    (the split carries about 1e-5 relative per X^2)."""
+    L, radius, iters, nclose, thr = 4, 2.0, 10, 2, 1e-6
+    Hd = block_lattice(L, radius, seed=3)
+    nb, N = L ** 3, Hd.shape[0]
+    set_partition(nb, nb)
+    try:
+        H = from_dense(Hd)
+        out = {}
+        for name, nc in (("exact", iters), ("mixed", nclose)):
+            D = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+            info = (C.c_double * 8)()
+            st = B.lib.bml_b200_ellblock_sp2_mixed(H, D, thr, N / 2.0, iters, -1.0, 0, nc, info)
+            assert st == B.OK, B.lib.bml_b200_error_string(st)
+            out[name] = (to_dense(D, N), list(info))
+            free(D)
+        (De, ie), (Dm, im) = out["exact"], out["mixed"]
+        assert ie[0] == im[0] == iters
+        assert ie[6] == 0 and im[6] == iters - nclose  # iterations on the tensor cores
+        tr_e, tr_m = np.trace(De), np.trace(Dm)
+        en_e, en_m = np.sum(De * Hd.T), np.sum(Dm * Hd.T)
+        fro = np.linalg.norm(Dm - De) / np.linalg.norm(De)
+        print("ellblock mixed SP2: trace err %.2e, energy err %.2e, ||dD||/||D|| %.2e"
+              % (abs(tr_m - tr_e) / abs(tr_e), abs(en_m - en_e) / abs(en_e), fro))
+        assert abs(tr_m - tr_e) <= 1e-4 * abs(tr_e)
+        assert abs(en_m - en_e) <= 1e-4 * abs(en_e)
+        assert fro <= 1e-4
+        free(H)
     finally:
         B.lib.bml_b200_reset_block_sizes()
