@@ -147,7 +147,7 @@ def run_b200(args, rank, world, local):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
         pg = dist
     v, ix, nz = inputs()
     H = B.Ellpack.from_arrays(v, ix, nz, N, M_H)
