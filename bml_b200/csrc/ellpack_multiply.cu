@@ -2193,7 +2193,11 @@ __global__ void __launch_bounds__(W * 32, MINB) dense_staged_kernel(MulArgs g, i
     }
 }
 
-// Staged dense tier: warps per row, ring stages, entries per unit, min blocks/SM
+// Staged dense tier: warps per row, ring stages, entries per unit, min
+// blocks/SM.  Measured on B200 over 4 FP64 SP2 iterations on the 40^3
+// lattice (A + dense tier): 4 warps x 2 stages x 1024 entries 360 ms;
+// 3 stages 368 ms; 512 entries 369 ms; 8 warps 382 ms; 2 warps x 512 entries
+// 355 ms, x 256 entries 386 ms (the unstaged reduction form: 377 ms).
 #ifndef B200_C_STAGED
 #define B200_C_STAGED 1
 #endif
