@@ -48,21 +48,26 @@ namespace {
 
 constexpr int TB = 32;            // block size this path handles
 constexpr int TC_THREADS = 128;   // 4 warps; warp q owns TMEM lanes 32q..32q+31
-constexpr int TC_TILES = 16;      // live output tiles (16 x 32 = 512 TMEM columns)
 constexpr int TC_GROUP = 4;       // block rows per group (M = 128)
-constexpr int TC_KCAP = 4096;     // output block columns per group
-constexpr int TC_JCAP = 1024;     // union of block columns per group
 constexpr int IMG = TB * TB;      // 16-bit elements per block image (2 KB)
 constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
-constexpr int TC_LCAP = 2048;     // product pairs per wave
-constexpr int TC_PCAP = 8192;     // product pairs per group
-#ifndef B200_TC_ABUF
-#define B200_TC_ABUF 6
-#endif
-#ifndef B200_TC_BBUF
-#define B200_TC_BBUF 12
-#endif
-constexpr int TC_ABUF = B200_TC_ABUF; // left-operand buffers
+// Two shapes of the kernel: a small one with two CTAs per SM (8 live tiles,
+// 256 TMEM columns each, so one CTA's set-up and epilogue overlap the
+// other's MMAs) that takes groups up to its capacities, and a large one with
+// one CTA per SM that the host falls back to when a group exceeds them.
+// ABUF/BBUF: left/right operand buffers; JCAP: union of block columns per
+// group; KCAP: output block columns per group; LCAP: product pairs per wave;
+// PCAP: product pairs per group.
+template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int JCAP_, int KCAP_, int LCAP_, int PCAP_> struct TcCfg
+{
+    static constexpr int TILES = TILES_, CTAS = CTAS_, ABUF = ABUF_, BBUF = BBUF_;
+    static constexpr int JCAP = JCAP_, KCAP = KCAP_, LCAP = LCAP_, PCAP = PCAP_;
+    static_assert(CTAS * TILES * 32 <= 512, "tensor memory holds 512 columns per SM");
+    static_assert(TILES <= 16, "tile numbers take 4 bits of a pair");
+};
+using TcSmall = TcCfg<8, 2, 3, 8, 512, 1024, 1024, 4096>;
+using TcBig = TcCfg<16, 1, 6, 12, 1024, 4096, 2048, 8192>;
+
 // Operand type of the split: FP16 (11-bit significands: hi and lo carry
 // about 22 bits, the dropped lo*lo about 2^-22 of a product) with the whole
 // matrix scaled by 2^s so that its largest entry is near 2^14 (entries down
@@ -91,7 +96,6 @@ __device__ __forceinline__ int tc_scale_exp(unsigned maxbits)
     frexpf(__uint_as_float(maxbits), &e); // max |x| in [2^(e-1), 2^e)
     return min(max(14 - e, -100), 100);
 }
-constexpr int TC_BBUF = B200_TC_BBUF; // right-operand buffers (pipeline depth)
 
 // 16-bit image of a block in the K-major no-swizzle layout, as a left operand
 // (element (r, k) of the block) or a right operand (element (n, k) = block
@@ -265,11 +269,11 @@ __device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32])
 }
 
 // Shared memory of the X^2 kernel.
-struct TcSmem
+template <class Cfg> struct TcSmem
 {
     union
     {
-        tc_t a[TC_ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
+        tc_t a[Cfg::ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
         struct
         {
             unsigned jbits[TC_NWCAP]; // the group's block columns jb (bitmap over NB)
@@ -280,24 +284,24 @@ struct TcSmem
     };
     union
     {
-        tc_t b[TC_BBUF][2][IMG]; // right operands, hi and lo: 32 x 32 (2 KB each)
+        tc_t b[Cfg::BBUF][2][IMG]; // right operands, hi and lo: 32 x 32 (2 KB each)
         float stage[TC_GROUP][TB][TB + 1]; // epilogue transpose (the ring is idle then)
     };
-    uint64_t full_a[TC_ABUF], full_b[TC_BBUF]; // bulk copies landed
-    uint64_t empty_b[TC_BBUF];            // MMAs reading a B buffer (and all before) done
-    uint64_t empty_a[TC_ABUF];            // MMAs reading an A buffer's fill (and all before) done
+    uint64_t full_a[Cfg::ABUF], full_b[Cfg::BBUF]; // bulk copies landed
+    uint64_t empty_b[Cfg::BBUF];            // MMAs reading a B buffer (and all before) done
+    uint64_t empty_a[Cfg::ABUF];            // MMAs reading an A buffer's fill (and all before) done
     uint64_t done;                        // all MMAs of a wave done
     unsigned tmem;
     int nJ, nK, npairs, ok, dead;
-    int jb[TC_JCAP];             // union of the group's block columns
-    short jslot[TC_JCAP][TC_GROUP]; // position of X[ib0+q, jb] in row ib0+q, or -1
-    int klist[TC_KCAP];          // kb of each output tile
-    int jcnt[TC_JCAP];           // pairs of the current wave per J entry, then their start
-    int list[TC_LCAP];           // pairs of the current wave: j << 20 | tile << 16 | kp
-    int jstart[TC_JCAP + 1];     // first pair of each J entry in ptile
-    unsigned short ptile[TC_PCAP]; // output tile of every pair (j, kp) of the group
-    unsigned char jmask[TC_JCAP];  // rows q of the group holding X[ib0+q, jb]
-    int touched[TC_TILES];         // rows q of the group with a product in the tile
+    int jb[Cfg::JCAP];             // union of the group's block columns
+    short jslot[Cfg::JCAP][TC_GROUP]; // position of X[ib0+q, jb] in row ib0+q, or -1
+    int klist[Cfg::KCAP];          // kb of each output tile
+    int jcnt[Cfg::JCAP];           // pairs of the current wave per J entry, then their start
+    int list[Cfg::LCAP];           // pairs of the current wave: j << 20 | tile << 16 | kp
+    int jstart[Cfg::JCAP + 1];     // first pair of each J entry in ptile
+    unsigned short ptile[Cfg::PCAP]; // output tile of every pair (j, kp) of the group
+    unsigned char jmask[Cfg::JCAP];  // rows q of the group holding X[ib0+q, jb]
+    int touched[Cfg::TILES];         // rows q of the group with a product in the tile
 };
 
 template <typename T> struct TcView
@@ -381,19 +385,22 @@ __device__ void rank_bits(const unsigned *bits, int *pre, int *list, int cap, in
 
 // flags: [0] row overflow, [1] widest kept row, [2] group over capacity,
 // [3] a tensor-core wait timed out
-template <typename T>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+template <typename T, class Cfg>
+__global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     tc_x2_kernel(TcView<T> X, TcOut<T> C, const tc_t *img, const tc_t *zimg, double thr,
                  double *dA, double *dC, int *flags)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
+    constexpr int TC_TILES = Cfg::TILES, TC_ABUF = Cfg::ABUF, TC_BBUF = Cfg::BBUF, TC_JCAP = Cfg::JCAP;
+    constexpr int TC_KCAP = Cfg::KCAP, TC_LCAP = Cfg::LCAP, TC_PCAP = Cfg::PCAP;
+    TcSmem<Cfg> &S = *reinterpret_cast<TcSmem<Cfg> *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ngroups = (X.NB + TC_GROUP - 1) / TC_GROUP;
 
     if (warp == 0)
     {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(su32(&S.tmem))
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&S.tmem)),
+                     "r"(TC_TILES * 32)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -866,10 +873,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TILES * 32)
+                     : "memory");
 }
 
 } // namespace
+
+template <typename T>
+bool tc_split(B200Context *c, const bml_matrix_ellblock_t *X, int sgrid, unsigned *maxbits, tc_t *img)
+{
+    const T *pool = static_cast<const T *>(X->d_pool);
+    tc_maxabs_kernel<T><<<sgrid, 256, 0, c->stream>>>(pool, X->d_nnzb, X->NB, X->MB, X->slot_elems, maxbits);
+    if (!LAUNCH_OK("tc_maxabs_kernel"))
+        return false;
+    tc_split_kernel<T><<<sgrid, 256, 0, c->stream>>>(pool, X->d_nnzb, X->NB, X->MB, X->slot_elems, maxbits, img);
+    return LAUNCH_OK("tc_split_kernel");
+}
+
+template <typename T, class Cfg>
+bool tc_launch(B200Context *c, const bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, const tc_t *img,
+               const tc_t *zimg, double threshold, double *dA, double *dC, int *flags)
+{
+    const size_t smem = sizeof(TcSmem<Cfg>) + 1024;
+    auto k = tc_x2_kernel<T, Cfg>;
+    if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+        return false;
+    k<<<c->sm_count * Cfg::CTAS, TC_THREADS, smem, c->stream>>>(
+        TcView<T>{static_cast<const T *>(X->d_pool), X->d_indexb, X->d_nnzb, X->NB, X->MB, X->slot_elems},
+        TcOut<T>{static_cast<T *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems}, img, zimg,
+        threshold, dA, dC, flags);
+    return LAUNCH_OK("tc_x2_kernel");
+}
 
 // X2 = X*X on the tensor cores (FP16 hi/lo split, FP32 accumulation); X and
 // X2 must have blocks of 32 throughout.  Returns false with a status set
@@ -902,7 +936,6 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     if (!c || !eb_to_device(X) || !eb_to_device(X2))
         return false;
     const int NB = X->NB, MB = X->MB;
-    const int grid = c->sm_count;
     const size_t n_img = (size_t) NB * MB * 4 * IMG;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t off_tr = al(n_img * sizeof(tc_t));
@@ -921,56 +954,39 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
         !CUDA_OK(cudaMemsetAsync(zimg, 0, IMG * sizeof(tc_t), c->stream)) ||
         !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)))
         return false;
-    const size_t smem = sizeof(TcSmem) + 1024;
     const int sgrid = (int) min((long long) NB * MB, (long long) c->sm_count * 32);
-    if (X->matrix_precision == double_real)
-    {
-        tc_maxabs_kernel<double><<<sgrid, 256, 0, c->stream>>>(static_cast<const double *>(X->d_pool),
-                                                               X->d_nnzb, NB, MB, X->slot_elems, maxbits);
-        if (!LAUNCH_OK("tc_maxabs_kernel"))
-            return false;
-        tc_split_kernel<double><<<sgrid, 256, 0, c->stream>>>(static_cast<const double *>(X->d_pool), X->d_nnzb,
-                                                              NB, MB, X->slot_elems, maxbits, img);
-        if (!LAUNCH_OK("tc_split_kernel"))
-            return false;
-        auto k = tc_x2_kernel<double>;
-        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
-            return false;
-        k<<<grid, TC_THREADS, smem, c->stream>>>(
-            TcView<double>{static_cast<const double *>(X->d_pool), X->d_indexb, X->d_nnzb, NB, MB, X->slot_elems},
-            TcOut<double>{static_cast<double *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems},
-            img, zimg, threshold, dA, dC, flags);
-    }
-    else
-    {
-        tc_maxabs_kernel<float><<<sgrid, 256, 0, c->stream>>>(static_cast<const float *>(X->d_pool), X->d_nnzb,
-                                                              NB, MB, X->slot_elems, maxbits);
-        if (!LAUNCH_OK("tc_maxabs_kernel"))
-            return false;
-        tc_split_kernel<float><<<sgrid, 256, 0, c->stream>>>(static_cast<const float *>(X->d_pool), X->d_nnzb, NB,
-                                                             MB, X->slot_elems, maxbits, img);
-        if (!LAUNCH_OK("tc_split_kernel"))
-            return false;
-        auto k = tc_x2_kernel<float>;
-        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
-            return false;
-        k<<<grid, TC_THREADS, smem, c->stream>>>(
-            TcView<float>{static_cast<const float *>(X->d_pool), X->d_indexb, X->d_nnzb, NB, MB, X->slot_elems},
-            TcOut<float>{static_cast<float *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems},
-            img, zimg, threshold, dA, dC, flags);
-    }
-    if (!LAUNCH_OK("tc_x2_kernel"))
+    bool ok = X->matrix_precision == double_real
+                  ? tc_split<double>(c, X, sgrid, maxbits, img)
+                  : tc_split<float>(c, X, sgrid, maxbits, img);
+    if (!ok)
         return false;
+    // the two-CTA shape first; the one-CTA shape if a group exceeded it
+    unsigned char *pin = static_cast<unsigned char *>(c->pinned) + 8192;
+    int hf[4];
+    for (int shape = 0; shape < 2; ++shape)
+    {
+        if (shape == 1 && !CUDA_OK(cudaMemsetAsync(flags, 0, 16, c->stream)))
+            return false;
+        if (X->matrix_precision == double_real)
+            ok = shape == 0 ? tc_launch<double, TcSmall>(c, X, X2, img, zimg, threshold, dA, dC, flags)
+                            : tc_launch<double, TcBig>(c, X, X2, img, zimg, threshold, dA, dC, flags);
+        else
+            ok = shape == 0 ? tc_launch<float, TcSmall>(c, X, X2, img, zimg, threshold, dA, dC, flags)
+                            : tc_launch<float, TcBig>(c, X, X2, img, zimg, threshold, dA, dC, flags);
+        if (!ok)
+            return false;
+        if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+            return false;
+        memcpy(hf, pin, sizeof(hf));
+        if (!hf[2] || hf[3])
+            break; // fitted (or timed out: reported below)
+    }
     double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 256);
     b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(dA, dC, NB, out);
     if (!LAUNCH_OK("b200_sum_rows_kernel"))
         return false;
-    unsigned char *pin = static_cast<unsigned char *>(c->pinned) + 8192;
-    if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 16, cudaMemcpyDeviceToHost, c->stream)) ||
-        !CUDA_OK(cudaMemcpyAsync(pin + 64, out, 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+    if (!CUDA_OK(cudaMemcpyAsync(pin + 64, out, 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
         return false;
-    int hf[4];
-    memcpy(hf, pin, sizeof(hf));
     X2->mirror = MIRROR_DEVICE_NEWER;
     if (trace)
         memcpy(trace, pin + 64, 2 * sizeof(double));

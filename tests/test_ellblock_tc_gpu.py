@@ -66,7 +66,9 @@ def free(h):
 
 
 @pytest.mark.parametrize("prec", [DOUBLE, SINGLE])
-@pytest.mark.parametrize("L,radius", [(3, 1.0), (4, 2.0)])
+# (6, 2.24): 57 block neighbours, about 7000 block products per group of four
+# block rows, more than the two-CTA shape takes: the one-CTA shape runs
+@pytest.mark.parametrize("L,radius", [(3, 1.0), (4, 2.0), (6, 2.24)])
 def test_tc_x2_matches_block_product(prec, L, radius):
     H = block_lattice(L, radius)
     nb, N = L ** 3, H.shape[0]
