@@ -65,7 +65,10 @@ template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int JCAP_, int KCAP_, int
     static_assert(CTAS * TILES * 32 <= 512, "tensor memory holds 512 columns per SM");
     static_assert(TILES <= 16, "tile numbers take 4 bits of a pair");
 };
-using TcSmall = TcCfg<8, 2, 3, 8, 512, 1024, 1024, 4096>;
+#ifndef B200_TCS_SHAPE
+#define B200_TCS_SHAPE 8, 2, 3, 8, 512, 1024, 1024, 4096
+#endif
+using TcSmall = TcCfg<B200_TCS_SHAPE>;
 using TcBig = TcCfg<16, 1, 6, 12, 1024, 4096, 2048, 8192>;
 
 // Operand type of the split: FP16 (11-bit significands: hi and lo carry
