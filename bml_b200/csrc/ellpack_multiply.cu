@@ -1944,13 +1944,14 @@ __global__ void __launch_bounds__(DenseCfg<RED>::warps * 32, DenseCfg<RED>::bloc
 }
 
 // -------------------------------------------------------------------------
-// Tier C, staged form (the reduction form with B's rows in shared memory):
+// Tier C, staged form (dense_tier_kernel with B's rows in shared memory):
 // B's rows stream through a ring of STAGES units of at most CHUNK entries,
 // copied by TMA bulk copies (cp.async.bulk) up to STAGES - 1 units ahead, as
 // in the team tiers; the accumulator is the per-block slab with the
-// shared-memory touched bitmap and L2 reductions.  The product loop then
-// reads B from shared memory, so no lane waits on a global load.  The
-// first-touch list is built per unit (units follow B's row order).
+// shared-memory touched bitmap, summed by L2 reductions (RED) or by load,
+// add and store.  The product loop then reads B from shared memory, so no
+// lane waits on a global load of B.  The first-touch list is built per unit
+// (units follow B's row order).
 // Shared memory: mbar[STAGES] | sv[STAGES][CHUNK] | sk[STAGES][CHUNK] |
 //                stg[W][SPW] (int) | cnt[2][W] | misc | bits[ncols/32]
 // -------------------------------------------------------------------------
@@ -1967,7 +1968,9 @@ template <typename T, int W, int STAGES, int CHUNK> struct StagedCfg
     static size_t bytes(int ncols) { return off_bits + (size_t) (ncols + 31) / 32 * sizeof(unsigned); }
 };
 
-template <typename T, int W, int STAGES, int CHUNK, int MINB>
+// RED: touched columns summed by L2 reductions; otherwise loaded, added and
+// stored (exact FP32, whose global add flushes subnormals).
+template <typename T, int W, int STAGES, int CHUNK, int MINB, bool RED>
 __global__ void __launch_bounds__(W * 32, MINB) dense_staged_kernel(MulArgs g, int ncols, const int *rows,
                                                                    TierLists *tl, unsigned char *slabs)
 {
@@ -2113,8 +2116,10 @@ __global__ void __launch_bounds__(W * 32, MINB) dense_staged_kernel(MulArgs g, i
                                 acc[k] = add_rn(T(0), p);
                                 ins = true;
                             }
-                            else
+                            else if (RED)
                                 atomicAdd(acc + k, p);
+                            else
+                                acc[k] = add_rn(acc[k], p);
                         }
                         const unsigned bal = __ballot_sync(FULL, ins);
                         if (ins)
@@ -2324,11 +2329,12 @@ bool multiply_typed(MulArgs g, int ncols, double *trace, int *required_M)
     }
     int gridC = c->sm_count * blocks_c;
     const size_t slab_bytes = (size_t) ncols * (sizeof(T) + 2 * sizeof(int));
-    // the staged form of the reduction kernel, while its shared memory fits
+    // the staged form of the dense tier, while its shared memory fits
     using SCfg = StagedCfg<T, CS_W, CS_STAGES, CS_CHUNK>;
-    auto staged_k = dense_staged_kernel<T, CS_W, CS_STAGES, CS_CHUNK, CS_MINB>;
+    auto staged_k = red ? dense_staged_kernel<T, CS_W, CS_STAGES, CS_CHUNK, CS_MINB, true>
+                        : dense_staged_kernel<T, CS_W, CS_STAGES, CS_CHUNK, CS_MINB, false>;
     const size_t smemS = SCfg::bytes(ncols);
-    bool staged = B200_C_STAGED && red && smemS <= c->smem_optin;
+    bool staged = B200_C_STAGED && smemS <= c->smem_optin;
     if (staged)
     {
         if (!CUDA_OK(cudaFuncSetAttribute(staged_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smemS)))
