@@ -47,6 +47,9 @@ SP2_ITERS = 4
 # the 30^3 lattice case (bench.py --profile): 122.82 GB read + 11.77 GB
 # written for 18,570,945,128 products.
 DRAM_BYTES_PER_PRODUCT = (122.821243e9 + 11.769428e9) / 18570945128
+# B200 FP64 (vector and tensor) nominal rate, HGX figure per GPU; no measured
+# FP64 peak is available, so fractions against it are "of nominal"
+FP64_NOMINAL_TFLOPS = 37.0
 METRIC = "s per SP2 solve & X² HBM GB/s, ELLPACK N=64K: FP64 vs mixed at ≤1e-6 err"
 WORKLOAD = ("SP2 on the 40^3 lattice Hamiltonian (N=64000, radius 3, M=%d, thr 1e-5, occ N/2, FP64), "
             "first %d iterations from X0 (the full solve fills in to dense)" % (M_X, SP2_ITERS))
@@ -379,6 +382,9 @@ def x2_roofline(B, H, info):
                       % (SP2_ITERS - 1),
             "x2_seconds": t, "nnz_x": int(nnz_x), "nnz_x2": int(nnz_x2), "products": P,
             "fp64_gflops": 2.0 * P / t / 1e9, "products_per_s": P / t,
+            "compute_frac": 2.0 * P / t / 1e12 / (FP64_NOMINAL_TFLOPS / 2),
+            "compute_frac_of": "nominal FP64 %.0f TFLOP/s halved (separately rounded multiply and add per "
+                               "product, as in the reference)" % FP64_NOMINAL_TFLOPS,
             "gathered_gbs": 12.0 * P / t / 1e9}
 
 
@@ -571,6 +577,26 @@ def run_profile_tc():
     print(json.dumps({"profile_case": "10^3 block lattice, tensor-core X^2", "trace": list(tr)}))
 
 
+def block_lattice_products(L, radius):
+    """Block products of X^2 on the L^3 block lattice: the (ib, jb, kb)
+    triples, sum over ib and its neighbours jb of jb's neighbour count."""
+    import itertools
+    import numpy as np
+    r = int(radius)
+    offs = [o for o in itertools.product(range(-r, r + 1), repeat=3) if sum(x * x for x in o) <= radius ** 2 + 1e-9]
+    pos = np.array([(x, y, z) for z in range(L) for y in range(L) for x in range(L)])
+    deg = np.zeros(L ** 3, np.int64)
+    for o in offs:
+        deg += np.all((pos + o >= 0) & (pos + o < L), axis=1)
+    total = 0
+    for o in offs:
+        q = pos + o
+        ok = np.all((q >= 0) & (q < L), axis=1)
+        q = q[ok]
+        total += int(deg[q[:, 0] + L * q[:, 1] + L * L * q[:, 2]].sum())
+    return total
+
+
 def ellblock_leg(reps=3):
     """The mixed ELLBLOCK configuration's product: X^2 of H on the 16^3 block
     lattice (4096 block rows of 32, N = 131072, threshold 1e-6), on the
@@ -601,9 +627,24 @@ def ellblock_leg(reps=3):
     tt = timed(lambda: B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, Xt, 1e-6, tr)))
     tre, trt = B.lib.bml_trace(Xe), B.lib.bml_trace(Xt)
     nnz_h = B.lib.bml_b200_nnz(H)
+    P = block_lattice_products(16, 2.0)
+    flops = 2.0 * 32 ** 3 * P
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    tc_peak = peaks.get("bf16_tflops") or 1590.0
     res = {"workload": "X^2 of H, 16^3 block lattice, 4096 block rows of 32x32 (N=131072), radius 2, thr 1e-6",
            "tc_s": tt, "fp64_s": te, "speedup": te / tt, "trace_rel_err": abs(trt - tre) / abs(tre),
-           "nnz_h": int(nnz_h), "nnz_x2": int(B.lib.bml_b200_nnz(Xt)),
+           "nnz_h": int(nnz_h), "nnz_x2": int(B.lib.bml_b200_nnz(Xt)), "block_products": P,
+           "fp64_tflops": flops / te / 1e12,
+           "fp64_ceiling_tflops": FP64_NOMINAL_TFLOPS / 2,
+           "fp64_ceiling": "nominal B200 FP64 %.0f TFLOP/s halved: every multiply and add is a separately "
+                           "rounded instruction (no FMA), as in the reference" % FP64_NOMINAL_TFLOPS,
+           "tc_tflops": 3 * flops / tt / 1e12, "tc_peak_tflops": tc_peak,
+           "tc_tflops_note": "three block products (hi*hi, hi*lo, lo*hi) per block pair over the measured "
+                             "dense bf16 peak (f16 runs at the same rate)",
            "method": "tcgen05 kind::f16, FP16 hi*hi + hi*lo + lo*hi of X scaled by 2^s, FP32 accumulation in TMEM"}
     for h in (H, Xe, Xt):
         hh = C.c_void_p(h)

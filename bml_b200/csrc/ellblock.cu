@@ -1018,7 +1018,7 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
         const int n = lb;
         int kept = 0;
         T trC = T(0);
-        for (int q = 0; q < n; ++q)
+        for (int q = 0; q < min(n, 1024); ++q)
         {
             const int kb = list[q];
             const int bk = B.bsize[kb];
@@ -1058,6 +1058,383 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
                 dC[ib] = (double) trC;
         }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same exact X^2 / A*B for a uniform partition of 32 x 32 blocks, with
+// the block products register-tiled.  Same arithmetic (every element
+// x = x + s, s = a0*b0 + a1*b1 + ... left to right, separately rounded), same
+// first-touch slot order, same keep rule, so the results are bit-identical to
+// eb_mul_kernel's.
+//
+// Four warps per CTA: warp w forms rows 8w..8w+7 of the 32 x 32 product and
+// lane c its column c, so for every 16 bytes of the left block a lane reads
+// (one broadcast shared-memory load) it does 16 / sizeof(T) multiply-adds
+// per row.  Thread 0 copies the blocks with cp.async.bulk ahead of use: the
+// left block X[ib,jb] into one of two buffers, the right blocks X[jb,kb]
+// through a ring of EB32_STAGES buffers, completing on mbarriers (bounded
+// waits; a wait that runs out raises flags[2]).  At the start of every left
+// block (in segments of EB32_SEG right blocks) all threads assign the slots
+// of its right blocks at once: a ballot prefix in kp order appends first
+// touches to the row's list.  Accumulators stay in the per-CTA slab, each
+// element owned by one thread.
+// Shared memory: EbS32<T> (48 KB for double, four CTAs per SM).
+// ---------------------------------------------------------------------------
+constexpr int EB32_STAGES = 3, EB32_THREADS = 128, EB32_SEG = 1024, EB32_LIST = 1024;
+
+template <typename T> struct EbS32
+{
+    uint64_t full_r[EB32_STAGES];
+    uint64_t full_l[2];
+    __align__(16) T L[2][1024];
+    __align__(16) T R[EB32_STAGES][1024];
+    int slotq[EB32_SEG]; // per kp of the segment: slot, or -(slot + 1) on first touch; then per slot:
+                         // output position, -1 when dropped
+    int list[EB32_LIST]; // kb per slot, first-touch order
+    int cnt[EB32_THREADS / 32];
+    int kept;
+};
+
+template <typename T> struct Vec16;
+template <> struct Vec16<double>
+{
+    using type = double2;
+    static constexpr int n = 2;
+    __device__ static double at(const double2 &v, int q) { return q ? v.y : v.x; }
+};
+template <> struct Vec16<float>
+{
+    using type = float4;
+    static constexpr int n = 4;
+    __device__ static float at(const float4 &v, int q) { return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w; }
+};
+
+__device__ __forceinline__ unsigned eb_su32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void eb_bulk(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(eb_su32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     eb_su32(dst)),
+                 "l"(src), "r"(bytes), "r"(eb_su32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool eb_test(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(eb_su32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of bar, at most about 2 s; false on timeout.
+__device__ bool eb_wait2s(uint64_t *bar, unsigned parity)
+{
+    unsigned long long t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;)
+    {
+        if (eb_test(bar, parity))
+            return true;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > 2000000000ull)
+            return false;
+    }
+}
+
+// The same, raising *flag on timeout.  Once the flag is up the kernel's
+// result is void, and later waits return at once.
+__device__ __forceinline__ void eb_wait(uint64_t *bar, unsigned parity, int *flag)
+{
+    if (eb_test(bar, parity) || *reinterpret_cast<volatile int *>(flag))
+        return;
+    if (!eb_wait2s(bar, parity))
+        atomicExch(flag, 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, EbView<T> B, EbView<T> C, double thr,
+                                                                  int use_norm_inf_fast, T *slab, int *marks,
+                                                                  double *dA, double *dC, int *flags)
+{
+    using V = Vec16<T>;
+    using VT = typename V::type;
+    constexpr int NV = V::n;
+    constexpr unsigned BLK = 1024 * sizeof(T);
+    extern __shared__ __align__(128) unsigned char smem[];
+    EbS32<T> &S = *reinterpret_cast<EbS32<T> *>(smem);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cap = min(C.MB + 1, EB32_LIST); // slab slots (one spare to detect overflow)
+    T *myslab = slab + (size_t) blockIdx.x * cap * 1024;
+    int *mark = marks + (size_t) blockIdx.x * B.NB;
+    int *tflag = &flags[2];
+
+    if (tid == 0)
+    {
+        for (int s = 0; s < EB32_STAGES; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(eb_su32(&S.full_r[s])) : "memory");
+        for (int s = 0; s < 2; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(eb_su32(&S.full_l[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // running counts over every row of this CTA (uniform): right blocks
+    // consumed, left blocks started
+    unsigned consumed = 0, lcur = 0;
+    // producer state (thread 0): copies issued, and the next pair (pj, pk)
+    unsigned issued = 0, lissued = 0;
+    int pj = 0, pk = 0, pnk = 0, pjb = 0;
+
+    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    {
+        const int na = A.nnzb[ib];
+        const int *arow = A.indexb + (size_t) ib * A.MB;
+        // left blocks whose block row of B is empty have no pairs
+        auto prod_skip = [&]() {
+            while (pj < na)
+            {
+                pjb = arow[pj];
+                pnk = B.nnzb[pjb];
+                if (pnk > 0)
+                    return;
+                ++pj;
+            }
+        };
+        auto produce = [&]() {
+            // generic-proxy reads of the buffers being refilled are ordered
+            // before the bulk copies by the barrier and this fence
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            while (pj < na && issued - consumed < (unsigned) EB32_STAGES && (pk > 0 || lissued <= lcur + 1))
+            {
+                if (pk == 0)
+                {
+                    eb_bulk(S.L[lissued & 1], A.blk(ib, pj), BLK, &S.full_l[lissued & 1]);
+                    ++lissued;
+                }
+                const unsigned s = issued % EB32_STAGES;
+                eb_bulk(S.R[s], B.blk(pjb, pk), BLK, &S.full_r[s]);
+                ++issued;
+                if (++pk == pnk)
+                {
+                    pk = 0;
+                    ++pj;
+                    prod_skip();
+                }
+            }
+        };
+        if (tid == 0)
+        {
+            pj = 0;
+            pk = 0;
+            prod_skip();
+            produce();
+        }
+
+        int lb = 0; // slots in use (uniform)
+        T trA = T(0);
+        for (int jp = 0; jp < na; ++jp)
+        {
+            const int jb = arow[jp];
+            const int nk = B.nnzb[jb];
+            if (jb == ib && tid == 0)
+            {
+                const T *L = A.blk(ib, jp);
+                for (int kk = 0; kk < 32; ++kk)
+                    trA = add_rn(trA, L[kk * 33]);
+            }
+            if (nk == 0)
+                continue;
+            const int *brow = B.indexb + (size_t) jb * B.MB;
+            eb_wait(&S.full_l[lcur & 1], (lcur >> 1) & 1, tflag);
+            const T *Ls = S.L[lcur & 1];
+            for (int seg0 = 0; seg0 < nk; seg0 += EB32_SEG)
+            {
+                const int ns = min(EB32_SEG, nk - seg0);
+                // slots of this segment's right blocks, first touches appended in kp order
+                for (int c0 = 0; c0 < ns; c0 += EB32_THREADS)
+                {
+                    const int q = c0 + tid;
+                    bool isnew = false;
+                    int sl = 0, kb = 0;
+                    if (q < ns)
+                    {
+                        kb = brow[seg0 + q];
+                        const int m = mark[kb];
+                        isnew = m == 0;
+                        sl = m - 1;
+                    }
+                    const unsigned bal = __ballot_sync(FULL, isnew);
+                    if (lane == 0)
+                        S.cnt[warp] = __popc(bal);
+                    __syncthreads();
+                    int pre = 0, tot = 0;
+#pragma unroll
+                    for (int w = 0; w < EB32_THREADS / 32; ++w)
+                    {
+                        const int cw = S.cnt[w];
+                        pre += w < warp ? cw : 0;
+                        tot += cw;
+                    }
+                    if (isnew)
+                    {
+                        sl = lb + pre + __popc(bal & lanemask_lt());
+                        mark[kb] = sl + 1;
+                        if (sl < EB32_LIST)
+                            S.list[sl] = kb;
+                    }
+                    if (q < ns)
+                        S.slotq[q] = isnew ? -(sl + 1) : sl;
+                    lb += tot;
+                    __syncthreads();
+                }
+                for (int q = 0; q < ns; ++q)
+                {
+                    const unsigned st = consumed % EB32_STAGES;
+                    eb_wait(&S.full_r[st], (consumed / EB32_STAGES) & 1, tflag);
+                    const int code = S.slotq[q];
+                    const bool first = code < 0;
+                    const int sl = first ? -code - 1 : code;
+                    if (sl < cap)
+                    {
+                        T *x = myslab + (size_t) sl * 1024 + warp * 8 * 32 + lane;
+                        T xo[8];
+#pragma unroll
+                        for (int r = 0; r < 8; ++r)
+                            xo[r] = first ? T(0) : x[r * 32];
+                        const T *Rs = S.R[st] + lane;
+                        const VT *La = reinterpret_cast<const VT *>(Ls + warp * 8 * 32);
+                        T s[8];
+#pragma unroll
+                        for (int l0 = 0; l0 < 32; l0 += NV)
+                        {
+                            VT a[8];
+#pragma unroll
+                            for (int r = 0; r < 8; ++r)
+                                a[r] = La[(r * 32 + l0) / NV];
+#pragma unroll
+                            for (int v = 0; v < NV; ++v)
+                            {
+                                const T b = Rs[(l0 + v) * 32];
+#pragma unroll
+                                for (int r = 0; r < 8; ++r)
+                                {
+                                    const T p = mul_rn(V::at(a[r], v), b);
+                                    s[r] = (l0 + v == 0) ? p : add_rn(s[r], p);
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < 8; ++r)
+                            x[r * 32] = add_rn(xo[r], s[r]);
+                    }
+                    __syncthreads();
+                    ++consumed;
+                    if (seg0 + q == nk - 1)
+                        ++lcur;
+                    if (tid == 0)
+                        produce();
+                }
+            }
+        }
+        __syncthreads();
+
+        // keep (kb == ib or max|x| > thr) and copy out in first-touch order
+        const int n = lb;
+        const int nl = min(n, cap);
+        for (int q = warp; q < nl; q += EB32_THREADS / 32)
+        {
+            const VT *x = reinterpret_cast<const VT *>(myslab + (size_t) q * 1024);
+            double m = 0.0;
+            for (int e = lane; e < 1024 / NV; e += 32)
+            {
+                const VT v = x[e];
+#pragma unroll
+                for (int u = 0; u < NV; ++u)
+                    m = fmax(m, (double) fabs(V::at(v, u)));
+            }
+            for (int o = 16; o; o >>= 1)
+                m = fmax(m, __shfl_xor_sync(FULL, m, o));
+            const int kb = S.list[q];
+            const bool keep = kb == ib || (use_norm_inf_fast ? m > thr : (T) m > (T) thr);
+            if (lane == 0)
+                S.slotq[q] = keep;
+        }
+        __syncthreads();
+        if (warp == 0)
+        {
+            int base = 0;
+            for (int c0 = 0; c0 < nl; c0 += 32)
+            {
+                const int q = c0 + lane;
+                const bool f = q < nl && S.slotq[q];
+                const unsigned bal = __ballot_sync(FULL, f);
+                if (q < nl)
+                    S.slotq[q] = f ? base + __popc(bal & lanemask_lt()) : -1;
+                base += __popc(bal);
+            }
+            if (lane == 0)
+                S.kept = base;
+        }
+        __syncthreads();
+        const int kept = S.kept;
+        for (int q = warp; q < nl; q += EB32_THREADS / 32)
+        {
+            const int d = S.slotq[q];
+            if (d < 0 || d >= C.MB)
+                continue;
+            const uint4 *src = reinterpret_cast<const uint4 *>(myslab + (size_t) q * 1024);
+            uint4 *dst = reinterpret_cast<uint4 *>(C.blk(ib, d));
+            for (int e = lane; e < (int) (BLK / 16); e += 32)
+                dst[e] = src[e];
+            if (lane == 0)
+                C.indexb[(size_t) ib * C.MB + d] = S.list[q];
+        }
+        if (tid == 0)
+        {
+            // the diagonal block is always kept; its trace in row order
+            T trC = T(0);
+            const int dq = mark[ib] - 1;
+            if (dq >= 0 && dq < nl)
+            {
+                const T *x = myslab + (size_t) dq * 1024;
+                for (int kk = 0; kk < 32; ++kk)
+                    trC = add_rn(trC, x[kk * 33]);
+            }
+            C.nnzb[ib] = kept < C.MB ? kept : C.MB;
+            atomicMax(&flags[1], kept);
+            if (kept > C.MB || n > cap)
+                atomicExch(&flags[0], 1);
+            if (dA)
+                dA[ib] = (double) trA;
+            if (dC)
+                dC[ib] = (double) trC;
+        }
+        __syncthreads();
+        for (int q = tid; q < min(n, EB32_LIST); q += EB32_THREADS)
+            mark[S.list[q]] = 0;
+        __syncthreads();
+    }
+    // after a timeout, copies still in flight land before the CTA leaves:
+    // the last fill of every buffer, each wait bounded
+    if (tid == 0 && *reinterpret_cast<volatile int *>(tflag))
+    {
+        for (unsigned b = 0; b < (unsigned) EB32_STAGES && b < issued; ++b)
+        {
+            const unsigned u = issued - 1 - b;
+            eb_wait2s(&S.full_r[u % EB32_STAGES], (u / EB32_STAGES) & 1);
+        }
+        for (unsigned b = 0; b < 2u && b < lissued; ++b)
+        {
+            const unsigned u = lissued - 1 - b;
+            eb_wait2s(&S.full_l[u & 1], (u >> 1) & 1);
+        }
     }
 }
 
@@ -1109,7 +1486,11 @@ bool eb_multiply_typed(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_m
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "ELLBLOCK multiply: blocks larger than 64");
         return false;
     }
-    const int grid = eb_grid<T>(c, A->NB, 2);
+    // uniform 32 x 32 blocks: the register-tiled kernel (same bits)
+    bool bs32 = A->maxbs == 32 && B->maxbs == 32 && C->maxbs == 32;
+    for (int ib = 0; bs32 && ib < A->NB; ib++)
+        bs32 = A->bsize[ib] == 32 && B->bsize[ib] == 32;
+    const int grid = bs32 ? eb_grid<T>(c, A->NB, 4) : eb_grid<T>(c, A->NB, 2);
     const int cap = C->MB + 1 < 1024 ? C->MB + 1 : 1024;
     const size_t slab = (size_t) grid * cap * A->slot_elems * sizeof(T);
     const size_t marks = (size_t) grid * B->NB * sizeof(int);
@@ -1124,14 +1505,28 @@ bool eb_multiply_typed(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_m
     int *flags = eb_flags(c);
     if (!flags || !CUDA_OK(cudaMemsetAsync(dmarks, 0, marks, c->stream)))
         return false;
-    const size_t smem = 2 * (size_t) A->slot_elems * sizeof(T) + 1024 * sizeof(int);
-    auto k = eb_mul_kernel<T>;
-    if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
-        return false;
-    k<<<grid, 256, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0, dslab,
-                                     dmarks, trace ? dA : nullptr, trace ? dC : nullptr, flags);
-    if (!LAUNCH_OK("eb_mul_kernel"))
-        return false;
+    if (bs32)
+    {
+        const size_t smem = sizeof(EbS32<T>);
+        auto k = eb_mul32_kernel<T>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, EB32_THREADS, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0,
+                                                   dslab, dmarks, trace ? dA : nullptr, trace ? dC : nullptr, flags);
+        if (!LAUNCH_OK("eb_mul32_kernel"))
+            return false;
+    }
+    else
+    {
+        const size_t smem = 2 * (size_t) A->slot_elems * sizeof(T) + 1024 * sizeof(int);
+        auto k = eb_mul_kernel<T>;
+        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return false;
+        k<<<grid, 256, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0, dslab,
+                                         dmarks, trace ? dA : nullptr, trace ? dC : nullptr, flags);
+        if (!LAUNCH_OK("eb_mul_kernel"))
+            return false;
+    }
     if (trace)
     {
         double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 64);
@@ -1143,13 +1538,18 @@ bool eb_multiply_typed(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_m
     int *pin = reinterpret_cast<int *>(static_cast<unsigned char *>(c->pinned) + 4096);
     if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 64 + 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
         return false;
-    memcpy(hf, pin, sizeof(int) * 2);
+    memcpy(hf, pin, sizeof(int) * 3);
     eb_mark_device(C);
     if (trace)
     {
         const double *t = reinterpret_cast<const double *>(reinterpret_cast<unsigned char *>(pin) + 64);
         trace[0] = t[0];
         trace[1] = t[1];
+    }
+    if (hf[2])
+    {
+        b200_set_error(BML_B200_ERR_TIMEOUT, "ELLBLOCK multiply: a block copy did not complete");
+        return false;
     }
     if (hf[0])
     {

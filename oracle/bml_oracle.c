@@ -387,98 +387,14 @@ int oracle_ellpack_sp2_d(int N, int M, const double *hv, const int *hix, const i
     return it;
 }
 
-/* ---- ELLBLOCK X^2: ellblock/bml_multiply_ellblock_typed.c:246-442 ----------
- * Block product x += X_ib,jb * X_jb,kb element by element as the reference's
- * micro-kernels form it (:28-168): for output (ii, jj) the sum
- * a0*b0 + a1*b1 + ... is evaluated left to right and then added to x. */
-int oracle_ellblock_x2_d(int NB, int MB, const int *bsize, double *const *blocks,
-                         const int *indexb, const int *nnzb, double thr, int MB2,
-                         double *const *out_blocks, int *out_indexb, int *out_nnzb,
-                         double *trace, int trace_quirk)
-{
-    int maxbs = 0;
-    for (int ib = 0; ib < NB; ib++)
-        if (bsize[ib] > maxbs)
-            maxbs = bsize[ib];
-    size_t bs2 = (size_t) maxbs * maxbs;
-    int *ix = calloc((size_t) NB, sizeof(int));
-    int *jx = calloc((size_t) NB, sizeof(int));
-    double *acc = calloc((size_t) NB * bs2, sizeof(double));
-    double trX = 0.0, trX2 = 0.0;
-    int maxw = 0;
-    for (int ib = 0; ib < NB; ib++)
-    {
-        int lb = 0;
-        for (int jp = 0; jp < nnzb[ib]; jp++)
-        {
-            int ind = ib * MB + jp;
-            const double *L = blocks[ind];
-            int jb = indexb[ind];
-            int bj = bsize[jb];
-            if (jb == ib)
-                for (int kk = 0; kk < bsize[ib]; kk++)
-                    trX += L[kk * (1 + bsize[ib])];
-            for (int kp = 0; kp < nnzb[jb]; kp++)
-            {
-                int indk = jb * MB + kp;
-                int kb = indexb[indk];
-                if (ix[kb] == 0)
-                {
-                    memset(acc + (size_t) kb * bs2, 0, sizeof(double) * bs2);
-                    jx[lb++] = kb;
-                    ix[kb] = ib + 1;
-                }
-                double *x = acc + (size_t) kb * bs2;
-                const double *R = blocks[indk];
-                int bk = bsize[kb];
-                for (int ii = 0; ii < bsize[ib]; ii++)
-                    for (int jj = 0; jj < bk; jj++)
-                    {
-                        double s = L[ii * bj + 0] * R[0 * bk + jj];
-                        for (int l = 1; l < bj; l++)
-                            s = s + L[ii * bj + l] * R[l * bk + jj];
-                        x[ii * bk + jj] = x[ii * bk + jj] + s;
-                    }
-            }
-        }
-        if (lb > maxw)
-            maxw = lb;
-        int ll = 0;
-        for (int q = 0; q < lb; q++)
-        {
-            int kb = jx[q];
-            double *x = acc + (size_t) kb * bs2;
-            int ne = bsize[ib] * bsize[kb];
-            double normx = 0.0;
-            for (int e = 0; e < ne; e++)
-                if (fabs(x[e]) > normx)
-                    normx = fabs(x[e]);
-            if (kb == ib || normx > thr)
-            {
-                if (kb == ib)
-                {
-                    int stride = trace_quirk ? 1 + bsize[q] : 1 + bsize[ib];
-                    for (int kk = 0; kk < bsize[ib]; kk++)
-                        trX2 += x[kk * stride];
-                }
-                if (ll < MB2)
-                {
-                    memcpy(out_blocks[ib * MB2 + ll], x, sizeof(double) * (size_t) ne);
-                    out_indexb[ib * MB2 + ll] = kb;
-                }
-                ll++;
-            }
-            ix[kb] = 0;
-        }
-        out_nnzb[ib] = ll < MB2 ? ll : MB2;
-    }
-    if (trace)
-    {
-        trace[0] = trX;
-        trace[1] = trX2;
-    }
-    free(ix);
-    free(jx);
-    free(acc);
-    return maxw;
-}
+/* ---- ELLBLOCK X^2 in both real precisions ---------------------------------- */
+#define EB_REAL double
+#define EB_X2_NAME oracle_ellblock_x2_d
+#include "bml_oracle_eb_x2.inc"
+#undef EB_REAL
+#undef EB_X2_NAME
+#define EB_REAL float
+#define EB_X2_NAME oracle_ellblock_x2_s
+#include "bml_oracle_eb_x2.inc"
+#undef EB_REAL
+#undef EB_X2_NAME

@@ -59,5 +59,10 @@ int oracle_ellblock_x2_d(int NB, int MB, const int *bsize, double *const *blocks
                          const int *indexb, const int *nnzb, double thr, int MB2,
                          double *const *out_blocks, int *out_indexb, int *out_nnzb,
                          double *trace, int trace_quirk);
+/* The same in single precision (blocks, products and sums in float). */
+int oracle_ellblock_x2_s(int NB, int MB, const int *bsize, float *const *blocks,
+                         const int *indexb, const int *nnzb, double thr, int MB2,
+                         float *const *out_blocks, int *out_indexb, int *out_nnzb,
+                         double *trace, int trace_quirk);
 
 #endif

@@ -231,37 +231,42 @@ def same_rows_exact(a, b, Ma, Mb):
     return True
 
 
-def rest_ellblock_x2(bsize, indexb, nnzb, MB, dense, thr, MB2, trace_quirk=0):
+def rest_ellblock_x2(bsize, indexb, nnzb, MB, dense, thr, MB2, trace_quirk=0, prec=DOUBLE, lists=False):
     """ELLBLOCK X^2 by the restatement; blocks of `dense` at the positions the
-    block lists name.  Returns (dense X^2, traces, widest block row)."""
+    block lists name, in the matrix precision `prec`.  Returns (dense X^2,
+    traces, widest block row), and with lists=True also the output block
+    lists (indexb[NB*MB2], nnzb[NB])."""
     lib = rest()
+    dt, ct = _dt(prec), _ct(prec)
     bsize = np.asarray(bsize, np.int32)
     NB = len(bsize)
     off = np.concatenate([[0], np.cumsum(bsize)])
     maxbs = int(bsize.max())
-    pool = np.zeros((NB * MB, maxbs * maxbs))
+    pool = np.zeros((NB * MB, maxbs * maxbs), dt)
     for ib in range(NB):
         for jp in range(int(nnzb[ib])):
             jb = int(indexb[ib * MB + jp])
             blk = dense[off[ib]:off[ib + 1], off[jb]:off[jb + 1]]
             pool[ib * MB + jp, :blk.size] = blk.reshape(-1)
-    out = np.zeros((NB * MB2, maxbs * maxbs))
-    ptrs = (C.POINTER(C.c_double) * (NB * MB))(*[pool[q].ctypes.data_as(C.POINTER(C.c_double)) for q in range(NB * MB)])
-    optrs = (C.POINTER(C.c_double) * (NB * MB2))(*[out[q].ctypes.data_as(C.POINTER(C.c_double)) for q in range(NB * MB2)])
+    out = np.zeros((NB * MB2, maxbs * maxbs), dt)
+    ptrs = (C.POINTER(ct) * (NB * MB))(*[pool[q].ctypes.data_as(C.POINTER(ct)) for q in range(NB * MB)])
+    optrs = (C.POINTER(ct) * (NB * MB2))(*[out[q].ctypes.data_as(C.POINTER(ct)) for q in range(NB * MB2)])
     oix = np.zeros(NB * MB2, np.int32)
     onz = np.zeros(NB, np.int32)
     tr = np.zeros(2)
     ib_ = np.ascontiguousarray(indexb, np.int32)
     nb_ = np.ascontiguousarray(nnzb, np.int32)
-    lib.oracle_ellblock_x2_d.restype = C.c_int
-    w = lib.oracle_ellblock_x2_d(NB, MB, _p(bsize, C.c_int), ptrs, _p(ib_, C.c_int), _p(nb_, C.c_int),
-                                 C.c_double(thr), MB2, optrs, _p(oix, C.c_int), _p(onz, C.c_int),
-                                 _p(tr, C.c_double), trace_quirk)
+    fn = lib.oracle_ellblock_x2_d if prec == DOUBLE else lib.oracle_ellblock_x2_s
+    fn.restype = C.c_int
+    w = fn(NB, MB, _p(bsize, C.c_int), ptrs, _p(ib_, C.c_int), _p(nb_, C.c_int), C.c_double(thr), MB2, optrs,
+           _p(oix, C.c_int), _p(onz, C.c_int), _p(tr, C.c_double), trace_quirk)
     N = int(off[-1])
-    d2 = np.zeros((N, N))
+    d2 = np.zeros((N, N), dt)
     for ib in range(NB):
         for jp in range(int(onz[ib])):
             jb = int(oix[ib * MB2 + jp])
             r, c = bsize[ib], bsize[jb]
             d2[off[ib]:off[ib + 1], off[jb]:off[jb + 1]] = out[ib * MB2 + jp, :r * c].reshape(r, c)
+    if lists:
+        return d2, tr, w, oix, onz
     return d2, tr, w

@@ -1,0 +1,168 @@
+"""ELLBLOCK X^2 and A*B with uniform 32 x 32 blocks (the register-tiled
+kernel) against the C restatement of bml_multiply_x2_ellblock
+(ellblock/bml_multiply_ellblock_typed.c:246-442), which is pinned to the
+reference at block sizes <= 6 (the reference itself cannot run 32-wide
+blocks without libxsmm).
+
+Bit-exact: every element of the product, in both precisions, and the block
+lists in first-touch order.  The second stage takes the product as its left
+input, so a list order that differed would change the sums.  A*B is checked
+through the square of the block matrix [[0, A], [0, B]], whose upper right
+part is A*B summed in the same order."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import bml_b200 as B
+
+pytestmark = pytest.mark.gpu
+ELLBLOCK, DOUBLE, SINGLE = 3, 2, 1
+BS = 32
+
+
+def block_lattice(L, radius, seed=0):
+    """Dense symmetric matrix of L^3 blocks of 32 x 32: block (a, b) nonzero
+    when the block sites are within `radius`, entries N(0,1) exp(-d)."""
+    rng = np.random.default_rng(seed)
+    nb = L ** 3
+    pos = np.array([(x, y, z) for z in range(L) for y in range(L) for x in range(L)])
+    H = np.zeros((nb * BS, nb * BS))
+    for a in range(nb):
+        for b in range(a, nb):
+            d = np.sqrt(((pos[a] - pos[b]) ** 2).sum())
+            if d <= radius:
+                blk = rng.standard_normal((BS, BS)) * np.exp(-d)
+                if a == b:
+                    blk = (blk + blk.T) / 2
+                H[a * BS:(a + 1) * BS, b * BS:(b + 1) * BS] = blk
+                H[b * BS:(b + 1) * BS, a * BS:(a + 1) * BS] = blk.T
+    return H
+
+
+def set_partition(nb):
+    arr = (C.c_int * nb)(*([BS] * nb))
+    B.lib.bml_b200_reset_block_sizes()
+    B.lib.bml_set_block_sizes(arr, nb, nb)
+
+
+def dt(prec):
+    return np.float64 if prec == DOUBLE else np.float32
+
+
+def from_dense(D, prec):
+    N = D.shape[0]
+    a = np.ascontiguousarray(D, dtype=dt(prec))
+    h = B.lib.bml_import_from_dense(ELLBLOCK, prec, 0, N, N, a.ctypes.data_as(C.c_void_p), 0.0, 0)
+    B.check()
+    return h
+
+
+def to_dense(h, N, prec):
+    p = B.lib.bml_export_to_dense(h, 0)
+    B.check()
+    ct = C.c_double if prec == DOUBLE else C.c_float
+    d = np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape=(N * N,)).copy()
+    B.lib.bml_free_memory(C.c_void_p(p))
+    return d.reshape(N, N)
+
+
+def lists(O, h):
+    """(indexb, nnzb, MB) of a matrix of this library, read from its host
+    mirror (the leading struct fields are the reference's)."""
+    assert B.lib.bml_get_bandwidth(h) >= 0  # brings the host mirror up to date
+    st = C.cast(h, C.POINTER(O.EllblockStruct)).contents
+    nnzb = np.ctypeslib.as_array(st.nnzb, shape=(st.NB,)).copy()
+    indexb = np.ctypeslib.as_array(st.indexb, shape=(st.NB * st.MB,)).copy()
+    return indexb, nnzb, st.MB
+
+
+def rows(indexb, nnzb, MB):
+    return [list(indexb[ib * MB:ib * MB + nnzb[ib]]) for ib in range(len(nnzb))]
+
+
+def free(*hs):
+    for h in hs:
+        hh = C.c_void_p(h)
+        B.lib.bml_deallocate(C.byref(hh))
+
+
+def same_bits(a, b):
+    return a.dtype == b.dtype and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.mark.parametrize("prec", [DOUBLE, SINGLE])
+@pytest.mark.parametrize("L,radius,thr", [(3, 1.0, 0.0), (4, 1.0, 0.05), (3, 1.8, 1e-3)])
+def test_x2_blocks32_bit_exact(oracle_mod, prec, L, radius, thr):
+    O = oracle_mod
+    nb = L ** 3
+    N = nb * BS
+    H = block_lattice(L, radius).astype(dt(prec))
+    set_partition(nb)
+    try:
+        X = from_dense(H, prec)
+        X2 = B.lib.bml_zero_matrix(ELLBLOCK, prec, N, N, 0)
+        X4 = B.lib.bml_zero_matrix(ELLBLOCK, prec, N, N, 0)
+        B.check()
+        p = B.lib.bml_multiply_x2(X, X2, C.c_double(thr))
+        B.check()
+        tr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(2,)).copy()
+        B.lib.bml_free_memory(C.c_void_p(p))
+        ix, nz, MB = lists(O, X)
+        d2, rtr, _, oix, onz = O.rest_ellblock_x2([BS] * nb, ix, nz, MB, H, thr, nb, prec=prec, lists=True)
+        got2 = to_dense(X2, N, prec)
+        assert same_bits(got2, d2), "X^2 differs from the restatement"
+        gix, gnz, gMB = lists(O, X2)
+        assert rows(gix, gnz, gMB) == rows(oix, onz, nb), "block lists differ"
+        rel = 1e-12 if prec == DOUBLE else 1e-5
+        assert tr[0] == pytest.approx(rtr[0], rel=rel)
+        assert tr[1] == pytest.approx(rtr[1], rel=rel)
+
+        # X^2 as the left input: its list order sets the order of the sums
+        B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(X2, X4, C.c_double(thr))))
+        B.check()
+        d4, _, _ = O.rest_ellblock_x2([BS] * nb, gix, gnz, gMB, got2, thr, nb, prec=prec)
+        assert same_bits(to_dense(X4, N, prec), d4), "(X^2)^2 differs from the restatement"
+        free(X, X2, X4)
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
+
+
+def test_multiply_ab_blocks32_bit_exact(oracle_mod):
+    O = oracle_mod
+    L, thr = 3, 0.0
+    nb = L ** 3
+    N = nb * BS
+    Ad = block_lattice(L, 1.5, seed=1)
+    Bd = block_lattice(L, 1.0, seed=2)
+    set_partition(nb)
+    try:
+        A = from_dense(Ad, DOUBLE)
+        Bm = from_dense(Bd, DOUBLE)
+        Cm = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+        B.check()
+        B.lib.bml_multiply_AB(A, Bm, Cm, C.c_double(thr))
+        B.check()
+        got = to_dense(Cm, N, DOUBLE)
+        ra = rows(*lists(O, A))
+        rb = rows(*lists(O, Bm))
+        gc = rows(*lists(O, Cm))
+        free(A, Bm, Cm)
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
+
+    # M = [[0, A], [0, B]]: row ib of M^2 (ib < nb) sums A[ib,jb] B[jb,kb] in
+    # the order of A's row, then B's row, exactly as A*B does
+    M = np.zeros((2 * N, 2 * N))
+    M[:N, N:] = Ad
+    M[N:, N:] = Bd
+    mrows = [[nb + j for j in r] for r in ra] + [[nb + k for k in r] for r in rb]
+    MB = max(len(r) for r in mrows)
+    indexb = np.zeros(2 * nb * MB, np.int32)
+    nnzb = np.array([len(r) for r in mrows], np.int32)
+    for ib, r in enumerate(mrows):
+        indexb[ib * MB:ib * MB + len(r)] = r
+    d2, _, _, oix, onz = O.rest_ellblock_x2([BS] * (2 * nb), indexb, nnzb, MB, M, thr, 2 * nb, lists=True)
+    assert same_bits(got, np.ascontiguousarray(d2[:N, N:]))
+    want = [[k - nb for k in r] for r in rows(oix, onz, 2 * nb)[:nb]]
+    assert gc == want

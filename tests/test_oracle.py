@@ -3,6 +3,7 @@
 from the reference library (tests/golden/make_golden.py) and, where the
 reference library is built here (oracle/_ref/libbml_ref.so), the reference
 itself on further inputs.  CPU only."""
+import ctypes as C
 import hashlib
 import json
 import os
@@ -100,3 +101,51 @@ def test_restatement_x2_matches_reference(ref, thr, prec):
         assert otr[1] == pytest.approx(tr[1], rel=1e-5 if prec == O.SINGLE else 1e-12)
         ref.ref_free(A)
         ref.ref_free(R2)
+
+
+@pytest.mark.parametrize("thr", [0.0, 0.5])
+@pytest.mark.parametrize("prec", [O.DOUBLE, O.SINGLE])
+def test_restatement_ellblock_x2_matches_reference(ref, prec, thr):
+    """The ELLBLOCK X^2 restatement, in both precisions, against the
+    reference's bml_multiply_x2 on block sizes 1..6 (the sizes its micro
+    kernels cover): identical products and block lists."""
+    N = 48
+    bs, count = [], 0
+    while count < N:
+        b = min((5 + len(bs)) % 6 + 1, N - count)
+        bs.append(b)
+        count += b
+    nb = len(bs)
+    lib = ref.ref()
+    lib.bml_set_block_sizes((C.c_int * nb)(*bs), nb, nb)
+    off = np.concatenate([[0], np.cumsum(bs)])
+    rng = np.random.default_rng(5)
+    D = np.zeros((N, N))
+    for a in range(nb):
+        for b in range(nb):
+            if a == b or rng.random() < 0.4:
+                D[off[a]:off[a + 1], off[b]:off[b + 1]] = rng.standard_normal((bs[a], bs[b]))
+    D = D.astype(O._dt(prec))
+    R = lib.bml_import_from_dense(3, prec, 0, N, N, D.ctypes.data_as(C.c_void_p), 0.0, 0)
+    R2 = lib.bml_zero_matrix(3, prec, N, N, 0)
+    p = lib.bml_multiply_x2(R, R2, thr)
+    rtr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(2,)).copy()
+    lib.bml_free_memory(p)
+    st = C.cast(R, C.POINTER(O.EllblockStruct)).contents
+    ix = np.ctypeslib.as_array(st.indexb, shape=(st.NB * st.MB,)).copy()
+    nz = np.ctypeslib.as_array(st.nnzb, shape=(st.NB,)).copy()
+    d2, tr, _, oix, onz = O.rest_ellblock_x2(bs, ix, nz, st.MB, D, thr, nb, trace_quirk=1, prec=prec, lists=True)
+    q = lib.bml_export_to_dense(R2, 0)
+    got = np.ctypeslib.as_array(C.cast(q, C.POINTER(O._ct(prec))), shape=(N * N,)).copy().reshape(N, N)
+    lib.bml_free_memory(q)
+    s2 = C.cast(R2, C.POINTER(O.EllblockStruct)).contents
+    rix = np.ctypeslib.as_array(s2.indexb, shape=(s2.NB * s2.MB,)).copy()
+    rnz = np.ctypeslib.as_array(s2.nnzb, shape=(s2.NB,)).copy()
+    for h in (R, R2):
+        ref.ref_free(h)
+    assert np.array_equal(got.view(np.uint8), d2.view(np.uint8))
+    assert np.array_equal(rnz, onz)
+    for ib in range(nb):
+        assert np.array_equal(rix[ib * s2.MB:ib * s2.MB + rnz[ib]], oix[ib * nb:ib * nb + onz[ib]])
+    assert tr[0] == pytest.approx(rtr[0], rel=1e-12 if prec == O.DOUBLE else 1e-6)
+    assert tr[1] == pytest.approx(rtr[1], rel=1e-12 if prec == O.DOUBLE else 1e-6)
