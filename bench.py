@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-tc", action="store_true",
                     help="run the small tensor-core ELLBLOCK case for an ncu capture (10^3 block lattice)")
+    ap.add_argument("--profile-eb", action="store_true",
+                    help="run the small exact ELLBLOCK case for an ncu capture (10^3 block lattice)")
     ap.add_argument("--no-ellblock", action="store_true", help="skip the ELLBLOCK tensor-core leg")
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: 30^3 lattice, 3 SP2 iterations then one X^2")
@@ -597,6 +599,18 @@ def block_lattice_products(L, radius):
     return total
 
 
+def run_profile_eb():
+    """Three exact FP64 X^2 calls on the 10^3 block lattice (N = 32000)."""
+    import bml_b200 as B
+    H, n = ellblock_case(10)
+    X2 = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    B.check()
+    for _ in range(3):
+        B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(H, X2, C.c_double(1e-6))))
+        B.check()
+    print(json.dumps({"profile_case": "10^3 block lattice, exact FP64 X^2", "trace": B.lib.bml_trace(X2)}))
+
+
 def ellblock_leg(reps=3):
     """The mixed ELLBLOCK configuration's product: X^2 of H on the 16^3 block
     lattice (4096 block rows of 32, N = 131072, threshold 1e-6), on the
@@ -664,6 +678,9 @@ def main():
         return
     if args.profile_ops:
         run_profile_ops()
+        return
+    if args.profile_eb:
+        run_profile_eb()
         return
     if args.impl == "reference":
         res = run_reference(args, rank, world)

@@ -1068,27 +1068,29 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
 // first-touch slot order, same keep rule, so the results are bit-identical to
 // eb_mul_kernel's.
 //
-// Four warps per CTA: warp w forms rows 8w..8w+7 of the 32 x 32 product and
-// lane c its column c, so for every 16 bytes of the left block a lane reads
-// (one broadcast shared-memory load) it does 16 / sizeof(T) multiply-adds
-// per row.  Thread 0 copies the blocks with cp.async.bulk ahead of use: the
-// left block X[ib,jb] into one of two buffers, the right blocks X[jb,kb]
-// through a ring of EB32_STAGES buffers, completing on mbarriers (bounded
-// waits; a wait that runs out raises flags[2]).  At the start of every left
-// block (in segments of EB32_SEG right blocks) all threads assign the slots
-// of its right blocks at once: a ballot prefix in kp order appends first
-// touches to the row's list.  Accumulators stay in the per-CTA slab, each
-// element owned by one thread.
-// Shared memory: EbS32<T> (48 KB for double, four CTAs per SM).
+// Four warps per CTA.  Lane r holds row r of the left block X[ib,jb] in
+// registers (staged once per left block through a padded transpose in
+// shared memory); warp w forms columns 8w..8w+7 of each block product, so a
+// broadcast 16-byte load of a right-block row feeds 16 / sizeof(T)
+// multiply-adds and the left block is not re-read per product.  Thread 0
+// copies the right blocks X[jb,kb] with cp.async.bulk through a ring of
+// EB32_STAGES buffers ahead of use, completing on mbarriers (bounded waits;
+// a wait that runs out raises flags[2]).  At the start of every left block
+// (in segments of EB32_SEG right blocks) all threads assign the slots of its
+// right blocks at once: a ballot prefix in kp order appends first touches to
+// the row's list.  Accumulators stay in the per-CTA slab, column-major
+// within a slot so that every access is coalesced, each element owned by one
+// thread; kept blocks are transposed back to row-major through shared memory
+// on the way out.
+// Shared memory: EbS32<T> (41 KB for double, four CTAs per SM).
 // ---------------------------------------------------------------------------
 constexpr int EB32_STAGES = 3, EB32_THREADS = 128, EB32_SEG = 1024, EB32_LIST = 1024;
 
 template <typename T> struct EbS32
 {
     uint64_t full_r[EB32_STAGES];
-    uint64_t full_l[2];
-    __align__(16) T L[2][1024];
-    __align__(16) T R[EB32_STAGES][1024];
+    __align__(16) T R[EB32_STAGES][1024]; // right blocks; after a row's products, transpose scratch
+    T Lt[32 * 33];                         // left block transposed, padded: Lt[l*33 + r] = L[r][l]
     int slotq[EB32_SEG]; // per kp of the segment: slot, or -(slot + 1) on first touch; then per slot:
                          // output position, -1 when dropped
     int list[EB32_LIST]; // kb per slot, first-touch order
@@ -1179,17 +1181,13 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
     {
         for (int s = 0; s < EB32_STAGES; ++s)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(eb_su32(&S.full_r[s])) : "memory");
-        for (int s = 0; s < 2; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(eb_su32(&S.full_l[s])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    // running counts over every row of this CTA (uniform): right blocks
-    // consumed, left blocks started
-    unsigned consumed = 0, lcur = 0;
+    unsigned consumed = 0; // right blocks consumed over every row of this CTA (uniform)
     // producer state (thread 0): copies issued, and the next pair (pj, pk)
-    unsigned issued = 0, lissued = 0;
+    unsigned issued = 0;
     int pj = 0, pk = 0, pnk = 0, pjb = 0;
 
     for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
@@ -1208,16 +1206,11 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
             }
         };
         auto produce = [&]() {
-            // generic-proxy reads of the buffers being refilled are ordered
-            // before the bulk copies by the barrier and this fence
+            // generic-proxy accesses of the buffers being refilled are
+            // ordered before the bulk copies by the barrier and this fence
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            while (pj < na && issued - consumed < (unsigned) EB32_STAGES && (pk > 0 || lissued <= lcur + 1))
+            while (pj < na && issued - consumed < (unsigned) EB32_STAGES)
             {
-                if (pk == 0)
-                {
-                    eb_bulk(S.L[lissued & 1], A.blk(ib, pj), BLK, &S.full_l[lissued & 1]);
-                    ++lissued;
-                }
                 const unsigned s = issued % EB32_STAGES;
                 eb_bulk(S.R[s], B.blk(pjb, pk), BLK, &S.full_r[s]);
                 ++issued;
@@ -1243,17 +1236,21 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
         {
             const int jb = arow[jp];
             const int nk = B.nnzb[jb];
+            const T *L = A.blk(ib, jp);
             if (jb == ib && tid == 0)
-            {
-                const T *L = A.blk(ib, jp);
                 for (int kk = 0; kk < 32; ++kk)
                     trA = add_rn(trA, L[kk * 33]);
-            }
             if (nk == 0)
                 continue;
+            // the left block, transposed into shared memory (ordered before
+            // its reads by the barriers of the slot assignment)
+#pragma unroll
+            for (int u = 0; u < 1024 / EB32_THREADS; ++u)
+            {
+                const int e = u * EB32_THREADS + tid;
+                S.Lt[(e & 31) * 33 + (e >> 5)] = L[e];
+            }
             const int *brow = B.indexb + (size_t) jb * B.MB;
-            eb_wait(&S.full_l[lcur & 1], (lcur >> 1) & 1, tflag);
-            const T *Ls = S.L[lcur & 1];
             for (int seg0 = 0; seg0 < nk; seg0 += EB32_SEG)
             {
                 const int ns = min(EB32_SEG, nk - seg0);
@@ -1294,6 +1291,11 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
                     lb += tot;
                     __syncthreads();
                 }
+                // this lane's row of the left block
+                T lrow[32];
+#pragma unroll
+                for (int l = 0; l < 32; ++l)
+                    lrow[l] = S.Lt[l * 33 + lane];
                 for (int q = 0; q < ns; ++q)
                 {
                     const unsigned st = consumed % EB32_STAGES;
@@ -1303,41 +1305,34 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
                     const int sl = first ? -code - 1 : code;
                     if (sl < cap)
                     {
+                        // element (r, c) of a slot at c*32 + r
                         T *x = myslab + (size_t) sl * 1024 + warp * 8 * 32 + lane;
                         T xo[8];
 #pragma unroll
-                        for (int r = 0; r < 8; ++r)
-                            xo[r] = first ? T(0) : x[r * 32];
-                        const T *Rs = S.R[st] + lane;
-                        const VT *La = reinterpret_cast<const VT *>(Ls + warp * 8 * 32);
+                        for (int c = 0; c < 8; ++c)
+                            xo[c] = first ? T(0) : x[c * 32];
+                        const VT *rb = reinterpret_cast<const VT *>(S.R[st] + warp * 8);
                         T s[8];
 #pragma unroll
-                        for (int l0 = 0; l0 < 32; l0 += NV)
+                        for (int l = 0; l < 32; ++l)
                         {
-                            VT a[8];
+                            VT bv[8 / NV];
 #pragma unroll
-                            for (int r = 0; r < 8; ++r)
-                                a[r] = La[(r * 32 + l0) / NV];
+                            for (int u = 0; u < 8 / NV; ++u)
+                                bv[u] = rb[l * (32 / NV) + u];
 #pragma unroll
-                            for (int v = 0; v < NV; ++v)
+                            for (int c = 0; c < 8; ++c)
                             {
-                                const T b = Rs[(l0 + v) * 32];
-#pragma unroll
-                                for (int r = 0; r < 8; ++r)
-                                {
-                                    const T p = mul_rn(V::at(a[r], v), b);
-                                    s[r] = (l0 + v == 0) ? p : add_rn(s[r], p);
-                                }
+                                const T p = mul_rn(lrow[l], V::at(bv[c / NV], c % NV));
+                                s[c] = l == 0 ? p : add_rn(s[c], p);
                             }
                         }
 #pragma unroll
-                        for (int r = 0; r < 8; ++r)
-                            x[r * 32] = add_rn(xo[r], s[r]);
+                        for (int c = 0; c < 8; ++c)
+                            x[c * 32] = add_rn(xo[c], s[c]);
                     }
                     __syncthreads();
                     ++consumed;
-                    if (seg0 + q == nk - 1)
-                        ++lcur;
                     if (tid == 0)
                         produce();
                 }
@@ -1384,15 +1379,30 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
         }
         __syncthreads();
         const int kept = S.kept;
+        // each warp transposes its blocks back to row-major, 16 columns at a
+        // time, through 32 x 17 elements of the (idle) right-block ring
+        T *tp = &S.R[0][0] + warp * (32 * 17);
         for (int q = warp; q < nl; q += EB32_THREADS / 32)
         {
             const int d = S.slotq[q];
             if (d < 0 || d >= C.MB)
                 continue;
-            const uint4 *src = reinterpret_cast<const uint4 *>(myslab + (size_t) q * 1024);
-            uint4 *dst = reinterpret_cast<uint4 *>(C.blk(ib, d));
-            for (int e = lane; e < (int) (BLK / 16); e += 32)
-                dst[e] = src[e];
+            const T *src = myslab + (size_t) q * 1024;
+            T *dst = C.blk(ib, d);
+            for (int h = 0; h < 2; ++h)
+            {
+#pragma unroll
+                for (int c = 0; c < 16; ++c)
+                    tp[lane * 17 + c] = src[(h * 16 + c) * 32 + lane];
+                __syncwarp();
+#pragma unroll
+                for (int u = 0; u < 16; ++u)
+                {
+                    const int e = u * 32 + lane, r = e >> 4, c = e & 15;
+                    dst[r * 32 + h * 16 + c] = tp[r * 17 + c];
+                }
+                __syncwarp();
+            }
             if (lane == 0)
                 C.indexb[(size_t) ib * C.MB + d] = S.list[q];
         }
@@ -1424,18 +1434,11 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
     // after a timeout, copies still in flight land before the CTA leaves:
     // the last fill of every buffer, each wait bounded
     if (tid == 0 && *reinterpret_cast<volatile int *>(tflag))
-    {
         for (unsigned b = 0; b < (unsigned) EB32_STAGES && b < issued; ++b)
         {
             const unsigned u = issued - 1 - b;
             eb_wait2s(&S.full_r[u % EB32_STAGES], (u / EB32_STAGES) & 1);
         }
-        for (unsigned b = 0; b < 2u && b < lissued; ++b)
-        {
-            const unsigned u = lissued - 1 - b;
-            eb_wait2s(&S.full_l[u & 1], (u >> 1) & 1);
-        }
-    }
 }
 
 template <typename T> int eb_grid(B200Context *c, int NB, int per_sm) { return max(1, min(NB, c->sm_count * per_sm)); }
