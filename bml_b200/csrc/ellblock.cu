@@ -1096,6 +1096,7 @@ template <typename T> struct EbS32
     int list[EB32_LIST]; // kb per slot, first-touch order
     int cnt[EB32_THREADS / 32];
     int kept;
+    int row;
 };
 
 template <typename T> struct Vec16;
@@ -1190,8 +1191,16 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
     unsigned issued = 0;
     int pj = 0, pk = 0, pnk = 0, pjb = 0;
 
-    for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
+    for (;;)
     {
+        // block rows are claimed from a counter (rows differ in cost), by
+        // one thread for the whole CTA
+        if (tid == 0)
+            S.row = atomicAdd(&flags[3], 1);
+        __syncthreads();
+        const int ib = S.row;
+        if (ib >= A.NB)
+            break;
         const int na = A.nnzb[ib];
         const int *arow = A.indexb + (size_t) ib * A.MB;
         // left blocks whose block row of B is empty have no pairs
