@@ -1084,7 +1084,10 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
 // on the way out.
 // Shared memory: EbS32<T> (41 KB for double, four CTAs per SM).
 // ---------------------------------------------------------------------------
-constexpr int EB32_STAGES = 3, EB32_THREADS = 128, EB32_SEG = 1024, EB32_LIST = 1024;
+#ifndef B200_EB32_STAGES
+#define B200_EB32_STAGES 3
+#endif
+constexpr int EB32_STAGES = B200_EB32_STAGES, EB32_THREADS = 128, EB32_SEG = 1024, EB32_LIST = 1024;
 
 template <typename T> struct EbS32
 {

@@ -12,7 +12,7 @@
 // result is written back in the matrix precision; blocks are kept as in the
 // reference (kb == ib, or max |x| > threshold), the traces are FP64 sums.
 //
-// Work: one CTA per SM, persistent over groups of four consecutive block rows
+// Work: persistent CTAs, claiming from a counter groups of four consecutive block rows
 // ib0..ib0+3, which share most of their block columns jb on a lattice.  For
 // the group, with M = 128 = 4 x 32 rows:
 //   D[kb] (128 x 32, FP32, in TMEM) += [X[ib0,jb]; ..; X[ib0+3,jb]] X[jb,kb]
@@ -295,7 +295,7 @@ template <class Cfg> struct TcSmem
     uint64_t empty_a[Cfg::ABUF];            // MMAs reading an A buffer's fill (and all before) done
     uint64_t done;                        // all MMAs of a wave done
     unsigned tmem;
-    int nJ, nK, npairs, ok, dead;
+    int nJ, nK, npairs, ok, dead, grp;
     int jb[Cfg::JCAP];             // union of the group's block columns
     short jslot[Cfg::JCAP][TC_GROUP]; // position of X[ib0+q, jb] in row ib0+q, or -1
     int klist[Cfg::KCAP];          // kb of each output tile
@@ -387,7 +387,7 @@ __device__ void rank_bits(const unsigned *bits, int *pre, int *list, int cap, in
 }
 
 // flags: [0] row overflow, [1] widest kept row, [2] group over capacity,
-// [3] a tensor-core wait timed out
+// [3] a tensor-core wait timed out, [4] next group to claim
 template <typename T, class Cfg>
 __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     tc_x2_kernel(TcView<T> X, TcOut<T> C, const tc_t *img, const tc_t *zimg, double thr,
@@ -433,8 +433,16 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     unsigned gp = 0, ga = 0, nwaves = 0;
     unsigned copied_a = 0; // left operands whose copies thread 0 issued
 
-    for (int grp = blockIdx.x; grp < ngroups && !dead; grp += gridDim.x)
+    for (;;)
     {
+        // groups are claimed from a counter (they differ in cost), by one
+        // thread for the whole CTA
+        if (tid == 0)
+            S.grp = atomicAdd(&flags[4], 1);
+        __syncthreads();
+        const int grp = S.grp;
+        if (grp >= ngroups || dead)
+            break;
         const int ib0 = grp * TC_GROUP;
         // ---- the group's block columns J: a bitmap over NB, index = rank ----
         const int nwords = (X.NB + 31) >> 5;
@@ -968,7 +976,7 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     int hf[4];
     for (int shape = 0; shape < 2; ++shape)
     {
-        if (shape == 1 && !CUDA_OK(cudaMemsetAsync(flags, 0, 16, c->stream)))
+        if (shape == 1 && !CUDA_OK(cudaMemsetAsync(flags, 0, 20, c->stream)))
             return false;
         if (X->matrix_precision == double_real)
             ok = shape == 0 ? tc_launch<double, TcSmall>(c, X, X2, img, zimg, threshold, dA, dC, flags)
