@@ -13,6 +13,7 @@
 #include "ellblock.h"
 #include "device_util.cuh"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
@@ -941,18 +942,18 @@ template <typename T> __global__ void eb_export_kernel(EbView<T> A, T *D, int N,
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, EbView<T> C, double thr,
-                                                     int use_norm_inf_fast, T *slab, int *marks,
-                                                     double *dA, double *dC, int *flags)
+                                                     int use_norm_inf_fast, int cap, T *slab, int *lists,
+                                                     int *marks, double *dA, double *dC, int *flags)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int maxbs = (int) sqrtf((float) A.slot + 0.5f);
     T *sL = reinterpret_cast<T *>(smem);
     T *sR = sL + (size_t) maxbs * maxbs;
-    int *list = reinterpret_cast<int *>(sR + (size_t) maxbs * maxbs); // kb in first-touch order
     __shared__ int lb, firstflag, slotq;
     __shared__ double red[32];
-    const int cap = min(C.MB + 1, 1024); // slab slots (one spare to detect overflow)
+    // cap slab slots and list entries per CTA (first-touch order)
     T *myslab = slab + (size_t) blockIdx.x * cap * A.slot;
+    int *list = lists + (size_t) blockIdx.x * cap;
     int *mark = marks + (size_t) blockIdx.x * B.NB;
     for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
     {
@@ -983,7 +984,7 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
                     {
                         firstflag = 1;
                         slotq = lb;
-                        if (lb < 1024)
+                        if (lb < cap)
                             list[lb] = kb;
                         mark[kb] = lb + 1;
                         lb++;
@@ -1018,14 +1019,12 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
         const int n = lb;
         int kept = 0;
         T trC = T(0);
-        for (int q = 0; q < min(n, 1024); ++q)
+        for (int q = 0; q < min(n, cap); ++q)
         {
             const int kb = list[q];
             const int bk = B.bsize[kb];
             if (threadIdx.x == 0)
                 mark[kb] = 0;
-            if (q >= cap)
-                continue;
             const T *x = myslab + (size_t) q * A.slot;
             const double normx = block_norm_inf(x, bi * bk, red);
             const bool keep = kb == ib || (use_norm_inf_fast ? normx > thr : (T) normx > (T) thr);
@@ -1050,8 +1049,10 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
         {
             C.nnzb[ib] = kept < C.MB ? kept : C.MB;
             atomicMax(&flags[1], kept);
-            if (kept > C.MB || n > cap)
+            if (kept > C.MB)
                 atomicExch(&flags[0], 1);
+            if (n > cap)
+                atomicExch(&flags[4], 1);
             if (dA)
                 dA[ib] = (double) trA;
             if (dC)
@@ -1087,16 +1088,15 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
 #ifndef B200_EB32_STAGES
 #define B200_EB32_STAGES 3
 #endif
-constexpr int EB32_STAGES = B200_EB32_STAGES, EB32_THREADS = 128, EB32_SEG = 1024, EB32_LIST = 1024;
+constexpr int EB32_STAGES = B200_EB32_STAGES, EB32_THREADS = 128, EB32_SEG = 1024;
 
 template <typename T> struct EbS32
 {
     uint64_t full_r[EB32_STAGES];
     __align__(16) T R[EB32_STAGES][1024]; // right blocks; after a row's products, transpose scratch
     T Lt[32 * 33];                         // left block transposed, padded: Lt[l*33 + r] = L[r][l]
-    int slotq[EB32_SEG]; // per kp of the segment: slot, or -(slot + 1) on first touch; then per slot:
-                         // output position, -1 when dropped
-    int list[EB32_LIST]; // kb per slot, first-touch order
+    int slotq[EB32_SEG]; // per kp of the segment: slot, or -(slot + 1) on first touch; then, per
+                         // chunk of EB32_SEG slots, output position (-1 when dropped)
     int cnt[EB32_THREADS / 32];
     int kept;
     int row;
@@ -1166,8 +1166,9 @@ __device__ __forceinline__ void eb_wait(uint64_t *bar, unsigned parity, int *fla
 
 template <typename T>
 __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, EbView<T> B, EbView<T> C, double thr,
-                                                                  int use_norm_inf_fast, T *slab, int *marks,
-                                                                  double *dA, double *dC, int *flags)
+                                                                  int use_norm_inf_fast, int cap, T *slab,
+                                                                  int *lists, int *marks, double *dA, double *dC,
+                                                                  int *flags)
 {
     using V = Vec16<T>;
     using VT = typename V::type;
@@ -1176,8 +1177,9 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
     extern __shared__ __align__(128) unsigned char smem[];
     EbS32<T> &S = *reinterpret_cast<EbS32<T> *>(smem);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cap = min(C.MB + 1, EB32_LIST); // slab slots (one spare to detect overflow)
+    // cap slab slots and list entries (kb per slot, first-touch order) per CTA
     T *myslab = slab + (size_t) blockIdx.x * cap * 1024;
+    int *list = lists + (size_t) blockIdx.x * cap;
     int *mark = marks + (size_t) blockIdx.x * B.NB;
     int *tflag = &flags[2];
 
@@ -1295,8 +1297,8 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
                     {
                         sl = lb + pre + __popc(bal & lanemask_lt());
                         mark[kb] = sl + 1;
-                        if (sl < EB32_LIST)
-                            S.list[sl] = kb;
+                        if (sl < cap)
+                            list[sl] = kb;
                     }
                     if (q < ns)
                         S.slotq[q] = isnew ? -(sl + 1) : sl;
@@ -1352,71 +1354,78 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
         }
         __syncthreads();
 
-        // keep (kb == ib or max|x| > thr) and copy out in first-touch order
+        // keep (kb == ib or max|x| > thr) and copy out in first-touch order,
+        // EB32_SEG slots at a time
         const int n = lb;
         const int nl = min(n, cap);
-        for (int q = warp; q < nl; q += EB32_THREADS / 32)
-        {
-            const VT *x = reinterpret_cast<const VT *>(myslab + (size_t) q * 1024);
-            double m = 0.0;
-            for (int e = lane; e < 1024 / NV; e += 32)
-            {
-                const VT v = x[e];
-#pragma unroll
-                for (int u = 0; u < NV; ++u)
-                    m = fmax(m, (double) fabs(V::at(v, u)));
-            }
-            for (int o = 16; o; o >>= 1)
-                m = fmax(m, __shfl_xor_sync(FULL, m, o));
-            const int kb = S.list[q];
-            const bool keep = kb == ib || (use_norm_inf_fast ? m > thr : (T) m > (T) thr);
-            if (lane == 0)
-                S.slotq[q] = keep;
-        }
-        __syncthreads();
-        if (warp == 0)
-        {
-            int base = 0;
-            for (int c0 = 0; c0 < nl; c0 += 32)
-            {
-                const int q = c0 + lane;
-                const bool f = q < nl && S.slotq[q];
-                const unsigned bal = __ballot_sync(FULL, f);
-                if (q < nl)
-                    S.slotq[q] = f ? base + __popc(bal & lanemask_lt()) : -1;
-                base += __popc(bal);
-            }
-            if (lane == 0)
-                S.kept = base;
-        }
-        __syncthreads();
-        const int kept = S.kept;
         // each warp transposes its blocks back to row-major, 16 columns at a
         // time, through 32 x 17 elements of the (idle) right-block ring
         T *tp = &S.R[0][0] + warp * (32 * 17);
-        for (int q = warp; q < nl; q += EB32_THREADS / 32)
+        int kept = 0; // uniform
+        for (int q0 = 0; q0 < nl; q0 += EB32_SEG)
         {
-            const int d = S.slotq[q];
-            if (d < 0 || d >= C.MB)
-                continue;
-            const T *src = myslab + (size_t) q * 1024;
-            T *dst = C.blk(ib, d);
-            for (int h = 0; h < 2; ++h)
+            const int qn = min(EB32_SEG, nl - q0);
+            for (int q = warp; q < qn; q += EB32_THREADS / 32)
             {
-#pragma unroll
-                for (int c = 0; c < 16; ++c)
-                    tp[lane * 17 + c] = src[(h * 16 + c) * 32 + lane];
-                __syncwarp();
-#pragma unroll
-                for (int u = 0; u < 16; ++u)
+                const VT *x = reinterpret_cast<const VT *>(myslab + (size_t) (q0 + q) * 1024);
+                double m = 0.0;
+                for (int e = lane; e < 1024 / NV; e += 32)
                 {
-                    const int e = u * 32 + lane, r = e >> 4, c = e & 15;
-                    dst[r * 32 + h * 16 + c] = tp[r * 17 + c];
+                    const VT v = x[e];
+#pragma unroll
+                    for (int u = 0; u < NV; ++u)
+                        m = fmax(m, (double) fabs(V::at(v, u)));
                 }
-                __syncwarp();
+                for (int o = 16; o; o >>= 1)
+                    m = fmax(m, __shfl_xor_sync(FULL, m, o));
+                const int kb = list[q0 + q];
+                const bool keep = kb == ib || (use_norm_inf_fast ? m > thr : (T) m > (T) thr);
+                if (lane == 0)
+                    S.slotq[q] = keep;
             }
-            if (lane == 0)
-                C.indexb[(size_t) ib * C.MB + d] = S.list[q];
+            __syncthreads();
+            if (warp == 0)
+            {
+                int base = kept;
+                for (int c0 = 0; c0 < qn; c0 += 32)
+                {
+                    const int q = c0 + lane;
+                    const bool f = q < qn && S.slotq[q];
+                    const unsigned bal = __ballot_sync(FULL, f);
+                    if (q < qn)
+                        S.slotq[q] = f ? base + __popc(bal & lanemask_lt()) : -1;
+                    base += __popc(bal);
+                }
+                if (lane == 0)
+                    S.kept = base;
+            }
+            __syncthreads();
+            kept = S.kept;
+            for (int q = warp; q < qn; q += EB32_THREADS / 32)
+            {
+                const int d = S.slotq[q];
+                if (d < 0 || d >= C.MB)
+                    continue;
+                const T *src = myslab + (size_t) (q0 + q) * 1024;
+                T *dst = C.blk(ib, d);
+                for (int h = 0; h < 2; ++h)
+                {
+#pragma unroll
+                    for (int c = 0; c < 16; ++c)
+                        tp[lane * 17 + c] = src[(h * 16 + c) * 32 + lane];
+                    __syncwarp();
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                    {
+                        const int e = u * 32 + lane, r = e >> 4, c = e & 15;
+                        dst[r * 32 + h * 16 + c] = tp[r * 17 + c];
+                    }
+                    __syncwarp();
+                }
+                if (lane == 0)
+                    C.indexb[(size_t) ib * C.MB + d] = list[q0 + q];
+            }
+            __syncthreads(); // slotq and S.kept are rewritten by the next chunk
         }
         if (tid == 0)
         {
@@ -1431,16 +1440,18 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
             }
             C.nnzb[ib] = kept < C.MB ? kept : C.MB;
             atomicMax(&flags[1], kept);
-            if (kept > C.MB || n > cap)
+            if (kept > C.MB)
                 atomicExch(&flags[0], 1);
+            if (n > cap)
+                atomicExch(&flags[4], 1);
             if (dA)
                 dA[ib] = (double) trA;
             if (dC)
                 dC[ib] = (double) trC;
         }
         __syncthreads();
-        for (int q = tid; q < min(n, EB32_LIST); q += EB32_THREADS)
-            mark[S.list[q]] = 0;
+        for (int q = tid; q < nl; q += EB32_THREADS)
+            mark[list[q]] = 0;
         __syncthreads();
     }
     // after a timeout, copies still in flight land before the CTA leaves:
@@ -1458,7 +1469,7 @@ template <typename T> int eb_grid(B200Context *c, int NB, int per_sm) { return m
 int *eb_flags(B200Context *c)
 {
     int *f = reinterpret_cast<int *>(static_cast<unsigned char *>(c->d_small) + 4096);
-    if (!CUDA_OK(cudaMemsetAsync(f, 0, 16, c->stream)))
+    if (!CUDA_OK(cudaMemsetAsync(f, 0, 32, c->stream)))
         return nullptr;
     return f;
 }
@@ -1505,62 +1516,80 @@ bool eb_multiply_typed(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_m
     bool bs32 = A->maxbs == 32 && B->maxbs == 32 && C->maxbs == 32;
     for (int ib = 0; bs32 && ib < A->NB; ib++)
         bs32 = A->bsize[ib] == 32 && B->bsize[ib] == 32;
-    const int grid = bs32 ? eb_grid<T>(c, A->NB, 4) : eb_grid<T>(c, A->NB, 2);
-    const int cap = C->MB + 1 < 1024 ? C->MB + 1 : 1024;
-    const size_t slab = (size_t) grid * cap * A->slot_elems * sizeof(T);
-    const size_t marks = (size_t) grid * B->NB * sizeof(int);
-    const size_t diag = (size_t) 2 * A->NB * sizeof(double);
-    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(slab + marks + diag + 1024));
-    if (!scr)
-        return false;
-    T *dslab = reinterpret_cast<T *>(scr);
-    int *dmarks = reinterpret_cast<int *>(scr + slab);
-    double *dA = reinterpret_cast<double *>(scr + ((slab + marks + 255) & ~size_t(255)));
-    double *dC = dA + A->NB;
-    int *flags = eb_flags(c);
-    if (!flags || !CUDA_OK(cudaMemsetAsync(dmarks, 0, marks, c->stream)))
-        return false;
-    if (bs32)
+    const int grid0 = bs32 ? eb_grid<T>(c, A->NB, 4) : eb_grid<T>(c, A->NB, 2);
+    const size_t slot_bytes = (size_t) A->slot_elems * sizeof(T);
+    // Accumulator slots per CTA: first room for the output's width plus one
+    // (which detects a wider row); a row that touches more block columns
+    // before thresholding makes the call run again with room for all NB.
+    // The slabs stay within about 24 GB (fewer CTAs when NB is large).
+    const size_t budget = size_t(24) << 30;
+    int cap = C->MB + 1 < B->NB ? C->MB + 1 : B->NB;
+    int hf[8];
+    for (int attempt = 0; attempt < 2; ++attempt)
     {
-        const size_t smem = sizeof(EbS32<T>);
-        auto k = eb_mul32_kernel<T>;
-        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+        const size_t per_cta = (size_t) cap * (slot_bytes + sizeof(int)) + (size_t) B->NB * sizeof(int);
+        const int grid = (int) std::max<size_t>(1, std::min<size_t>((size_t) grid0, budget / per_cta));
+        const size_t slab = (size_t) grid * cap * slot_bytes;
+        const size_t lists = (size_t) grid * cap * sizeof(int);
+        const size_t marks = (size_t) grid * B->NB * sizeof(int);
+        const size_t diag = (size_t) 2 * A->NB * sizeof(double);
+        unsigned char *scr = static_cast<unsigned char *>(b200_scratch(slab + lists + marks + diag + 1024));
+        if (!scr)
             return false;
-        k<<<grid, EB32_THREADS, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0,
-                                                   dslab, dmarks, trace ? dA : nullptr, trace ? dC : nullptr, flags);
-        if (!LAUNCH_OK("eb_mul32_kernel"))
+        T *dslab = reinterpret_cast<T *>(scr);
+        int *dlists = reinterpret_cast<int *>(scr + slab);
+        int *dmarks = dlists + (size_t) grid * cap;
+        double *dA = reinterpret_cast<double *>(scr + ((slab + lists + marks + 255) & ~size_t(255)));
+        double *dC = dA + A->NB;
+        int *flags = eb_flags(c);
+        if (!flags || !CUDA_OK(cudaMemsetAsync(dmarks, 0, marks, c->stream)))
             return false;
+        if (bs32)
+        {
+            const size_t smem = sizeof(EbS32<T>);
+            auto k = eb_mul32_kernel<T>;
+            if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+                return false;
+            k<<<grid, EB32_THREADS, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0,
+                                                       cap, dslab, dlists, dmarks, trace ? dA : nullptr,
+                                                       trace ? dC : nullptr, flags);
+            if (!LAUNCH_OK("eb_mul32_kernel"))
+                return false;
+        }
+        else
+        {
+            const size_t smem = 2 * slot_bytes;
+            auto k = eb_mul_kernel<T>;
+            if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+                return false;
+            k<<<grid, 256, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0, cap,
+                                             dslab, dlists, dmarks, trace ? dA : nullptr, trace ? dC : nullptr,
+                                             flags);
+            if (!LAUNCH_OK("eb_mul_kernel"))
+                return false;
+        }
+        if (trace)
+        {
+            // the traces, summed over block rows, land after the flags
+            double *out = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(flags) + 64);
+            b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(dA, dC, A->NB, out);
+            if (!LAUNCH_OK("b200_sum_rows_kernel"))
+                return false;
+        }
+        unsigned char *pin = static_cast<unsigned char *>(c->pinned) + 4096;
+        if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 64 + 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+            return false;
+        memcpy(hf, pin, sizeof(hf));
+        if (trace)
+            memcpy(trace, pin + 64, 2 * sizeof(double));
+        if (hf[4] && !hf[2] && cap < B->NB)
+        {
+            cap = B->NB;
+            continue;
+        }
+        break;
     }
-    else
-    {
-        const size_t smem = 2 * (size_t) A->slot_elems * sizeof(T) + 1024 * sizeof(int);
-        auto k = eb_mul_kernel<T>;
-        if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
-            return false;
-        k<<<grid, 256, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0, dslab,
-                                         dmarks, trace ? dA : nullptr, trace ? dC : nullptr, flags);
-        if (!LAUNCH_OK("eb_mul_kernel"))
-            return false;
-    }
-    if (trace)
-    {
-        double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 64);
-        b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(dA, dC, A->NB, out);
-        if (!LAUNCH_OK("b200_sum_rows_kernel"))
-            return false;
-    }
-    int hf[2 + 4];
-    int *pin = reinterpret_cast<int *>(static_cast<unsigned char *>(c->pinned) + 4096);
-    if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 64 + 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
-        return false;
-    memcpy(hf, pin, sizeof(int) * 3);
     eb_mark_device(C);
-    if (trace)
-    {
-        const double *t = reinterpret_cast<const double *>(reinterpret_cast<unsigned char *>(pin) + 64);
-        trace[0] = t[0];
-        trace[1] = t[1];
-    }
     if (hf[2])
     {
         b200_set_error(BML_B200_ERR_TIMEOUT, "ELLBLOCK multiply: a block copy did not complete");

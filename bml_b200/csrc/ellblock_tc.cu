@@ -1081,16 +1081,22 @@ extern "C" int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, dou
         const bool closing = it >= maxiter - nclose;
         double tr[2];
         const auto t0 = std::chrono::steady_clock::now();
-        bool ok;
-        if (closing)
+        bool ok = false, on_tc = false;
+        if (!closing)
+        {
+            ok = on_tc = eb_multiply_x2_tc(static_cast<bml_matrix_ellblock_t *>(D),
+                                           static_cast<bml_matrix_ellblock_t *>(X2), threshold, tr);
+            // blocks other than 32 x 32, or a group beyond the tensor-core
+            // kernel's capacities: this iteration on the exact product
+            if (!on_tc && b200_get_error() == BML_B200_ERR_UNSUPPORTED)
+                bml_b200_clear_error();
+        }
+        if (closing || (!on_tc && !bml_b200_last_error()))
             ok = eb_multiply_x2(static_cast<bml_matrix_ellblock_t *>(D), static_cast<bml_matrix_ellblock_t *>(X2),
                                 threshold, tr);
-        else
-            ok = eb_multiply_x2_tc(static_cast<bml_matrix_ellblock_t *>(D),
-                                   static_cast<bml_matrix_ellblock_t *>(X2), threshold, tr);
         const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         x2s += dt;
-        if (!closing)
+        if (on_tc)
         {
             x2s_tc += dt;
             ++it_tc;

@@ -394,8 +394,11 @@ BML_B200_API int bml_b200_ellblock_multiply_x2_tc(bml_matrix_t *X, bml_matrix_t 
 /* SP2 on ELLBLOCK matrices in mixed precision (no reference counterpart):
  * bulk iterations use bml_b200_ellblock_multiply_x2_tc, the last nclose
  * iterations the matrix-precision X^2 of bml_multiply_x2; adds, copies, the
- * branch choice and the stop tests as bml_b200_sp2.  info as for
- * bml_b200_sp2_mixed ([4] is 0). */
+ * branch choice and the stop tests as bml_b200_sp2.  A bulk iteration that
+ * the tensor-core X^2 rejects as UNSUPPORTED (blocks other than 32 x 32, or
+ * four block rows together beyond its capacities) runs on the exact X^2.
+ * info as for bml_b200_sp2_mixed ([4] is 0; [6] and [7] count the
+ * iterations that ran on the tensor cores). */
 BML_B200_API int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold,
     double occupation, int maxiter, double tol, int stall, int nclose, double *info);
 

@@ -21,12 +21,13 @@ ELLBLOCK, DOUBLE, SINGLE = 3, 2, 1
 BS = 32
 
 
-def block_lattice(L, radius, seed=0):
-    """Dense symmetric matrix of L^3 blocks of 32 x 32: block (a, b) nonzero
+def block_lattice(L, radius, seed=0, bs=BS):
+    """Dense symmetric matrix of L^3 blocks of bs x bs: block (a, b) nonzero
     when the block sites are within `radius`, entries N(0,1) exp(-d)."""
     rng = np.random.default_rng(seed)
     nb = L ** 3
     pos = np.array([(x, y, z) for z in range(L) for y in range(L) for x in range(L)])
+    BS = bs
     H = np.zeros((nb * BS, nb * BS))
     for a in range(nb):
         for b in range(a, nb):
@@ -40,10 +41,10 @@ def block_lattice(L, radius, seed=0):
     return H
 
 
-def set_partition(nb):
-    arr = (C.c_int * nb)(*([BS] * nb))
+def set_partition(nb, MB=None, bs=BS):
+    arr = (C.c_int * nb)(*([bs] * nb))
     B.lib.bml_b200_reset_block_sizes()
-    B.lib.bml_set_block_sizes(arr, nb, nb)
+    B.lib.bml_set_block_sizes(arr, nb, MB or nb)
 
 
 def dt(prec):
@@ -166,3 +167,51 @@ def test_multiply_ab_blocks32_bit_exact(oracle_mod):
     assert same_bits(got, np.ascontiguousarray(d2[:N, N:]))
     want = [[k - nb for k in r] for r in rows(oix, onz, 2 * nb)[:nb]]
     assert gc == want
+
+
+@pytest.mark.parametrize("bs", [32, 4])
+def test_x2_more_block_columns_than_mb_before_threshold(oracle_mod, bs):
+    """Rows of X^2 that touch more block columns than the output's MB before
+    thresholding, but keep at most MB: the call runs again with room for
+    every block column (the reference's accumulator spans all NB) and gives
+    the restatement's blocks and lists."""
+    O = oracle_mod
+    L, MB = 3, 12
+    nb = L ** 3
+    N = nb * bs
+    H = block_lattice(L, 1.0, seed=4, bs=bs)
+    # a threshold that leaves at most MB blocks in every row of X^2
+    d2, _, w, _, _ = O.rest_ellblock_x2([bs] * nb, *full_lists(H, nb, bs), H, 0.0, nb, lists=True)
+    assert w > MB + 1  # wider than the first attempt's room before thresholding
+    thr = 0.0
+    for ib in range(nb):
+        norms = sorted((np.abs(d2[ib * bs:(ib + 1) * bs, kb * bs:(kb + 1) * bs]).max()
+                        for kb in range(nb) if kb != ib), reverse=True)
+        thr = max(thr, norms[MB - 2])
+    set_partition(nb, MB, bs)
+    try:
+        X = from_dense(H, DOUBLE)
+        X2 = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+        B.check()
+        B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(X, X2, C.c_double(thr))))
+        B.check()
+        ix, nz, xMB = lists(O, X)
+        r2, _, _, oix, onz = O.rest_ellblock_x2([bs] * nb, ix, nz, xMB, H, thr, MB, lists=True)
+        assert int(onz.max()) <= MB
+        assert same_bits(to_dense(X2, N, DOUBLE), r2)
+        gix, gnz, gMB = lists(O, X2)
+        assert rows(gix, gnz, gMB) == rows(oix, onz, MB)
+        free(X, X2)
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
+
+
+def full_lists(H, nb, bs):
+    """Block lists (ascending) of the nonzero blocks of H, with MB = nb."""
+    indexb = np.zeros(nb * nb, np.int32)
+    nnzb = np.zeros(nb, np.int32)
+    for ib in range(nb):
+        cols = [jb for jb in range(nb) if np.any(H[ib * bs:(ib + 1) * bs, jb * bs:(jb + 1) * bs])]
+        indexb[ib * nb:ib * nb + len(cols)] = cols
+        nnzb[ib] = len(cols)
+    return indexb, nnzb, nb
