@@ -254,6 +254,7 @@ def run_b200(args, rank, world, local):
     # without the sharded solve
     mixed = mixed_leg(B, v, ix, nz, max(3, min(args.steps, 5))) if world == 1 else None
     ellb = None if (args.no_ellblock or world > 1) else ellblock_leg()
+    ellb_sp2 = None if (args.no_ellblock or world > 1) else ellblock_sp2_leg()
     res = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms, "higher_is_better": False,
@@ -273,6 +274,7 @@ def run_b200(args, rank, world, local):
                 "x2_seconds_per_run": x2_seconds_per_run},
         "mixed": mixed,
         "ellblock_tc": ellb,
+        "ellblock_sp2": ellb_sp2,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res["cpu_baseline"] = cpu_baseline()
@@ -609,6 +611,42 @@ def run_profile_eb():
         B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(H, X2, C.c_double(1e-6))))
         B.check()
     print(json.dumps({"profile_case": "10^3 block lattice, exact FP64 X^2", "trace": B.lib.bml_trace(X2)}))
+
+
+def ellblock_sp2_leg(iters=5, nclose=2):
+    """The mixed ELLBLOCK SP2 configuration on the 16^3 block lattice (4096
+    block rows of 32, N = 131072, threshold 1e-6, occupation N/2): the first
+    `iters` iterations from X0, every X^2 exact (FP64) against bulk X^2 on the
+    tensor cores and the last `nclose` exact, with their errors.  Device time
+    by CUDA events on the library stream."""
+    import bml_b200 as B
+    H, n = ellblock_case(16)
+    out = {}
+    for name, nc in (("fp64", iters), ("mixed", nclose)):
+        D = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+        B.check()
+        info = (C.c_double * 8)()
+        with _StdoutToStderr():
+            B.check(B.lib.bml_b200_synchronize())
+            B.check(B.lib.bml_b200_event_record(6))
+            B.check(B.lib.bml_b200_ellblock_sp2_mixed(H, D, 1e-6, n / 2.0, iters, -1.0, 0, nc, info))
+            B.check(B.lib.bml_b200_event_record(7))
+        t = B.event_ms(6, 7) / 1e3
+        out[name] = {"s": t, "trace": B.lib.bml_trace(D), "energy_trDH": B.lib.bml_trace_mult(D, H),
+                     "idempotency_t_minus_t2": info[3], "tc_iterations": int(info[6]), "nnz": int(B.lib.bml_b200_nnz(D))}
+        hh = C.c_void_p(D)
+        B.lib.bml_deallocate(C.byref(hh))
+    hh = C.c_void_p(H)
+    B.lib.bml_deallocate(C.byref(hh))
+    B.lib.bml_b200_reset_block_sizes()
+    e, m = out["fp64"], out["mixed"]
+    return {"workload": "SP2 on the 16^3 block lattice Hamiltonian (4096 block rows of 32x32, N=131072, radius 2, "
+                        "thr 1e-6, occ N/2), first %d iterations from X0" % iters,
+            "iterations": iters, "closing_fp64": nclose, "fp64": e, "mixed": m, "speedup": e["s"] / m["s"],
+            "trace_rel_err": abs(m["trace"] - e["trace"]) / abs(e["trace"]),
+            "energy_rel_err": abs(m["energy_trDH"] - e["energy_trDH"]) / abs(e["energy_trDH"]),
+            "note": "bulk X^2 run on the tensor cores where a group of four block rows fits the kernel's "
+                    "capacities (here only X0^2); wider iterates run on the exact FP64 product"}
 
 
 def ellblock_leg(reps=3):

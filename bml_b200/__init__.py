@@ -122,6 +122,7 @@ _PROTOS = {
     "bml_b200_reset_block_sizes": (None, []),
     "bml_b200_last_tier_counts": (_i, [_ip, _i]),
     "bml_b200_set_x2_tiers": (_i, [_i]),
+    "bml_b200_set_ellblock_slab_budget": (C.c_longlong, [C.c_longlong]),
     "bml_b200_set_device": (_i, [_i]),
     "bml_b200_launch_count": (C.c_ulonglong, []),
     "bml_b200_event_record": (_i, [_i]),

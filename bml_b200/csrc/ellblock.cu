@@ -949,7 +949,7 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
     const int maxbs = (int) sqrtf((float) A.slot + 0.5f);
     T *sL = reinterpret_cast<T *>(smem);
     T *sR = sL + (size_t) maxbs * maxbs;
-    __shared__ int lb, firstflag, slotq;
+    __shared__ int lb, firstflag, slotq, stopflag;
     __shared__ double red[32];
     // cap slab slots and list entries per CTA (first-touch order)
     T *myslab = slab + (size_t) blockIdx.x * cap * A.slot;
@@ -957,9 +957,15 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
     int *mark = marks + (size_t) blockIdx.x * B.NB;
     for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
     {
+        // (no further rows once a row has outgrown the slots: the call runs again)
         if (threadIdx.x == 0)
+        {
             lb = 0;
+            stopflag = *reinterpret_cast<volatile int *>(&flags[4]);
+        }
         __syncthreads();
+        if (stopflag)
+            break;
         T trA = T(0);
         const int bi = A.bsize[ib];
         for (int jp = 0; jp < A.nnzb[ib]; ++jp)
@@ -988,6 +994,8 @@ __global__ void __launch_bounds__(256) eb_mul_kernel(EbView<T> A, EbView<T> B, E
                             list[lb] = kb;
                         mark[kb] = lb + 1;
                         lb++;
+                        if (lb > cap)
+                            atomicExch(&flags[4], 1);
                     }
                     else
                     {
@@ -1200,8 +1208,9 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
     {
         // block rows are claimed from a counter (rows differ in cost), by
         // one thread for the whole CTA
+        // (none once a row has outgrown the slots: the call runs again)
         if (tid == 0)
-            S.row = atomicAdd(&flags[3], 1);
+            S.row = *reinterpret_cast<volatile int *>(&flags[4]) ? A.NB : atomicAdd(&flags[3], 1);
         __syncthreads();
         const int ib = S.row;
         if (ib >= A.NB)
@@ -1303,6 +1312,8 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
                     if (q < ns)
                         S.slotq[q] = isnew ? -(sl + 1) : sl;
                     lb += tot;
+                    if (tid == 0 && lb > cap)
+                        atomicExch(&flags[4], 1);
                     __syncthreads();
                 }
                 // this lane's row of the left block
@@ -1466,6 +1477,9 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
 
 template <typename T> int eb_grid(B200Context *c, int NB, int per_sm) { return max(1, min(NB, c->sm_count * per_sm)); }
 
+constexpr long long EB_SLAB_BUDGET_DEFAULT = 24ll << 30;
+long long g_eb_slab_budget = EB_SLAB_BUDGET_DEFAULT;
+
 int *eb_flags(B200Context *c)
 {
     int *f = reinterpret_cast<int *>(static_cast<unsigned char *>(c->d_small) + 4096);
@@ -1518,17 +1532,21 @@ bool eb_multiply_typed(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_m
         bs32 = A->bsize[ib] == 32 && B->bsize[ib] == 32;
     const int grid0 = bs32 ? eb_grid<T>(c, A->NB, 4) : eb_grid<T>(c, A->NB, 2);
     const size_t slot_bytes = (size_t) A->slot_elems * sizeof(T);
-    // Accumulator slots per CTA: first room for the output's width plus one
-    // (which detects a wider row); a row that touches more block columns
-    // before thresholding makes the call run again with room for all NB.
-    // The slabs stay within about 24 GB (fewer CTAs when NB is large).
-    const size_t budget = size_t(24) << 30;
-    int cap = C->MB + 1 < B->NB ? C->MB + 1 : B->NB;
+    // Accumulator slots per CTA: room for all NB block columns (the
+    // reference's accumulator) when the slabs of a full grid fit the budget
+    // (bml_b200_set_ellblock_slab_budget, 24 GiB by default); otherwise first room for the output's width plus one, and a row
+    // that touches more block columns before thresholding stops the launch
+    // early and makes the call run again with room for all NB (on fewer CTAs
+    // if need be).
+    const size_t budget = (size_t) g_eb_slab_budget;
+    const auto per_cta = [&](int cp) {
+        return (size_t) cp * (slot_bytes + sizeof(int)) + (size_t) B->NB * sizeof(int);
+    };
+    int cap = (size_t) grid0 * per_cta(B->NB) <= budget ? B->NB : std::min(C->MB + 1, B->NB);
     int hf[8];
     for (int attempt = 0; attempt < 2; ++attempt)
     {
-        const size_t per_cta = (size_t) cap * (slot_bytes + sizeof(int)) + (size_t) B->NB * sizeof(int);
-        const int grid = (int) std::max<size_t>(1, std::min<size_t>((size_t) grid0, budget / per_cta));
+        const int grid = (int) std::max<size_t>(1, std::min<size_t>((size_t) grid0, budget / per_cta(cap)));
         const size_t slab = (size_t) grid * cap * slot_bytes;
         const size_t lists = (size_t) grid * cap * sizeof(int);
         const size_t marks = (size_t) grid * B->NB * sizeof(int);
@@ -2127,6 +2145,13 @@ template <typename T> void fill_block_lattice(bml_matrix_ellblock_t *A, int L, d
 }
 
 } // namespace
+
+extern "C" BML_B200_API long long bml_b200_set_ellblock_slab_budget(long long bytes)
+{
+    const long long old = g_eb_slab_budget;
+    g_eb_slab_budget = bytes > 0 ? bytes : EB_SLAB_BUDGET_DEFAULT;
+    return old;
+}
 
 extern "C" bml_matrix_t *bml_b200_gen_block_lattice(int L, double radius, int bs, unsigned long long seed,
                                                     bml_matrix_precision_t prec)

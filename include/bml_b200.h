@@ -301,6 +301,15 @@ BML_B200_API int bml_b200_last_tier_counts(int *counts, int n);
  * last multiply.  Returns the previous mask.  No reference counterpart. */
 BML_B200_API int bml_b200_set_x2_tiers(int mask);
 
+/* Device-memory budget, in bytes, for the accumulator slabs of the exact
+ * ELLBLOCK products (bml_multiply_x2, bml_multiply_AB, bml_multiply): every
+ * CTA holds a slot for each block column a row can touch, NB of them, when
+ * that fits the budget; otherwise it first holds MB + 1 slots and a call
+ * whose rows touch more runs again with NB slots on fewer CTAs.  0 restores
+ * the default of 24 GiB.  Results do not depend on it.  Returns the previous
+ * budget.  No reference counterpart. */
+BML_B200_API long long bml_b200_set_ellblock_slab_budget(long long bytes);
+
 /* Raw ELLPACK transfer between the device matrix and caller host arrays laid
  * out like the reference (row-major value[N*M], index[N*M], nnz[N]).  Only
  * the columns up to the widest row are transferred: entries past a row's nnz

@@ -169,12 +169,15 @@ def test_multiply_ab_blocks32_bit_exact(oracle_mod):
     assert gc == want
 
 
+@pytest.mark.parametrize("budget", [0, 1 << 16])
 @pytest.mark.parametrize("bs", [32, 4])
-def test_x2_more_block_columns_than_mb_before_threshold(oracle_mod, bs):
+def test_x2_more_block_columns_than_mb_before_threshold(oracle_mod, bs, budget):
     """Rows of X^2 that touch more block columns than the output's MB before
-    thresholding, but keep at most MB: the call runs again with room for
-    every block column (the reference's accumulator spans all NB) and gives
-    the restatement's blocks and lists."""
+    thresholding, but keep at most MB (the reference's accumulator spans all
+    NB): with the default slab budget every CTA has room for all NB at once;
+    with a 64 KiB budget the first launch has MB + 1 slots, stops early, and
+    the call runs again with NB slots on fewer CTAs.  Both give the
+    restatement's blocks and lists."""
     O = oracle_mod
     L, MB = 3, 12
     nb = L ** 3
@@ -189,6 +192,7 @@ def test_x2_more_block_columns_than_mb_before_threshold(oracle_mod, bs):
                         for kb in range(nb) if kb != ib), reverse=True)
         thr = max(thr, norms[MB - 2])
     set_partition(nb, MB, bs)
+    old_budget = B.lib.bml_b200_set_ellblock_slab_budget(budget)
     try:
         X = from_dense(H, DOUBLE)
         X2 = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
@@ -203,6 +207,7 @@ def test_x2_more_block_columns_than_mb_before_threshold(oracle_mod, bs):
         assert rows(gix, gnz, gMB) == rows(oix, onz, MB)
         free(X, X2)
     finally:
+        B.lib.bml_b200_set_ellblock_slab_budget(old_budget)
         B.lib.bml_b200_reset_block_sizes()
 
 
