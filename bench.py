@@ -621,6 +621,13 @@ def ellblock_sp2_leg(iters=5, nclose=2):
     by CUDA events on the library stream."""
     import bml_b200 as B
     H, n = ellblock_case(16)
+    # warm-up: the exact and tensor-core X^2 size their device scratch once
+    W = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    B.check()
+    B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(H, W, C.c_double(1e-6))))
+    B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, W, 1e-6, None))
+    hh = C.c_void_p(W)
+    B.lib.bml_deallocate(C.byref(hh))
     out = {}
     for name, nc in (("fp64", iters), ("mixed", nclose)):
         D = B.lib.bml_zero_matrix(3, 2, n, n, 0)
