@@ -182,8 +182,13 @@ bool eb_to_device(bml_matrix_ellblock_t *A)
     if (!c)
         return false;
     const size_t sz = prec_size(A->matrix_precision);
-    if (!CUDA_OK(cudaMemcpyAsync(A->d_pool, A->h_pool, eb_pool_elems(A) * sz, cudaMemcpyHostToDevice,
-                                 c->stream)) ||
+    // only the first w slots of every block row, w the widest row
+    int w = 0;
+    for (int ib = 0; ib < A->NB; ib++)
+        w = A->nnzb[ib] > w ? A->nnzb[ib] : w;
+    const size_t slot = (size_t) A->slot_elems * sz, pitch = slot * A->MB;
+    if ((w > 0 && !CUDA_OK(cudaMemcpy2DAsync(A->d_pool, pitch, A->h_pool, pitch, slot * w, A->NB,
+                                             cudaMemcpyHostToDevice, c->stream))) ||
         !CUDA_OK(cudaMemcpyAsync(A->d_indexb, A->indexb, sizeof(int) * (size_t) A->NB * A->MB,
                                  cudaMemcpyHostToDevice, c->stream)) ||
         !CUDA_OK(cudaMemcpyAsync(A->d_nnzb, A->nnzb, sizeof(int) * A->NB, cudaMemcpyHostToDevice,
@@ -202,12 +207,19 @@ bool eb_to_host(bml_matrix_ellblock_t *A)
     if (!c)
         return false;
     const size_t sz = prec_size(A->matrix_precision);
-    if (!CUDA_OK(cudaMemcpyAsync(A->h_pool, A->d_pool, eb_pool_elems(A) * sz, cudaMemcpyDeviceToHost,
+    // the row widths first, then only the first w slots of every block row
+    if (!CUDA_OK(cudaMemcpyAsync(A->nnzb, A->d_nnzb, sizeof(int) * A->NB, cudaMemcpyDeviceToHost,
                                  c->stream)) ||
+        !b200_sync())
+        return false;
+    int w = 0;
+    for (int ib = 0; ib < A->NB; ib++)
+        w = A->nnzb[ib] > w ? A->nnzb[ib] : w;
+    const size_t slot = (size_t) A->slot_elems * sz, pitch = slot * A->MB;
+    if ((w > 0 && !CUDA_OK(cudaMemcpy2DAsync(A->h_pool, pitch, A->d_pool, pitch, slot * w, A->NB,
+                                             cudaMemcpyDeviceToHost, c->stream))) ||
         !CUDA_OK(cudaMemcpyAsync(A->indexb, A->d_indexb, sizeof(int) * (size_t) A->NB * A->MB,
                                  cudaMemcpyDeviceToHost, c->stream)) ||
-        !CUDA_OK(cudaMemcpyAsync(A->nnzb, A->d_nnzb, sizeof(int) * A->NB, cudaMemcpyDeviceToHost,
-                                 c->stream)) ||
         !b200_sync())
         return false;
     host_pointers(A);
