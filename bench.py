@@ -328,7 +328,16 @@ def mixed_leg(B, v, ix, nz, reps):
            "density_rel_fro_err": dist / n64,
            "idempotency_fro": {"fp64": idem(D64), "mixed": idem(Dm)},
            "target": "mixed >= 2x faster than FP64 at <= 1e-6 relative trace/energy error"}
-    for m in (Hp, D64, Dm, T):
+    # the same with one FP32 iteration and the rest in FP64
+    D1, i1 = B.Ellpack(N, M_X), (C.c_double * 8)()
+    t1 = timed(lambda: B.check(B.lib.bml_b200_sp2_mixed(Hp.h, D1.h, THRESHOLD, OCC, SP2_ITERS, 1e-8, 0,
+                                                        SP2_ITERS - 1, i1)), reps)
+    e1 = B.lib.bml_trace_mult(D1.h, Hp.h)
+    res["one_fp32_iteration"] = {"value": t1, "speedup_vs_fp64": t64 / t1, "fp32_iterations": int(i1[6]),
+                                 "trace_rel_err": abs(i1[2] - i64[2]) / abs(i64[2]),
+                                 "energy_trDH_rel_err": abs(e1 - e64) / abs(e64),
+                                 "density_rel_fro_err": B.lib.bml_fnorm2(D1.h, D64.h) / n64}
+    for m in (Hp, D64, Dm, D1, T):
         m.free()
     return res
 
