@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-tc", action="store_true",
                     help="run the small tensor-core ELLBLOCK case for an ncu capture (10^3 block lattice)")
+    ap.add_argument("--profile-eb-ops", action="store_true",
+                    help="the one-pass ELLBLOCK operations, once each, for an ncu capture (7^3 block lattice)")
+    ap.add_argument("--eb-ops-L", type=int, default=7, help="block lattice side for --profile-eb-ops")
     ap.add_argument("--profile-eb", action="store_true",
                     help="run the small exact ELLBLOCK case for an ncu capture (10^3 block lattice)")
     ap.add_argument("--no-ellblock", action="store_true", help="skip the ELLBLOCK tensor-core leg")
@@ -622,6 +625,46 @@ def run_profile_eb():
     print(json.dumps({"profile_case": "10^3 block lattice, exact FP64 X^2", "trace": B.lib.bml_trace(X2)}))
 
 
+def run_profile_eb_ops(L=7):
+    """The one-pass ELLBLOCK operations, each launched once, on the L^3 block
+    lattice (radius 2, MB = 257; L = 7: 343 block rows of 32x32, N = 10976):
+    H, and X2 = H^2 (exact, threshold 1e-6), at L = 7 about 280 MB of blocks,
+    larger than L2.  Prints the block counts from which each operation's
+    compulsory bytes follow."""
+    import bml_b200 as B
+    H, n = ellblock_case(L)
+    X2 = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    S = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    T = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+    B.check()
+    B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(H, X2, C.c_double(1e-6))))
+    B.check()
+    blocks = lambda h: int(B.lib.bml_b200_nnz(h)) // 1024
+    n_h, n_x2 = blocks(H), blocks(X2)
+    # the operations, in launch order
+    B.lib.bml_copy(X2, S)                                   # eb_copy_kernel: X2 -> S
+    B.lib.bml_add(S, H, C.c_double(2.0), C.c_double(-1.0), C.c_double(1e-6))  # eb_add_kernel: S = 2 S - H
+    n_add = blocks(S)
+    B.lib.bml_copy(X2, T)                                   # eb_copy_kernel: X2 -> T
+    B.lib.bml_threshold(T, C.c_double(1e-1))                # eb_threshold_kernel, in place
+    n_thr = blocks(T)
+    alpha = C.c_double(0.5)
+    B.lib.bml_scale_inplace(C.byref(alpha), X2)             # eb_scale_kernel on X2
+    trace = B.lib.bml_trace(X2)                             # eb_diag_kernel
+    eb = B.lib.bml_gershgorin(X2)                           # eb_gersh_kernel
+    B.lib.bml_free_memory(eb)
+    Xt = B.lib.bml_transpose_new(X2)                        # eb_transpose_kernel
+    tm = B.lib.bml_trace_mult(X2, H)                        # eb_trace_mult_kernel
+    B.check()
+    for h in (X2, S, T, Xt, H):
+        hh = C.c_void_p(h)
+        B.lib.bml_deallocate(C.byref(hh))
+    B.lib.bml_b200_reset_block_sizes()
+    print(json.dumps({"profile_case": "one-pass ELLBLOCK operations on the %d^3 block lattice's H and H^2" % L,
+                      "N": n, "blocks_h": n_h, "blocks_x2": n_x2, "blocks_add": n_add, "blocks_threshold": n_thr,
+                      "trace": trace, "trace_mult": tm}))
+
+
 def ellblock_sp2_leg(iters=5, nclose=2):
     """The mixed ELLBLOCK SP2 configuration on the 16^3 block lattice (4096
     block rows of 32, N = 131072, threshold 1e-6, occupation N/2): the first
@@ -735,6 +778,9 @@ def main():
         return
     if args.profile_eb:
         run_profile_eb()
+        return
+    if args.profile_eb_ops:
+        run_profile_eb_ops(args.eb_ops_L)
         return
     if args.impl == "reference":
         res = run_reference(args, rank, world)

@@ -814,56 +814,73 @@ template <typename T> __global__ void eb_gersh_kernel(EbView<T> A, double *hi, d
 // transpose: block (ib, jb) -> (jb, ib) transposed, appended to block row jb
 // in ascending ib (the serial order of ellblock/bml_transpose_ellblock_typed.c:
 // 29-70).  One thread per destination block row gathers its blocks in order.
-template <typename T> __global__ void eb_transpose_kernel(EbView<T> A, EbView<T> B, int *overflow)
+// Transpose, in two passes.  Block row jb of B = A^T lists the blocks
+// (ib, jb) of A in ascending ib, the order of the reference's loop over
+// block rows (ellblock/bml_transpose_ellblock_typed.c:29-70).
+// Pass 1: every block (ib, jp) of A takes a slot in its target row jb
+// (atomic count) and records its source there (ib*MB + jp).
+__global__ void eb_tr_scatter_kernel(const int *indexb, const int *nnzb, int NB, int MBa, int MBb, int *cnt,
+                                     int *src, int *overflow)
 {
+    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < (long long) NB * MBa;
+         e += (long long) gridDim.x * blockDim.x)
+    {
+        const int ib = (int) (e / MBa), jp = (int) (e % MBa);
+        if (jp >= nnzb[ib])
+            continue;
+        const int jb = indexb[e];
+        const int slot = atomicAdd(&cnt[jb], 1);
+        if (slot < MBb)
+            src[(size_t) jb * MBb + slot] = (int) e;
+        else
+            atomicExch(overflow, 1);
+    }
+}
+
+// Pass 2: one CTA per row jb of B ranks its sources by ib (they are
+// distinct) and writes each block transposed at its rank, through a padded
+// shared-memory tile.
+// Shared memory: ids[MBb] (source slots) | rank[MBb] | tile[maxbs][maxbs+1]
+template <typename T> __global__ void eb_tr_place_kernel(EbView<T> A, EbView<T> B, const int *cnt, const int *src)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int maxbs = (int) sqrtf((float) A.slot + 0.5f);
+    int *ids = reinterpret_cast<int *>(smem);
+    int *rank = ids + B.MB;
+    T *tile = reinterpret_cast<T *>(smem + (((size_t) 2 * B.MB * sizeof(int) + 15) & ~size_t(15)));
+    const int ld = maxbs + 1;
     for (int jb = blockIdx.x; jb < A.NB; jb += gridDim.x)
     {
-        __shared__ int n;
-        if (threadIdx.x == 0)
-            n = 0;
+        const int n = min(cnt[jb], B.MB);
+        for (int q = threadIdx.x; q < n; q += blockDim.x)
+            ids[q] = src[(size_t) jb * B.MB + q];
         __syncthreads();
-        for (int ib = 0; ib < A.NB; ++ib)
+        for (int q = threadIdx.x; q < n; q += blockDim.x)
         {
-            __shared__ int found;
-            if (threadIdx.x == 0)
-            {
-                found = -1;
-                for (int jp = 0; jp < A.nnzb[ib]; ++jp)
-                    if (A.indexb[(size_t) ib * A.MB + jp] == jb)
-                    {
-                        found = jp;
-                        break;
-                    }
-            }
+            const int ib = ids[q] / A.MB;
+            int r = 0;
+            for (int u = 0; u < n; ++u)
+                r += ids[u] / A.MB < ib;
+            rank[q] = r;
+        }
+        __syncthreads();
+        const int bj = A.bsize[jb];
+        for (int q = 0; q < n; ++q)
+        {
+            const int e = ids[q], ib = e / A.MB, bi = A.bsize[ib];
+            const T *a = A.pool + (size_t) e * A.slot; // block (ib, jp): bi x bj, row-major
+            for (int x = threadIdx.x; x < bi * bj; x += blockDim.x)
+                tile[(x / bj) * ld + x % bj] = a[x];
             __syncthreads();
-            if (found >= 0)
-            {
-                if (n >= B.MB)
-                {
-                    if (threadIdx.x == 0)
-                        atomicExch(overflow, 1);
-                }
-                else
-                {
-                    const int bi = A.bsize[ib], bj = A.bsize[jb];
-                    const T *a = A.blk(ib, found);
-                    T *b = B.blk(jb, n);
-                    for (int e = threadIdx.x; e < bi * bj; e += blockDim.x)
-                    {
-                        const int ii = e / bj, jj = e % bj;
-                        b[jj * bi + ii] = a[e];
-                    }
-                    if (threadIdx.x == 0)
-                        B.indexb[(size_t) jb * B.MB + n] = ib;
-                }
-                __syncthreads();
-                if (threadIdx.x == 0)
-                    n++;
-            }
+            T *b = B.blk(jb, rank[q]); // bj x bi, row-major
+            for (int x = threadIdx.x; x < bi * bj; x += blockDim.x)
+                b[x] = tile[(x % bi) * ld + x / bi];
+            if (threadIdx.x == 0)
+                B.indexb[(size_t) jb * B.MB + rank[q]] = ib;
             __syncthreads();
         }
         if (threadIdx.x == 0)
-            B.nnzb[jb] = n < B.MB ? n : B.MB;
+            B.nnzb[jb] = n;
         __syncthreads();
     }
 }
@@ -1890,13 +1907,43 @@ bml_matrix_ellblock_t *eb_transpose_new(bml_matrix_ellblock_t *A)
         eb_free(B);
         return nullptr;
     }
+    const size_t smem = (((size_t) 2 * B->MB * sizeof(int) + 15) & ~size_t(15)) +
+                        (size_t) A->maxbs * (A->maxbs + 1) * prec_size(A->matrix_precision);
+    if (smem > (size_t) c->smem_optin)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "ELLBLOCK transpose: MB=%d too large", B->MB);
+        eb_free(B);
+        return nullptr;
+    }
+    // per row of B: a count and the source slot of every block
+    int *cnt = static_cast<int *>(b200_scratch((size_t) A->NB * (1 + (size_t) B->MB) * sizeof(int)));
+    if (!cnt || !CUDA_OK(cudaMemsetAsync(cnt, 0, sizeof(int) * A->NB, c->stream)))
+    {
+        eb_free(B);
+        return nullptr;
+    }
+    int *src = cnt + A->NB;
+    const long long entries = (long long) A->NB * A->MB;
+    const int sgrid = (int) std::min<long long>((entries + 255) / 256, (long long) c->sm_count * 8);
+    eb_tr_scatter_kernel<<<sgrid, 256, 0, c->stream>>>(A->d_indexb, A->d_nnzb, A->NB, A->MB, B->MB, cnt, src, f);
     const int grid = eb_grid<double>(c, A->NB, 8);
-    if (A->matrix_precision == double_real)
-        eb_transpose_kernel<double><<<grid, 128, 0, c->stream>>>(view<double>(A), view<double>(B), f);
-    else
-        eb_transpose_kernel<float><<<grid, 128, 0, c->stream>>>(view<float>(A), view<float>(B), f);
+    bool launched = LAUNCH_OK("eb_tr_scatter_kernel");
+    if (launched && A->matrix_precision == double_real)
+    {
+        launched = CUDA_OK(cudaFuncSetAttribute(eb_tr_place_kernel<double>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        if (launched)
+            eb_tr_place_kernel<double><<<grid, 128, smem, c->stream>>>(view<double>(A), view<double>(B), cnt, src);
+    }
+    else if (launched)
+    {
+        launched = CUDA_OK(cudaFuncSetAttribute(eb_tr_place_kernel<float>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        if (launched)
+            eb_tr_place_kernel<float><<<grid, 128, smem, c->stream>>>(view<float>(A), view<float>(B), cnt, src);
+    }
     int hf = 0;
-    if (!LAUNCH_OK("eb_transpose_kernel") || !eb_read_flags(c, f, &hf, 1))
+    if (!launched || !LAUNCH_OK("eb_tr_place_kernel") || !eb_read_flags(c, f, &hf, 1))
     {
         eb_free(B);
         return nullptr;

@@ -119,6 +119,15 @@ def test_x2_blocks32_bit_exact(oracle_mod, prec, L, radius, thr):
         assert tr[0] == pytest.approx(rtr[0], rel=rel)
         assert tr[1] == pytest.approx(rtr[1], rel=rel)
 
+        # the transpose: blocks transposed, block rows in ascending source row
+        Xt = B.lib.bml_transpose_new(X2)
+        B.check()
+        assert same_bits(to_dense(Xt, N, prec), np.ascontiguousarray(got2.T))
+        tix, tnz, tMB = lists(O, Xt)
+        src_rows = rows(gix, gnz, gMB)
+        assert rows(tix, tnz, tMB) == [[ib for ib in range(nb) if jb in src_rows[ib]] for jb in range(nb)]
+        free(Xt)
+
         # X^2 as the left input: its list order sets the order of the sums
         B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(X2, X4, C.c_double(thr))))
         B.check()
