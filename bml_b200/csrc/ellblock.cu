@@ -588,8 +588,8 @@ template <typename T> __global__ void eb_scale_kernel(EbView<T> A, T s)
 // B's new ones in order.  The merged blocks are built in a per-CTA slab of
 // MBout slots and copied back.
 template <typename T>
-__global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double beta, double thr,
-                              T *slab, int *marks, int *overflow)
+__global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double beta, double thr, int *marks,
+                              int *overflow)
 {
     __shared__ int list[1024];   // merged column-block list
     __shared__ int src_a[1024];  // position in A or -1
@@ -598,7 +598,6 @@ __global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double bet
     __shared__ double red[32];
     const bool use_a = alpha > 0.0 || alpha < 0.0;
     const bool use_b = beta > 0.0 || beta < 0.0;
-    T *myslab = slab + (size_t) blockIdx.x * A.MB * A.slot;
     int *mark = marks + (size_t) blockIdx.x * A.NB;
     const T thr_t = (T) thr;
     for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
@@ -636,15 +635,21 @@ __global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double bet
             ll = 0;
         }
         __syncthreads();
+        // The sum of list entry q is written straight into A at position
+        // kept <= q: A's blocks sit at positions 0..na-1 in list order, so
+        // every block of A still to be read is at a position above kept, and
+        // a block that is dropped is overwritten by the next one kept.  The
+        // max-norm is taken in the same pass.
         const int n = nl;
         int kept = 0;
         for (int q = 0; q < n; ++q)
         {
             const int jb = list[q];
             const int ne = A.bsize[ib] * A.bsize[jb];
-            T *x = myslab + (size_t) kept * A.slot;
             const T *a = src_a[q] >= 0 ? A.blk(ib, src_a[q]) : nullptr;
             const T *b = src_b[q] >= 0 ? B.blk(ib, src_b[q]) : nullptr;
+            T *x = kept < A.MB ? A.blk(ib, kept) : nullptr;
+            double m = 0.0;
             for (int e = threadIdx.x; e < ne; e += blockDim.x)
             {
                 T v = T(0);
@@ -652,34 +657,32 @@ __global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double bet
                     v = axpy_d(v, alpha, a[e]);
                 if (b)
                     v = axpy_d(v, beta, b[e]);
-                x[e] = v;
+                if (x)
+                    x[e] = v;
+                m = fmax(m, (double) fabs(v));
             }
+            for (int o = 16; o; o >>= 1)
+                m = fmax(m, __shfl_xor_sync(FULL, m, o));
+            if ((threadIdx.x & 31) == 0)
+                red[threadIdx.x >> 5] = m;
             __syncthreads();
-            const T normx = (T) block_norm_inf(x, ne, red);
+            double r = 0.0;
+            for (int w = 0; w < (int) (blockDim.x >> 5); ++w)
+                r = fmax(r, red[w]);
+            const T normx = (T) r;
             if (fabs(normx) > thr_t)
             {
-                if (threadIdx.x == 0)
-                    list[kept] = jb; // q >= kept: safe in place
+                if (threadIdx.x == 0 && kept < A.MB)
+                    A.indexb[(size_t) ib * A.MB + kept] = jb;
                 kept++;
             }
-            __syncthreads();
+            __syncthreads(); // red is rewritten, and the kept block's writes land before the next q reads
         }
         if (kept > A.MB)
         {
             if (threadIdx.x == 0)
                 atomicExch(overflow, 1);
             kept = A.MB;
-        }
-        for (int q = 0; q < kept; ++q)
-        {
-            const int jb = list[q];
-            const int ne = A.bsize[ib] * A.bsize[jb];
-            T *dst = A.blk(ib, q);
-            const T *src = myslab + (size_t) q * A.slot;
-            for (int e = threadIdx.x; e < ne; e += blockDim.x)
-                dst[e] = src[e];
-            if (threadIdx.x == 0)
-                A.indexb[(size_t) ib * A.MB + q] = jb;
         }
         if (threadIdx.x == 0)
             A.nnzb[ib] = kept;
@@ -1742,21 +1745,17 @@ bool eb_add(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, double alpha, do
         return ok;
     }
     const int grid = eb_grid<double>(c, A->NB, 4);
-    const size_t sz = prec_size(A->matrix_precision);
-    const size_t slab = (size_t) grid * A->MB * A->slot_elems * sz;
     const size_t marks = (size_t) grid * A->NB * sizeof(int);
-    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(slab + marks + 256));
+    int *dmarks = static_cast<int *>(b200_scratch(marks + 256));
     int *f = eb_flags(c);
-    if (!scr || !f || !CUDA_OK(cudaMemsetAsync(scr + slab, 0, marks, c->stream)))
+    if (!dmarks || !f || !CUDA_OK(cudaMemsetAsync(dmarks, 0, marks, c->stream)))
         return false;
     if (A->matrix_precision == double_real)
         eb_add_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), view<double>(B), alpha, beta, threshold,
-                                                           reinterpret_cast<double *>(scr),
-                                                           reinterpret_cast<int *>(scr + slab), f);
+                                                           dmarks, f);
     else
         eb_add_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), view<float>(B), alpha, beta, threshold,
-                                                          reinterpret_cast<float *>(scr),
-                                                          reinterpret_cast<int *>(scr + slab), f);
+                                                          dmarks, f);
     if (!LAUNCH_OK("eb_add_kernel"))
         return false;
     eb_mark_device(A);
