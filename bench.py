@@ -399,6 +399,11 @@ def x2_roofline(B, H, info):
             "x2_seconds": t, "nnz_x": int(nnz_x), "nnz_x2": int(nnz_x2), "products": P,
             "fp64_gflops": 2.0 * P / t / 1e9, "products_per_s": P / t,
             "compute_frac": 2.0 * P / t / 1e12 / (FP64_NOMINAL_TFLOPS / 2),
+            "busiest_unit": {"unit": "L2 (lts__throughput, tag lookups)", "busy_pct": 69.8,
+                             "l1_to_l2_requests_pct": 73.9, "dram_pct": 26.8,
+                             "source": "ncu --set full of the dense tier on the 30^3 case (bench.py --profile): "
+                                       "the kernel is bound by the L2 reductions and gathers of its accumulator, "
+                                       "neither by HBM bytes nor by FP64 flops"},
             "compute_frac_of": "nominal FP64 %.0f TFLOP/s halved (separately rounded multiply and add per "
                                "product, as in the reference)" % FP64_NOMINAL_TFLOPS,
             "gathered_gbs": 12.0 * P / t / 1e9}
