@@ -692,9 +692,13 @@ __global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double bet
 
 // threshold: drop blocks with max|x| <= thr (order kept), zero the elements
 // with |x| <= thr in the others (ellblock/bml_threshold_ellblock_typed.c:95-140)
-template <typename T> __global__ void eb_threshold_kernel(EbView<T> A, EbView<T> B, double thr)
+template <typename T> __global__ void __launch_bounds__(256) eb_threshold_kernel(EbView<T> A, EbView<T> B, double thr)
 {
-    __shared__ double red[32];
+    // one read of every block: each thread holds its (at most 16) elements
+    // in registers across the max-norm reduction (blocks of at most 64 x 64,
+    // 256 threads); B may be A (kept blocks move down, out <= jp)
+    constexpr int PER = 64 * 64 / 256;
+    __shared__ double red[8];
     const T thr_t = (T) thr;
     for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
     {
@@ -705,14 +709,34 @@ template <typename T> __global__ void eb_threshold_kernel(EbView<T> A, EbView<T>
             const int jb = A.indexb[(size_t) ib * A.MB + jp];
             const int ne = A.bsize[ib] * A.bsize[jb];
             const T *x = A.blk(ib, jp);
-            const T normx = (T) block_norm_inf(x, ne, red);
+            T v[PER];
+            double m = 0.0;
+#pragma unroll
+            for (int u = 0; u < PER; ++u)
+            {
+                const int e = u * 256 + threadIdx.x;
+                v[u] = e < ne ? x[e] : T(0);
+                m = fmax(m, (double) fabs(v[u]));
+            }
+            for (int o = 16; o; o >>= 1)
+                m = fmax(m, __shfl_xor_sync(FULL, m, o));
+            if ((threadIdx.x & 31) == 0)
+                red[threadIdx.x >> 5] = m;
+            __syncthreads();
+            double r = 0.0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w)
+                r = fmax(r, red[w]);
+            const T normx = (T) r;
             if (fabs(normx) > thr_t)
             {
                 T *y = B.blk(ib, out);
-                for (int e = threadIdx.x; e < ne; e += blockDim.x)
+#pragma unroll
+                for (int u = 0; u < PER; ++u)
                 {
-                    const T v = x[e];
-                    y[e] = fabs(v) > thr_t ? v : T(0);
+                    const int e = u * 256 + threadIdx.x;
+                    if (e < ne)
+                        y[e] = fabs(v[u]) > thr_t ? v[u] : T(0);
                 }
                 if (threadIdx.x == 0)
                     B.indexb[(size_t) ib * B.MB + out] = jb;
@@ -1799,9 +1823,17 @@ bool eb_scale_add_identity(bml_matrix_ellblock_t *A, double alpha, double beta, 
            eb_add_identity(A, beta, threshold);
 }
 
+static bool eb_threshold_fits(const bml_matrix_ellblock_t *A)
+{
+    if (A->maxbs <= 64)
+        return true;
+    b200_set_error(BML_B200_ERR_UNSUPPORTED, "ELLBLOCK threshold: blocks larger than 64");
+    return false;
+}
+
 bml_matrix_ellblock_t *eb_threshold_new(bml_matrix_ellblock_t *A, double threshold)
 {
-    if (!A)
+    if (!A || !eb_threshold_fits(A))
         return nullptr;
     bml_matrix_ellblock_t *B = eb_alloc_blocks(A->matrix_precision, A->NB, A->MB, A->M, A->bsize,
                                                A->distribution_mode);
@@ -1828,7 +1860,7 @@ bml_matrix_ellblock_t *eb_threshold_new(bml_matrix_ellblock_t *A, double thresho
 bool eb_threshold(bml_matrix_ellblock_t *A, double threshold)
 {
     B200Context *c = b200_ctx();
-    if (!A || !c || !eb_to_device(A))
+    if (!A || !c || !eb_threshold_fits(A) || !eb_to_device(A))
         return false;
     // in place: each block row's surviving blocks move to lower positions only
     const int grid = eb_grid<double>(c, A->NB, 8);
