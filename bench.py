@@ -143,6 +143,15 @@ def inputs():
     return B.gen_lattice(L, RADIUS, N, M_H, SEED)
 
 
+def bench_config(world):
+    """The `config` object of the JSON line, the same in both arms."""
+    return {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
+            "sp2_iterations": SP2_ITERS,
+            "parallelism": ("rows sharded over %d GPUs (NCCL all-gather of the iterate)" % world)
+            if world > 1 else "1 GPU",
+            "l2": "inputs larger than L2 (iterates ~0.8-1.3 GB)"}
+
+
 # ---------------------------------------------------------------------------
 # libbml_b200 arm
 # ---------------------------------------------------------------------------
@@ -256,6 +265,7 @@ def run_b200(args, rank, world, local):
     # the single-GPU legs (mixed precision, ELLBLOCK tensor cores) run only
     # without the sharded solve
     mixed = mixed_leg(B, v, ix, nz, max(3, min(args.steps, 5))) if world == 1 else None
+    chain = chain_solve_leg(B) if world == 1 else None
     ellb = None if (args.no_ellblock or world > 1) else ellblock_leg()
     ellb_sp2 = None if (args.no_ellblock or world > 1) else ellblock_sp2_leg()
     res = {
@@ -263,9 +273,7 @@ def run_b200(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms, "higher_is_better": False,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded splitmix64 lattice Hamiltonian, generated on the host)",
-        "config": {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
-                   "sp2_iterations": SP2_ITERS, "parallelism": ("rows sharded over %d GPUs (NCCL all-gather of the iterate)" % world) if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (iterates ~0.8-1.3 GB)"},
+        "config": bench_config(world),
         # the transfers move each row's columns up to the widest row
         "e2e": {"value": e2e, "unit": "s",
                 "h2d_bytes_per_step": int(N * int(nz.max()) * (v.itemsize + ix.itemsize) + nz.nbytes),
@@ -276,6 +284,7 @@ def run_b200(args, rank, world, local):
         "sp2": {"iterations": info[0], "trace": info[2], "idempotency": info[3], "max_row_width": widths,
                 "x2_seconds_per_run": x2_seconds_per_run},
         "mixed": mixed,
+        "chain_solve": chain,
         "ellblock_tc": ellb,
         "ellblock_sp2": ellb_sp2,
     }
@@ -341,6 +350,64 @@ def mixed_leg(B, v, ix, nz, reps):
                                  "energy_trDH_rel_err": abs(e1 - e64) / abs(e64),
                                  "density_rel_fro_err": B.lib.bml_fnorm2(D1.h, D64.h) / n64}
     for m in (Hp, D64, Dm, D1, T):
+        m.free()
+    return res
+
+
+def chain_solve_leg(B, reps=3, nclose=2):
+    """Config 1 timed as a full SP2 solve: the 1-D chain Hamiltonian (N=4096,
+    H_ij = u exp(-|i-j|/4) for |i-j| <= 16, seed 0), threshold 1e-5,
+    occupation N/2, M = 512 (the iterates' widths reach ~390; the stated
+    M = 128 overflows, as it does on the reference), run until
+    |tr X - tr X^2| < 1e-8, until that error has not improved for 10
+    iterations, or for 100 iterations.  FP64 against the mixed form (FP32
+    bulk on the unordered kernel, FP64 traces/branch/stop tests, `nclose`
+    closing FP64 iterations).  Device time by CUDA events on the library
+    stream, `reps` solves each; errors of the mixed result against the FP64
+    one: tr D, band energy tr(DH), ||D_mixed - D||_F / ||D||_F, and the
+    idempotency ||D^2 - D||_F of both."""
+    import numpy as np
+    Nc, MHc, Mc = 4096, 128, 512
+    v, ix, nz = B.gen_chain(Nc, MHc, 0)
+    pad = lambda a: np.pad(a.reshape(Nc, MHc), ((0, 0), (0, Mc - MHc))).reshape(-1)
+    H = B.Ellpack.from_arrays(pad(v), pad(ix), nz, Nc, Mc)
+    thr, occ, maxit, tol, stall = 1e-5, Nc / 2.0, 100, 1e-8, 10
+
+    def timed(fn):
+        fn()
+        B.check(B.lib.bml_b200_synchronize())
+        B.check(B.lib.bml_b200_event_record(4))
+        for _ in range(reps):
+            fn()
+        B.check(B.lib.bml_b200_event_record(5))
+        return B.event_ms(4, 5) / 1e3 / reps
+
+    D64, Dm = B.Ellpack(Nc, Mc), B.Ellpack(Nc, Mc)
+    i64, im = (C.c_double * 6)(), (C.c_double * 8)()
+    t64 = timed(lambda: B.check(B.lib.bml_b200_sp2(H.h, D64.h, thr, occ, maxit, tol, stall, i64)))
+    tm = timed(lambda: B.check(B.lib.bml_b200_sp2_mixed(H.h, Dm.h, thr, occ, maxit, tol, stall, nclose, im)))
+    e64, em = B.lib.bml_trace_mult(D64.h, H.h), B.lib.bml_trace_mult(Dm.h, H.h)
+    T = B.Ellpack(Nc, 2 * Mc)
+
+    def idem(D):
+        st, _ = B.multiply_x2(D, T, thr)
+        B.check(st)
+        return B.lib.bml_fnorm2(T.h, D.h)
+
+    rules = {1: "tol", 2: "stall", 3: "maxiter", 4: "error"}
+    res = {"workload": "SP2 solve on the 1-D chain Hamiltonian (N=4096, M=512, thr 1e-5, occ N/2) to the stop "
+                       "rule (|trX - trX^2| < 1e-8, no improvement in 10 iterations, or 100 iterations)",
+           "fp64": {"s": t64, "iterations": int(i64[0]), "rule": rules.get(int(i64[1])), "trace": i64[2],
+                    "trace_err_t_minus_t2": i64[3], "energy_trDH": e64, "idempotency_fro": idem(D64)},
+           "mixed": {"s": tm, "iterations": int(im[0]), "fp32_iterations": int(im[6]),
+                     "fp64_closing_iterations": nclose, "rule": rules.get(int(im[1])), "trace": im[2],
+                     "energy_trDH": em, "idempotency_fro": idem(Dm)},
+           "speedup": t64 / tm,
+           "trace_rel_err": abs(im[2] - i64[2]) / abs(i64[2]),
+           "energy_trDH_rel_err": abs(em - e64) / abs(e64),
+           "density_rel_fro_err": B.lib.bml_fnorm2(Dm.h, D64.h) / B.lib.bml_fnorm(D64.h),
+           "target": "mixed >= 2x faster than FP64 at <= 1e-6 relative trace/energy error"}
+    for m in (H, D64, Dm, T):
         m.free()
     return res
 
@@ -445,7 +512,9 @@ def _ref_setup():
     if not O.available():
         raise RuntimeError("oracle/_ref is not built")
     import numpy as np
-    v, ix, nz = inputs()
+    # the oracle's own copy of the seeded generator: this process never loads
+    # the library under test
+    v, ix, nz = O.gen_lattice(L, RADIUS, N, M_H, SEED)
     # the reference copies whole padded rows: H and the iterates share M
     pad = lambda a: np.pad(a.reshape(N, M_H), ((0, 0), (0, M_X - M_H))).reshape(-1)
     H = O.ref_ellpack(pad(v), pad(ix), nz, N, M_X)
@@ -468,8 +537,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     O, H, D, X2, threads = _ref_setup()
-    warm = max(0, min(args.warmup, 1))
-    steps = max(1, min(args.steps, 2))
+    warm, steps = args.warmup, args.steps
     for _ in range(warm):
         ref_sp2(O, H, D, X2, SP2_ITERS)
     t0 = time.perf_counter()
@@ -482,8 +550,7 @@ def run_reference(args, rank, world):
             "steps": steps, "warmup": warm, "ms_per_step": dt * 1e3, "higher_is_better": False,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded splitmix64 lattice Hamiltonian)",
-            "config": {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
-                       "sp2_iterations": SP2_ITERS},
+            "config": bench_config(world),
             "cpu_baseline": {"value": dt, "unit": "s", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": dt, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

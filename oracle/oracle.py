@@ -90,6 +90,8 @@ def ref():
             "bml_set_block_sizes": (None, [C.POINTER(i), i, i]),
             "bml_get_N": (i, [vp]),
             "bml_get_M": (i, [vp]),
+            "bml_write_bml_matrix": (None, [vp, C.c_char_p]),
+            "bml_read_bml_matrix": (None, [vp, C.c_char_p]),
         }
         for name, (res, args) in protos.items():
             f = getattr(lib, name)
@@ -201,6 +203,33 @@ def rest_sp2(v, ix, nz, N, M, thr, occ, maxiter, tol, stall):
                              _p(dv, C.c_double), _p(dix, C.c_int), _p(dnz, C.c_int),
                              _p(info, C.c_double))
     return (dv, dix, dnz), info
+
+
+# ---------------------------------------------------------------------------
+# seeded inputs without the library under test (bml_oracle_gen.c)
+# ---------------------------------------------------------------------------
+def gen_chain(N, M, seed=0):
+    """The 1-D chain Hamiltonian, reference ELLPACK host layout."""
+    v = np.zeros(N * M, np.float64)
+    ix = np.zeros(N * M, np.int32)
+    nz = np.zeros(N, np.int32)
+    f = rest().oracle_gen_chain
+    f.restype = C.c_int
+    if f(N, M, C.c_ulonglong(seed), _p(v, C.c_double), _p(ix, C.c_int), _p(nz, C.c_int)) < 0:
+        raise ValueError("chain generator: a row needs more than M=%d entries" % M)
+    return v, ix, nz
+
+
+def gen_lattice(L, radius, N, M, seed=0):
+    """The L^3 lattice Hamiltonian (first N sites), reference ELLPACK host layout."""
+    v = np.zeros(N * M, np.float64)
+    ix = np.zeros(N * M, np.int32)
+    nz = np.zeros(N, np.int32)
+    f = rest().oracle_gen_lattice
+    f.restype = C.c_int
+    if f(L, radius, N, M, C.c_ulonglong(seed), _p(v, C.c_double), _p(ix, C.c_int), _p(nz, C.c_int)) < 0:
+        raise ValueError("lattice generator: a row needs more than M=%d entries" % M)
+    return v, ix, nz
 
 
 # ---------------------------------------------------------------------------

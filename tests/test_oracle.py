@@ -31,6 +31,23 @@ def test_generators_match_digests():
         assert h.hexdigest() == dig[name], name
 
 
+def test_oracle_generators_match_digests():
+    """The oracle's own generators (used where the library must not be
+    loaded, as in bench.py's reference arm) give the same bytes."""
+    dig = json.load(open(os.path.join(GOLD, "generators.json")))
+    for name, args in (("chain_4096_128", lambda: O.gen_chain(4096, 128, 0)),
+                       ("lattice_40_r3_256", lambda: O.gen_lattice(40, 3, 64000, 256, 0))):
+        h = hashlib.sha256()
+        for a in args():
+            h.update(np.ascontiguousarray(a).tobytes())
+        assert h.hexdigest() == dig[name], name
+    # a truncated lattice and another seed agree with the library too
+    a = O.gen_lattice(26, 3, 16384, 128, 7)
+    b = B.gen_lattice(26, 3, 16384, 128, 7)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
 def test_restatement_x2_matches_golden_chain():
     g = gold("x2_chain.npz")
     N, M, M2 = 256, 64, int(g["M2"])
@@ -149,3 +166,22 @@ def test_restatement_ellblock_x2_matches_reference(ref, prec, thr):
         assert np.array_equal(rix[ib * s2.MB:ib * s2.MB + rnz[ib]], oix[ib * nb:ib * nb + onz[ib]])
     assert tr[0] == pytest.approx(rtr[0], rel=1e-12 if prec == O.DOUBLE else 1e-6)
     assert tr[1] == pytest.approx(rtr[1], rel=1e-12 if prec == O.DOUBLE else 1e-6)
+
+
+def test_restatement_on_example_hamiltonian(oracle_mod):
+    """The reference's example Hamiltonian (fixture from make_golden.py):
+    the restatement's X^2 equals the reference's bit for bit."""
+    O = oracle_mod
+    g = gold("hamiltonian600.npz")
+    v, ix, nz, N, M = g["value"], g["index"], g["nnz"], int(g["N"]), int(g["M"])
+    assert int(nz.sum()) == 12246 and int(nz.max()) <= M
+    for thr in (0.0, 1e-3, 1e-1):
+        A = O.ref_ellpack(v, ix, nz, N, M)
+        R = O.ref().bml_zero_matrix(2, 2, N, N, 0)
+        tr_ref = O.ref_x2(A, R, thr)
+        ref = O.ref_ellpack_arrays(R)
+        O.ref_free(A)
+        O.ref_free(R)
+        got, tr, _ = O.rest_x2(v, ix, nz, N, M, thr, N)
+        assert O.same_rows_exact(got, ref, N, N)
+        assert tr[1] == pytest.approx(tr_ref[1], rel=1e-12)
