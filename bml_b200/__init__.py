@@ -122,6 +122,10 @@ _PROTOS = {
     "bml_b200_reset_block_sizes": (None, []),
     "bml_b200_last_tier_counts": (_i, [_ip, _i]),
     "bml_b200_set_x2_tiers": (_i, [_i]),
+    "bml_b200_set_x2_exact": (_i, [_i]),
+    "bml_getNRanks": (_i, []),
+    "bml_getMyRank": (_i, []),
+    "bml_printRank": (_i, []),
     "bml_b200_set_ellblock_slab_budget": (C.c_longlong, [C.c_longlong]),
     "bml_b200_set_device": (_i, [_i]),
     "bml_b200_launch_count": (C.c_ulonglong, []),

@@ -77,6 +77,9 @@ struct bml_matrix_ellblock_t
 // ---------------------------------------------------------------------------
 void b200_set_error(int status, const char *fmt, ...);
 int b200_get_error();
+// Sets whether errors are printed as they are recorded; returns the previous
+// setting (a caller that expects and handles an error mutes it around the call).
+int b200_swap_verbose(int on);
 
 // Evaluates a CUDA runtime call; on failure records ERR_CUDA and yields false.
 bool b200_cuda_ok(cudaError_t err, const char *what, const char *file, int line);
@@ -137,6 +140,14 @@ void ell_set_f32_reduce(bool on);
 bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B,
                      bml_matrix_ellpack_t *C, double threshold, double *trace,
                      int *required_M, int x2_rows = 0);
+// The unordered product (ellpack_x2_fast.cu): the same products and keep
+// rule, sums in no fixed order, rows written in ascending column order.
+// ell_multiply_AB uses it unless the ordered (bit-identical) form is selected
+// (bml_b200_set_x2_exact) or the row width exceeds what it holds.
+bool ell_x2_exact();
+bool ell_unordered_fits(const bml_matrix_ellpack_t *A);
+bool ell_multiply_unordered(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C,
+                            double threshold, double *trace, int *required_M, bool check_pre);
 // A view of rows [r0, r1) of A: the same storage, N = r1 - r0 (columns keep
 // their global numbering).  Operations on the view touch only those rows.
 bml_matrix_ellpack_t ell_row_view(const bml_matrix_ellpack_t *A, int r0, int r1);

@@ -225,6 +225,10 @@ BML_B200_API void bml_b200_reset_block_sizes(void);
 /* ---- init / shutdown / logging / printing -------------------------------- */
 BML_B200_API void bml_init(void);                                  /* bml_init.h:12 (non-MPI form) */
 BML_B200_API void bml_shutdown(void);                              /* bml_shutdown.h:8 */
+/* one process per library context: rank 0 of 1 (the reference's non-MPI build) */
+BML_B200_API int bml_getNRanks(void);                              /* bml_parallel.h:22 */
+BML_B200_API int bml_getMyRank(void);                              /* bml_parallel.h:26 */
+BML_B200_API int bml_printRank(void);                              /* bml_parallel.h:38 */
 BML_B200_API void bml_log(bml_log_level_t log_level, char *format, ...);  /* bml_logger.h:24 */
 BML_B200_API void bml_log_location(bml_log_level_t log_level, char *filename,
     int linenumber, char *format, ...);                            /* bml_logger.h:29 */
@@ -300,6 +304,18 @@ BML_B200_API int bml_b200_last_tier_counts(int *counts, int n);
  * next enabled one.  Also discards the per-row width estimates kept from the
  * last multiply.  Returns the previous mask.  No reference counterpart. */
 BML_B200_API int bml_b200_set_x2_tiers(int mask);
+
+/* Chooses how later ELLPACK products (bml_multiply_x2, bml_multiply,
+ * bml_multiply_AB and the SP2 drivers) sum.  exact = 0 (the default): the
+ * unordered kernel, which forms the same products and applies the same keep
+ * rule but adds the products of one entry in no fixed order (each still a
+ * separately rounded multiply and add), so an entry differs from the
+ * reference's by at most (n-1) u sum|a_ij b_jk| for n products, and writes a
+ * row's kept entries in ascending column order.  exact = 1: the ordered tiers
+ * above, bit-identical to the reference, rows in its first-touch order.
+ * Rows wider than the unordered kernel holds (M above about 8000) always use
+ * the ordered tiers.  Returns the previous choice.  No reference counterpart. */
+BML_B200_API int bml_b200_set_x2_exact(int exact);
 
 /* Device-memory budget, in bytes, for the accumulator slabs of the exact
  * ELLBLOCK products (bml_multiply_x2, bml_multiply_AB, bml_multiply): every

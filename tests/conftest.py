@@ -11,6 +11,8 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    config.addinivalue_line("markers", "unordered: runs the ELLPACK products in the unordered form "
+                                       "(GPU tests default to the ordered, bit-identical form)")
 
 
 def _ensure_built():
@@ -38,3 +40,16 @@ def oracle_mod():
     if not oracle.available():
         pytest.skip("oracle/_ref not built (make -C oracle needs the reference sources)")
     return oracle
+
+
+@pytest.fixture(autouse=True)
+def _ellpack_product_form(request):
+    """GPU tests that compare bit for bit run the ordered products; tests
+    marked `unordered` run the unordered (default) form."""
+    if request.node.get_closest_marker("gpu") is None:
+        yield
+        return
+    import bml_b200 as B
+    old = B.lib.bml_b200_set_x2_exact(0 if request.node.get_closest_marker("unordered") else 1)
+    yield
+    B.lib.bml_b200_set_x2_exact(old)
