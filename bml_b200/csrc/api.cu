@@ -530,6 +530,11 @@ void bml_set_element(bml_matrix_t *A, int i, int j, void *value)
 // (ellpack/bml_setters_ellpack_typed.c:126-160).
 void bml_set_row(bml_matrix_t *A, int i, void *row, double threshold)
 {
+    if (type_of(A) == ellblock)
+    {
+        eb_set_row(static_cast<bml_matrix_ellblock_t *>(A), i, row, threshold);
+        return;
+    }
     bml_matrix_ellpack_t *E = as_ell(A, "set_row");
     if (!E || !row || !ell_to_host(E) || i < 0 || i >= E->N)
         return;
@@ -561,6 +566,11 @@ void bml_set_row(bml_matrix_t *A, int i, void *row, double threshold)
 // if absent), as ellpack/bml_setters_ellpack_typed.c:175-225.
 void bml_set_diagonal(bml_matrix_t *A, void *diagonal, double threshold)
 {
+    if (type_of(A) == ellblock)
+    {
+        eb_set_diagonal(static_cast<bml_matrix_ellblock_t *>(A), diagonal, threshold);
+        return;
+    }
     bml_matrix_ellpack_t *E = as_ell(A, "set_diagonal");
     if (!E || !diagonal || !ell_to_host(E))
         return;
@@ -1011,12 +1021,28 @@ int bml_sqrtint(const int x)
     return r;
 }
 
-// Matrix Market coordinate real general, 1-based (the format the reference
-// writes in ellpack/bml_utilities_ellpack_typed.c).
+// Matrix Market coordinate files, 1-based, in the reference's formats
+// (bml_utilities.c:496-540 dispatch; ellpack/bml_utilities_ellpack_typed.c:
+// 22-203, ellblock/bml_utilities_ellblock_typed.c:25-256).  Both formats
+// write the header "%%%MatrixMarket matrix coordinate real general" and
+// "N N nnz"; ELLPACK writes each stored entry as "%d %d %20.15lg" (FP32:
+// "%20.15g"), ELLBLOCK every element of every stored block as
+// "%d %d %20.15e".  Reading appends to the matrix it is given (entries
+// already there are kept); a "symmetric" header mirrors off-diagonal entries.
 void bml_write_bml_matrix(bml_matrix_t *A, char *filename)
 {
-    bml_matrix_ellpack_t *E = as_ell(A, "write_bml_matrix");
-    if (!E || !filename || !ell_to_host(E))
+    if (!A || !filename)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "write_bml_matrix: NULL argument");
+        return;
+    }
+    const bml_matrix_type_t t = type_of(A);
+    if (t != ellpack && t != ellblock)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "write_bml_matrix: matrix type %d", (int) t);
+        return;
+    }
+    if (t == ellpack && !ell_to_host(static_cast<bml_matrix_ellpack_t *>(A)))
         return;
     FILE *f = fopen(filename, "w");
     if (!f)
@@ -1024,79 +1050,156 @@ void bml_write_bml_matrix(bml_matrix_t *A, char *filename)
         b200_set_error(BML_B200_ERR_INVALID, "write_bml_matrix: cannot open %s", filename);
         return;
     }
+    if (t == ellblock)
+    {
+        eb_write_mm(static_cast<bml_matrix_ellblock_t *>(A), f);
+        fclose(f);
+        return;
+    }
+    bml_matrix_ellpack_t *E = static_cast<bml_matrix_ellpack_t *>(A);
     long long nnz = 0;
     for (int i = 0; i < E->N; i++)
         nnz += E->nnz[i];
-    fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n");
+    fprintf(f, "%%%%%%MatrixMarket matrix coordinate real general\n");
     fprintf(f, "%d %d %lld\n", E->N, E->N, nnz);
     for (int i = 0; i < E->N; i++)
         for (int p = 0; p < E->nnz[i]; p++)
         {
             const size_t at = (size_t) i * E->M + p;
-            const double v = E->matrix_precision == double_real ? static_cast<double *>(E->value)[at]
-                                                                : static_cast<float *>(E->value)[at];
-            fprintf(f, "%d %d %20.15e\n", i + 1, E->index[at] + 1, v);
+            if (E->matrix_precision == double_real)
+                fprintf(f, "%d %d %20.15lg\n", i + 1, E->index[at] + 1, static_cast<double *>(E->value)[at]);
+            else
+                fprintf(f, "%d %d %20.15g\n", i + 1, E->index[at] + 1, (double) static_cast<float *>(E->value)[at]);
         }
     fclose(f);
 }
 
+} // extern "C"
+
+namespace {
+
+// Header: five words, the fifth "symmetric" or not (the reference reads them
+// with "%s %s %s %s %s"), then "rows cols entries" after any comment lines.
+bool read_mm_header(FILE *f, const char *filename, int *n, long long *ne, bool *symmetric)
+{
+    char w[5][64];
+    if (fscanf(f, "%63s %63s %63s %63s %63s", w[0], w[1], w[2], w[3], w[4]) != 5)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: %s: read error on header", filename);
+        return false;
+    }
+    *symmetric = strcmp(w[4], "symmetric") == 0;
+    int c;
+    while ((c = fgetc(f)) != EOF)
+    {
+        if (c == '%')
+        {
+            while ((c = fgetc(f)) != EOF && c != '\n')
+                ;
+            continue;
+        }
+        if (c != ' ' && c != '\t' && c != '\n' && c != '\r')
+        {
+            ungetc(c, f);
+            break;
+        }
+    }
+    int nc = 0;
+    if (fscanf(f, "%d %d %lld", n, &nc, ne) != 3 || *ne < 0)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: %s: read error on the size line", filename);
+        return false;
+    }
+    return true;
+}
+
+template <typename T> bool ell_read_mm(bml_matrix_ellpack_t *E, FILE *f, long long ne, bool symmetric)
+{
+    T *val = static_cast<T *>(E->value);
+    auto put = [&](int i, int j, T v) {
+        if (E->nnz[i] >= E->M)
+        {
+            b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "read_bml_matrix: row %d needs more than M=%d entries",
+                           i + 1, E->M);
+            return false;
+        }
+        const size_t at = (size_t) i * E->M + E->nnz[i];
+        E->index[at] = j;
+        val[at] = v;
+        E->nnz[i]++;
+        return true;
+    };
+    for (long long e = 0; e < ne; e++)
+    {
+        int i, j;
+        T v;
+        const int got = sizeof(T) == 8 ? fscanf(f, "%d %d %lf", &i, &j, reinterpret_cast<double *>(&v))
+                                       : fscanf(f, "%d %d %f", &i, &j, reinterpret_cast<float *>(&v));
+        if (got != 3)
+        {
+            b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: entry %lld of %lld unreadable", e + 1, ne);
+            return false;
+        }
+        i--;
+        j--;
+        if (i < 0 || j < 0 || i >= E->N || j >= E->N)
+        {
+            b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: entry (%d, %d) outside N=%d", i + 1, j + 1, E->N);
+            return false;
+        }
+        if (!put(i, j, v) || (symmetric && j != i && !put(j, i, v)))
+            return false;
+    }
+    return true;
+}
+
+} // namespace
+
+extern "C" {
+
 void bml_read_bml_matrix(bml_matrix_t *A, char *filename)
 {
-    bml_matrix_ellpack_t *E = as_ell(A, "read_bml_matrix");
-    if (!E || !filename || !ell_to_host(E))
+    if (!A || !filename)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: NULL argument");
         return;
+    }
+    const bml_matrix_type_t t = type_of(A);
+    if (t != ellpack && t != ellblock)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "read_bml_matrix: matrix type %d", (int) t);
+        return;
+    }
     FILE *f = fopen(filename, "r");
     if (!f)
     {
         b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: cannot open %s", filename);
         return;
     }
-    char line[1024];
-    int hdr = 0;
-    int nr = 0, nc = 0;
+    int n = 0;
     long long ne = 0;
-    while (fgets(line, sizeof line, f))
+    bool symmetric = false;
+    if (read_mm_header(f, filename, &n, &ne, &symmetric))
     {
-        if (line[0] == '%')
-            continue;
-        if (sscanf(line, "%d %d %lld", &nr, &nc, &ne) == 3)
-        {
-            hdr = 1;
-            break;
-        }
-    }
-    if (!hdr || nr != E->N)
-    {
-        b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: header of %s does not match N=%d",
-                       filename, E->N);
-        fclose(f);
-        return;
-    }
-    memset(E->nnz, 0, sizeof(int) * E->N);
-    for (long long e = 0; e < ne; e++)
-    {
-        int i, j;
-        double v;
-        if (fscanf(f, "%d %d %lf", &i, &j, &v) != 3)
-            break;
-        i--;
-        j--;
-        if (i < 0 || i >= E->N || j < 0 || j >= E->N || E->nnz[i] >= E->M)
-        {
-            b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: entry (%d, %d) out of range or row full",
-                           i + 1, j + 1);
-            continue;
-        }
-        const size_t at = (size_t) i * E->M + E->nnz[i];
-        if (E->matrix_precision == double_real)
-            static_cast<double *>(E->value)[at] = v;
+        if (n != bml_get_N(A))
+            b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: %s holds N=%d, the matrix has N=%d", filename, n,
+                           bml_get_N(A));
+        else if (t == ellblock)
+            eb_read_mm(static_cast<bml_matrix_ellblock_t *>(A), f, ne, symmetric);
         else
-            static_cast<float *>(E->value)[at] = (float) v;
-        E->index[at] = j;
-        E->nnz[i]++;
+        {
+            bml_matrix_ellpack_t *E = static_cast<bml_matrix_ellpack_t *>(A);
+            if (ell_to_host(E))
+            {
+                if (E->matrix_precision == double_real)
+                    ell_read_mm<double>(E, f, ne, symmetric);
+                else
+                    ell_read_mm<float>(E, f, ne, symmetric);
+                ell_mark_host(E);
+            }
+        }
     }
     fclose(f);
-    ell_mark_host(E);
 }
 
 // ---------------------------------------------------------------------------

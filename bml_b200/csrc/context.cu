@@ -39,6 +39,13 @@ void b200_set_error(int status, const char *fmt, ...)
 
 int b200_get_error() { return g_last_error; }
 
+int b200_swap_verbose(int on)
+{
+    const int old = g_verbose;
+    g_verbose = on;
+    return old;
+}
+
 bool b200_cuda_ok(cudaError_t err, const char *what, const char *file, int line)
 {
     if (err == cudaSuccess)
@@ -186,6 +193,12 @@ int bml_b200_device_info(int *sm_count, int *device)
 }
 
 void bml_init(void) { (void) b200_ctx(); }
+
+int bml_getNRanks(void) { return 1; }
+
+int bml_getMyRank(void) { return 0; }
+
+int bml_printRank(void) { return 1; }
 
 int bml_b200_set_device(int device)
 {

@@ -381,6 +381,178 @@ void eb_set_element(bml_matrix_ellblock_t *A, int i, int j, const void *value, b
     eb_mark_host(A);
 }
 
+// ---------------------------------------------------------------------------
+// Matrix Market I/O (ellblock/bml_utilities_ellblock_typed.c:25-256)
+// ---------------------------------------------------------------------------
+// Writes every element of every stored block, block rows in order, blocks in
+// list order, elements row-major, 1-based, "%d %d %20.15e" (:174-256).
+bool eb_write_mm(bml_matrix_ellblock_t *A, FILE *f)
+{
+    if (!eb_to_host(A))
+        return false;
+    std::vector<int> off(A->NB + 1, 0);
+    for (int ib = 0; ib < A->NB; ib++)
+        off[ib + 1] = off[ib] + A->bsize[ib];
+    long long msum = 0;
+    for (int ib = 0; ib < A->NB; ib++)
+        for (int jp = 0; jp < A->nnzb[ib]; jp++)
+            msum += (long long) A->bsize[ib] * A->bsize[A->indexb[(size_t) ib * A->MB + jp]];
+    fprintf(f, "%%%%%%MatrixMarket matrix coordinate real general\n");
+    fprintf(f, "%d %d %lld\n", A->N, A->N, msum);
+    const bool dbl = A->matrix_precision == double_real;
+    for (int ib = 0; ib < A->NB; ib++)
+        for (int jp = 0; jp < A->nnzb[ib]; jp++)
+        {
+            const int jb = A->indexb[(size_t) ib * A->MB + jp];
+            for (int ii = 0; ii < A->bsize[ib]; ii++)
+                for (int jj = 0; jj < A->bsize[jb]; jj++)
+                {
+                    const int e = ii * A->bsize[jb] + jj;
+                    const double v = dbl ? (double) hblk<double>(A, ib, jp)[e] : (double) hblk<float>(A, ib, jp)[e];
+                    fprintf(f, "%d %d %20.15e\n", off[ib] + 1 + ii, off[jb] + 1 + jj, v);
+                }
+        }
+    return true;
+}
+
+// Reads `ne` entries "%d %d value" (1-based) into A: each entry is written
+// into its block, a block the row lacks is appended zeroed (existing blocks
+// and entries are kept, as the reference reads into the matrix it is given);
+// with a symmetric header the transposed entry is set too (:25-167; where
+// the reference's symmetric branch appends a block it writes the column
+// index at slot nnzb[jb] of block row 0 and leaves the block unallocated,
+// :148-156, here the block goes to its own row, zeroed).  Values are parsed
+// in the matrix precision (%e / %le).
+template <typename T> static bool eb_read_mm_typed(bml_matrix_ellblock_t *A, FILE *f, long long ne, bool symmetric)
+{
+    for (long long e = 0; e < ne; e++)
+    {
+        int i, j;
+        T v;
+        const int got = sizeof(T) == 8 ? fscanf(f, "%d %d %le", &i, &j, reinterpret_cast<double *>(&v))
+                                       : fscanf(f, "%d %d %e", &i, &j, reinterpret_cast<float *>(&v));
+        if (got != 3)
+        {
+            b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: entry %lld of %lld unreadable", e + 1, ne);
+            return false;
+        }
+        i--;
+        j--;
+        if (i < 0 || j < 0 || i >= A->N || j >= A->N)
+        {
+            b200_set_error(BML_B200_ERR_INVALID, "read_bml_matrix: entry (%d, %d) outside N=%d", i + 1, j + 1, A->N);
+            return false;
+        }
+        eb_set_element_host<T>(A, i, j, v, true);
+        if (symmetric && i != j)
+            eb_set_element_host<T>(A, j, i, v, true);
+        if (b200_get_error() == BML_B200_ERR_ROW_OVERFLOW)
+            return false;
+    }
+    return true;
+}
+
+bool eb_read_mm(bml_matrix_ellblock_t *A, FILE *f, long long ne, bool symmetric)
+{
+    if (!eb_to_host(A))
+        return false;
+    bml_b200_clear_error();
+    const bool ok = A->matrix_precision == double_real ? eb_read_mm_typed<double>(A, f, ne, symmetric)
+                                                       : eb_read_mm_typed<float>(A, f, ne, symmetric);
+    host_pointers(A);
+    eb_mark_host(A);
+    return ok;
+}
+
+// Row i <- the entries of row[0..N) with |row[k]| > threshold, written into
+// their blocks (a missing block is appended zeroed); entries already in the
+// row are kept (ellblock/bml_setters_ellblock_typed.c:131-198).
+template <typename T> static void eb_set_row_host(bml_matrix_ellblock_t *A, int i, const T *row, double threshold)
+{
+    for (int k = 0; k < A->N; k++)
+        if (fabs((double) row[k]) > threshold)
+        {
+            eb_set_element_host<T>(A, i, k, row[k], true);
+            if (b200_get_error() == BML_B200_ERR_ROW_OVERFLOW)
+                return;
+        }
+}
+
+void eb_set_row(bml_matrix_ellblock_t *A, int i, const void *row, double threshold)
+{
+    if (!A || !row || i < 0 || i >= A->N)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK set_row %d", i);
+        return;
+    }
+    if (!eb_to_host(A))
+        return;
+    if (A->matrix_precision == double_real)
+        eb_set_row_host<double>(A, i, static_cast<const double *>(row), threshold);
+    else
+        eb_set_row_host<float>(A, i, static_cast<const float *>(row), threshold);
+    host_pointers(A);
+    eb_mark_host(A);
+}
+
+// Diagonal <- diagonal[0..N): per block row, when the max |d| of the block's
+// segment exceeds threshold the diagonal block's diagonal takes the segment
+// (the block is appended zeroed if missing), otherwise an existing diagonal
+// block's diagonal is zeroed (ellblock/bml_setters_ellblock_typed.c:209-284).
+template <typename T> static void eb_set_diagonal_host(bml_matrix_ellblock_t *A, const T *d, double threshold)
+{
+    int off = 0;
+    for (int ib = 0; ib < A->NB; ib++)
+    {
+        const int bs = A->bsize[ib];
+        double norm = 0.0;
+        for (int ii = 0; ii < bs; ii++)
+            norm = fmax(norm, (double) fabs((double) d[off + ii]));
+        bool found = false;
+        for (int jp = 0; jp < A->nnzb[ib]; jp++)
+            if (A->indexb[(size_t) ib * A->MB + jp] == ib)
+            {
+                T *b = hblk<T>(A, ib, jp);
+                for (int ii = 0; ii < bs; ii++)
+                    b[ii * bs + ii] = norm > threshold ? d[off + ii] : T(0);
+                found = true;
+            }
+        if (!found && norm > threshold)
+        {
+            if (A->nnzb[ib] == A->MB)
+            {
+                b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "set_diagonal: block row %d is full (MB=%d)", ib, A->MB);
+                return;
+            }
+            const int jp = A->nnzb[ib];
+            T *b = hblk<T>(A, ib, jp);
+            memset(b, 0, sizeof(T) * bs * bs);
+            for (int ii = 0; ii < bs; ii++)
+                b[ii * bs + ii] = d[off + ii];
+            A->indexb[(size_t) ib * A->MB + jp] = ib;
+            A->nnzb[ib]++;
+        }
+        off += bs;
+    }
+}
+
+void eb_set_diagonal(bml_matrix_ellblock_t *A, const void *diagonal, double threshold)
+{
+    if (!A || !diagonal)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "ELLBLOCK set_diagonal: NULL argument");
+        return;
+    }
+    if (!eb_to_host(A))
+        return;
+    if (A->matrix_precision == double_real)
+        eb_set_diagonal_host<double>(A, static_cast<const double *>(diagonal), threshold);
+    else
+        eb_set_diagonal_host<float>(A, static_cast<const float *>(diagonal), threshold);
+    host_pointers(A);
+    eb_mark_host(A);
+}
+
 template <typename T> static T eb_get_host(bml_matrix_ellblock_t *A, int i, int j, bool &found, T **where)
 {
     int ib = 0, jb = 0, ii = i, jj = j;
@@ -585,20 +757,22 @@ template <typename T> __global__ void eb_scale_kernel(EbView<T> A, T s)
 // A <- alpha*A + beta*B, block kept if max|x| > thr (norm rounded to the
 // matrix precision, as `REAL_T normx = bml_norm_inf(...)` does)
 // (ellblock/bml_add_ellblock_typed.c:35-197).  Blocks: A's in order, then
-// B's new ones in order.  The merged blocks are built in a per-CTA slab of
-// MBout slots and copied back.
+// B's new ones in order.  Thread 0 of each CTA merges the two block lists of
+// a block row into the CTA's scratch (mark[NB] | list[cap] | src_a[cap] |
+// src_b[cap], cap = A.MB + B.MB, so a merged row of any width fits); the
+// sums are then written in place (see below).
 template <typename T>
-__global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double beta, double thr, int *marks,
-                              int *overflow)
+__global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double beta, double thr, int *scr,
+                              int cap, int *overflow)
 {
-    __shared__ int list[1024];   // merged column-block list
-    __shared__ int src_a[1024];  // position in A or -1
-    __shared__ int src_b[1024];  // position in B or -1
-    __shared__ int nl, ll;
+    __shared__ int nl;
     __shared__ double red[32];
     const bool use_a = alpha > 0.0 || alpha < 0.0;
     const bool use_b = beta > 0.0 || beta < 0.0;
-    int *mark = marks + (size_t) blockIdx.x * A.NB;
+    int *mark = scr + (size_t) blockIdx.x * (A.NB + 3 * (size_t) cap);
+    int *list = mark + A.NB;   // merged column-block list
+    int *src_a = list + cap;   // position in A or -1
+    int *src_b = src_a + cap;  // position in B or -1
     const T thr_t = (T) thr;
     for (int ib = blockIdx.x; ib < A.NB; ib += gridDim.x)
     {
@@ -606,7 +780,7 @@ __global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double bet
         {
             int n = 0;
             const int na = use_a ? A.nnzb[ib] : 0, nb = use_b ? B.nnzb[ib] : 0;
-            for (int p = 0; p < na && n < 1024; ++p)
+            for (int p = 0; p < na; ++p)
             {
                 const int jb = A.indexb[(size_t) ib * A.MB + p];
                 mark[jb] = n + 1;
@@ -615,7 +789,7 @@ __global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double bet
                 src_b[n] = -1;
                 n++;
             }
-            for (int p = 0; p < nb && n < 1024; ++p)
+            for (int p = 0; p < nb; ++p)
             {
                 const int jb = B.indexb[(size_t) ib * B.MB + p];
                 if (mark[jb])
@@ -632,7 +806,6 @@ __global__ void eb_add_kernel(EbView<T> A, EbView<T> B, double alpha, double bet
             for (int q = 0; q < n; ++q)
                 mark[list[q]] = 0;
             nl = n;
-            ll = 0;
         }
         __syncthreads();
         // The sum of list entry q is written straight into A at position
@@ -1769,17 +1942,18 @@ bool eb_add(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, double alpha, do
         return ok;
     }
     const int grid = eb_grid<double>(c, A->NB, 4);
-    const size_t marks = (size_t) grid * A->NB * sizeof(int);
+    const int cap = A->MB + B->MB;
+    const size_t marks = (size_t) grid * (A->NB + 3 * (size_t) cap) * sizeof(int);
     int *dmarks = static_cast<int *>(b200_scratch(marks + 256));
     int *f = eb_flags(c);
     if (!dmarks || !f || !CUDA_OK(cudaMemsetAsync(dmarks, 0, marks, c->stream)))
         return false;
     if (A->matrix_precision == double_real)
         eb_add_kernel<double><<<grid, 256, 0, c->stream>>>(view<double>(A), view<double>(B), alpha, beta, threshold,
-                                                           dmarks, f);
+                                                           dmarks, cap, f);
     else
         eb_add_kernel<float><<<grid, 256, 0, c->stream>>>(view<float>(A), view<float>(B), alpha, beta, threshold,
-                                                          dmarks, f);
+                                                          dmarks, cap, f);
     if (!LAUNCH_OK("eb_add_kernel"))
         return false;
     eb_mark_device(A);

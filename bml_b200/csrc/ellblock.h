@@ -25,6 +25,11 @@ void *eb_get_element(bml_matrix_ellblock_t *A, int i, int j);
 void *eb_get_row(bml_matrix_ellblock_t *A, int i);
 void *eb_get_diagonal(bml_matrix_ellblock_t *A);
 void eb_set_element(bml_matrix_ellblock_t *A, int i, int j, const void *value, bool append_new);
+void eb_set_row(bml_matrix_ellblock_t *A, int i, const void *row, double threshold);
+void eb_set_diagonal(bml_matrix_ellblock_t *A, const void *diagonal, double threshold);
+// Matrix Market coordinate I/O on the host mirror (the header is handled by the caller).
+bool eb_write_mm(bml_matrix_ellblock_t *A, FILE *f);
+bool eb_read_mm(bml_matrix_ellblock_t *A, FILE *f, long long ne, bool symmetric);
 // X2 = X*X on the tensor cores: FP16 hi/lo split, FP32 accumulation; blocks of 32.
 bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, double threshold, double *trace);
 bool eb_multiply_x2(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, double threshold,

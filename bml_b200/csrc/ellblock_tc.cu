@@ -1084,12 +1084,22 @@ extern "C" int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, dou
         bool ok = false, on_tc = false;
         if (!closing)
         {
+            // Blocks other than 32 x 32, or a group beyond the tensor-core
+            // kernel's capacities, are an expected outcome here: that
+            // iteration runs on the exact product, noted as information.
+            const int verbose = b200_swap_verbose(0);
             ok = on_tc = eb_multiply_x2_tc(static_cast<bml_matrix_ellblock_t *>(D),
                                            static_cast<bml_matrix_ellblock_t *>(X2), threshold, tr);
-            // blocks other than 32 x 32, or a group beyond the tensor-core
-            // kernel's capacities: this iteration on the exact product
+            b200_swap_verbose(verbose);
             if (!on_tc && b200_get_error() == BML_B200_ERR_UNSUPPORTED)
+            {
                 bml_b200_clear_error();
+                if (verbose)
+                    fprintf(stderr, "[bml_b200 info] ellblock_sp2_mixed: iteration %d runs on the exact block "
+                                    "product (outside the tensor-core kernel's capacities)\n", it);
+            }
+            else if (!on_tc)
+                b200_set_error(b200_get_error(), "ellblock_sp2_mixed: tensor-core X^2 failed in iteration %d", it);
         }
         if (closing || (!on_tc && !bml_b200_last_error()))
             ok = eb_multiply_x2(static_cast<bml_matrix_ellblock_t *>(D), static_cast<bml_matrix_ellblock_t *>(X2),

@@ -18,6 +18,7 @@
 // and give wrong results; calls on one stream run one after the other.
 #include "device_util.cuh"
 
+#include <atomic>
 #include <mutex>
 
 #define B200_NOALLOC_MAX_ROWS (1 << 19)
@@ -28,7 +29,8 @@ static __device__ __align__(256) double g_noalloc_rows[B200_NOALLOC_MAX_ROWS];
 
 // Device address of g_noalloc_rows per device ordinal, found once per device.
 constexpr int kMaxDevices = 64;
-double *g_noalloc_ptr[kMaxDevices] = {nullptr};
+// published with release order under the mutex, read with acquire order
+std::atomic<double *> g_noalloc_ptr[kMaxDevices] = {};
 std::mutex g_noalloc_mutex;
 
 // Value of the first diagonal entry of each row (the reference's
@@ -104,13 +106,13 @@ extern "C" int bml_b200_ellpack_trace_noalloc(const void *d_value, const int *d_
         b200_set_error(BML_B200_ERR_INVALID, "ellpack_trace_noalloc: device %d", dev);
         return BML_B200_ERR_INVALID;
     }
-    double *rows = g_noalloc_ptr[dev];
+    double *rows = g_noalloc_ptr[dev].load(std::memory_order_acquire);
     if (!rows)
     {
         // First call on this device (with it current): host code cannot use
         // the array's name as a device address, so look the address up.
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev])
+        if (!g_noalloc_ptr[dev].load(std::memory_order_relaxed))
         {
             void *p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_rows);
@@ -120,9 +122,9 @@ extern "C" int bml_b200_ellpack_trace_noalloc(const void *d_value, const int *d_
                                cudaGetErrorString(e));
                 return BML_B200_ERR_CUDA;
             }
-            g_noalloc_ptr[dev] = static_cast<double *>(p);
+            g_noalloc_ptr[dev].store(static_cast<double *>(p), std::memory_order_release);
         }
-        rows = g_noalloc_ptr[dev];
+        rows = g_noalloc_ptr[dev].load(std::memory_order_relaxed);
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (N > 0)

@@ -18,6 +18,14 @@ Fixtures (numpy .npz):
                    N=24, and the dense form of its X^2 at threshold 0.
   generators.json  sha256 of the chain (N=4096, M=128) and 40^3 lattice
                    (radius 3, M=256) generator outputs, seed 0.
+  hamiltonian600.npz  the reference's example Hamiltonian
+                   (examples/example1/hamiltonian.dat: N=600, dense, read as
+                   examples/example1/main.f90 reads it) imported by the
+                   reference into ELLPACK at threshold 0.05 with M=64 (the
+                   example converts at 0.05): value, index, nnz.  The tests
+                   run the reference library itself on it for the products.
+                   `python tests/golden/make_golden.py hamiltonian` writes
+                   only this file (it needs the reference's source tree).
 """
 import ctypes as C
 import hashlib
@@ -111,5 +119,24 @@ def main():
     print("golden fixtures written")
 
 
+def hamiltonian():
+    ref_dir = os.environ.get("BML_REFERENCE_DIR", "/root/reference")
+    raw = np.loadtxt(os.path.join(ref_dir, "examples", "example1", "hamiltonian.dat"))
+    n = int(raw[0])
+    H = np.ascontiguousarray(raw[1:].reshape(n, n))  # read(1,*) H(i,j), j fastest
+    lib = O.ref()
+    M = 64
+    A = lib.bml_import_from_dense(2, 2, 0, n, M, H.ctypes.data_as(C.c_void_p), 0.05, 0)
+    h = O.ref_ellpack_arrays(A)
+    out = {"value": h[0], "index": h[1], "nnz": h[2], "N": n, "M": M}
+    O.ref_free(A)
+    np.savez_compressed(os.path.join(HERE, "hamiltonian600.npz"), **out)
+    print("hamiltonian600.npz written")
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["hamiltonian"]:
+        hamiltonian()
+    else:
+        main()
+        hamiltonian()

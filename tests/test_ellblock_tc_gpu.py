@@ -98,6 +98,74 @@ def test_tc_x2_matches_block_product(prec, L, radius):
         B.lib.bml_b200_reset_block_sizes()
 
 
+def _fp64_block_x2(H, nb, thr, bs=32):
+    """FP64 oracle of the ELLBLOCK X^2: the dense product H H in FP64 (torch,
+    on the GPU), restricted to the structural block pattern of the product
+    and to the reference's block keep rule (block (ib, kb) kept when kb == ib
+    or its max-norm exceeds thr, ellblock/bml_multiply_ellblock_typed.c:
+    406-408).  Also returns S = |H| |H|, the product magnitudes."""
+    import torch
+    dev = torch.device("cuda")
+    Ht = torch.from_numpy(H).to(dev)
+    P = (Ht.reshape(nb, bs, nb, bs).abs().amax(dim=(1, 3)) > 0).to(torch.float64)
+    pattern = (P @ P) > 0
+    X2 = Ht @ Ht
+    S = Ht.abs() @ Ht.abs()
+    del Ht
+    norm = X2.reshape(nb, bs, nb, bs).abs().amax(dim=(1, 3))
+    keep = pattern & ((norm > thr) | torch.eye(nb, dtype=torch.bool, device=dev))
+    mask = keep[:, None, :, None].expand(nb, bs, nb, bs).reshape(nb * bs, nb * bs)
+    X2 = torch.where(mask, X2, torch.zeros((), dtype=torch.float64, device=dev))
+    return X2, S, keep
+
+
+# Bound: the FP16 hi/lo split holds every entry to about 2^-22 of its size,
+# and the tensor cores accumulate in FP32, so an entry of X^2 carries an error
+# of a few 2^-24 of its product magnitude sum S = (|H| |H|)_ik for each of the
+# up to 32 * 57 terms summed; asserted: |X2_tc - X2_fp64| <= 2e-5 * S.  A block
+# that one side keeps and the other drops has its max-norm within that error of
+# the threshold.
+TC_EPS = 2e-5
+
+
+@pytest.mark.parametrize("L,radius", [(3, 1.0), (4, 2.0), (6, 2.24), (10, 2.0)])
+def test_tc_x2_against_fp64_dense(L, radius):
+    import torch
+    thr = 1e-6
+    H = block_lattice(L, radius)
+    nb, N = L ** 3, H.shape[0]
+    set_partition(nb, 257 if L == 10 else nb)
+    try:
+        X = from_dense(H)
+        Xt = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+        B.check()
+        trt = (C.c_double * 2)()
+        st = B.lib.bml_b200_ellblock_multiply_x2_tc(X, Xt, thr, trt)
+        assert st == B.OK, B.lib.bml_b200_error_string(st)
+        want, S, keep = _fp64_block_x2(H, nb, thr)
+        got = torch.from_numpy(to_dense(Xt, N)).to(want.device)
+        gkeep = got.reshape(nb, 32, nb, 32).abs().amax(dim=(1, 3)) > 0
+        both = (gkeep & keep)[:, None, :, None].expand(nb, 32, nb, 32).reshape(N, N)
+        err = torch.where(both, (got - want).abs(), torch.zeros((), dtype=torch.float64, device=want.device))
+        ratio = float((err / S.clamp_min(1e-300)).max())
+        rel_to_max = float(err.max() / want.abs().max())
+        print("tc X^2 %d^3: max |err|/S %.2e, max |err|/max|X2| %.2e" % (L, ratio, rel_to_max))
+        assert ratio <= TC_EPS
+        differ = gkeep ^ keep
+        if bool(differ.any()):
+            # blocks kept by one side only: their max-norm sits at the threshold
+            norm = want.reshape(nb, 32, nb, 32).abs().amax(dim=(1, 3))
+            smax = S.reshape(nb, 32, nb, 32).amax(dim=(1, 3))
+            assert bool(((norm[differ] - thr).abs() <= TC_EPS * smax[differ]).all())
+        assert trt[1] == pytest.approx(float(torch.trace(want)), rel=TC_EPS)
+        for h in (X, Xt):
+            free(h)
+        del want, S, got, err
+        torch.cuda.empty_cache()
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
+
+
 def test_tc_rejects_other_block_sizes():
     set_partition(16, 16, bs=8)
     try:
