@@ -123,6 +123,8 @@ _PROTOS = {
     "bml_b200_last_tier_counts": (_i, [_ip, _i]),
     "bml_b200_set_x2_tiers": (_i, [_i]),
     "bml_b200_set_x2_exact": (_i, [_i]),
+    "bml_b200_set_x2_symmetric": (_i, [_i]),
+    "bml_b200_last_x2_symmetric": (_i, []),
     "bml_getNRanks": (_i, []),
     "bml_getMyRank": (_i, []),
     "bml_printRank": (_i, []),

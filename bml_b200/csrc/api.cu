@@ -362,6 +362,14 @@ bml_matrix_t *bml_convert(bml_matrix_t *A, bml_matrix_type_t matrix_type,
         }
         return B;
     }
+    // ELLPACK <-> ELLBLOCK on the device, without a dense copy
+    if (type_of(A) == ellpack && matrix_type == ellblock && real_prec(matrix_precision))
+    {
+        bml_matrix_ellpack_t *E = as_ell(A, "convert");
+        return E ? eb_from_ellpack(E, matrix_precision, M, distrib_mode) : nullptr;
+    }
+    if (type_of(A) == ellblock && matrix_type == ellpack && real_prec(matrix_precision))
+        return ell_from_ellblock(static_cast<bml_matrix_ellblock_t *>(A), matrix_precision, M, distrib_mode);
     // Other types through a dense copy, as the reference does
     // (bml_convert.c:20-63).
     void *D = bml_export_to_dense(A, dense_row_major);

@@ -2205,6 +2205,319 @@ bool eb_normalize(bml_matrix_ellblock_t *A, double mineval, double maxeval)
            eb_add_identity(A, maxeval / mm, 0.0);
 }
 
+// ---------------------------------------------------------------------------
+// ELLPACK <-> ELLBLOCK on the device (bml_convert,
+// ellblock/bml_convert_ellblock_typed.c:16-73, ellpack/bml_convert_ellpack_typed.c:13-36).
+// The reference builds the ELLBLOCK matrix with every one of the NB x NB
+// blocks, filled element by element through bml_get_element; here each
+// block row holds the blocks its rows have entries in, in ascending block
+// column, with the same values (the dense forms are identical), and the
+// slots per block row are sized to the widest block row.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Block columns touched by the rows of block row ib, as a bitmap over NB in
+// shared memory (NB/32 words); one CTA per block row.
+// Entries with a column outside [0, N) or a row length outside [0, ldE]
+// raise *bad and are skipped.
+template <typename Tin>
+__device__ void conv_bitmap(const int *En, const int *Ei, int ldE, int N, const int *colblk, int r0, int r1,
+                            unsigned *bits, int words, int *bad)
+{
+    for (int w = threadIdx.x; w < words; w += blockDim.x)
+        bits[w] = 0u;
+    __syncthreads();
+    for (int i = r0; i < r1; ++i)
+    {
+        const int n = En[i];
+        if (n < 0 || n > ldE)
+        {
+            *bad = 1;
+            continue;
+        }
+        for (int p = threadIdx.x; p < n; p += blockDim.x)
+        {
+            const int j = Ei[(size_t) i * ldE + p];
+            if (j < 0 || j >= N)
+            {
+                *bad = 1;
+                continue;
+            }
+            const int jb = colblk[j];
+            atomicOr(&bits[jb >> 5], 1u << (jb & 31));
+        }
+    }
+    __syncthreads();
+}
+
+template <typename Tin>
+__global__ void __launch_bounds__(256) conv_count_kernel(const int *En, const int *Ei, int ldE, int N,
+                                                         const int *colblk, const int *boff, int NB, int *maxcnt)
+{
+    extern __shared__ unsigned bits[];
+    const int words = (NB + 31) >> 5;
+    __shared__ int cnt;
+    for (int ib = blockIdx.x; ib < NB; ib += gridDim.x)
+    {
+        conv_bitmap<Tin>(En, Ei, ldE, N, colblk, boff[ib], boff[ib + 1], bits, words, maxcnt + 1);
+        if (threadIdx.x == 0)
+            cnt = 0;
+        __syncthreads();
+        int c = 0;
+        for (int w = threadIdx.x; w < words; w += blockDim.x)
+            c += __popc(bits[w]);
+        atomicAdd(&cnt, c);
+        __syncthreads();
+        if (threadIdx.x == 0)
+            atomicMax(maxcnt, cnt);
+        __syncthreads();
+    }
+}
+
+// Slots in ascending block column (rank = popcount prefix of the bitmap),
+// then every entry written into its block (the pool starts zeroed).
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(256) conv_fill_kernel(const Tin *Ev, const int *Ei, const int *En, int ldE, int N,
+                                                        const int *colblk, EbView<Tout> B, int *bad)
+{
+    extern __shared__ unsigned bits[];
+    const int words = (B.NB + 31) >> 5;
+    int *pre = reinterpret_cast<int *>(bits + words); // prefix popcounts per word
+    for (int ib = blockIdx.x; ib < B.NB; ib += gridDim.x)
+    {
+        const int r0 = B.boff[ib], r1 = B.boff[ib + 1];
+        conv_bitmap<Tin>(En, Ei, ldE, N, colblk, r0, r1, bits, words, bad);
+        if (threadIdx.x == 0)
+        {
+            int run = 0;
+            for (int w = 0; w < words; ++w)
+            {
+                pre[w] = run;
+                run += __popc(bits[w]);
+            }
+            B.nnzb[ib] = run;
+        }
+        __syncthreads();
+        for (int w = threadIdx.x; w < words; w += blockDim.x)
+        {
+            unsigned m = bits[w];
+            int r = pre[w];
+            while (m)
+            {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                B.indexb[(size_t) ib * B.MB + r++] = w * 32 + b;
+            }
+        }
+        for (int i = r0; i < r1; ++i)
+        {
+            const int n = En[i];
+            const int ii = i - r0;
+            if (n < 0 || n > ldE)
+                continue;
+            for (int p = threadIdx.x; p < n; p += blockDim.x)
+            {
+                const int j = Ei[(size_t) i * ldE + p];
+                if (j < 0 || j >= N)
+                    continue;
+                const int jb = colblk[j];
+                const int w = jb >> 5;
+                const int rank = pre[w] + __popc(bits[w] & ((1u << (jb & 31)) - 1u));
+                Tout *blk = B.blk(ib, rank);
+                blk[ii * B.bsize[jb] + (j - B.boff[jb])] = (Tout) Ev[(size_t) i * ldE + p];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ELLBLOCK -> ELLPACK: row i takes the nonzero elements of its block row's
+// row ii, blocks in list order; one warp per scalar row.  Counts only when
+// `count` (the widest row into *maxw).
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(256) conv_back_kernel(EbView<Tin> A, const int *rowblk, Tout *Ev, int *Ei, int *En,
+                                                        int ldE, int M, int N, int count, int *maxw)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const int ib = rowblk[i];
+        const int ii = i - A.boff[ib];
+        int n = 0;
+        for (int jp = 0; jp < A.nnzb[ib]; ++jp)
+        {
+            const int jb = A.indexb[(size_t) ib * A.MB + jp];
+            const int bs = A.bsize[jb];
+            const Tin *row = A.blk(ib, jp) + (size_t) ii * bs;
+            for (int b = 0; b < bs; b += 32)
+            {
+                const int jj = b + lane;
+                const Tin v = jj < bs ? row[jj] : Tin(0);
+                const bool keep = jj < bs && v != Tin(0);
+                const unsigned bal = __ballot_sync(FULL, keep);
+                const int pos = n + __popc(bal & lanemask_lt());
+                if (!count && keep && pos < M)
+                {
+                    Ei[(size_t) i * ldE + pos] = A.boff[jb] + jj;
+                    Ev[(size_t) i * ldE + pos] = (Tout) v;
+                }
+                n += __popc(bal);
+            }
+        }
+        if (lane == 0)
+        {
+            atomicMax(maxw, n);
+            if (!count)
+                En[i] = min(n, M);
+        }
+    }
+}
+
+template <typename Tin, typename Tout>
+bool conv_fill(B200Context *c, bml_matrix_ellpack_t *E, const int *colblk, bml_matrix_ellblock_t *B, size_t smem)
+{
+    const int grid = max(1, min(B->NB, c->sm_count * 4));
+    conv_fill_kernel<Tin, Tout><<<grid, 256, smem, c->stream>>>(static_cast<const Tin *>(E->d_value), E->d_index,
+                                                                E->d_nnz, E->ld, E->N, colblk, view<Tout>(B),
+                                                                eb_flags(c) + 1);
+    return LAUNCH_OK("conv_fill_kernel");
+}
+
+} // namespace
+
+bml_matrix_ellblock_t *eb_from_ellpack(bml_matrix_ellpack_t *E, bml_matrix_precision_t prec, int M,
+                                       bml_distribution_mode_t mode)
+{
+    B200Context *c = b200_ctx();
+    if (!c || !ell_to_device(E))
+        return nullptr;
+    const int N = E->N;
+    int *bsize = bml_get_block_sizes(N, M);
+    const int NB = bml_get_nb();
+    std::vector<int> colblk(N), boff(NB + 1, 0);
+    for (int ib = 0; ib < NB; ++ib)
+    {
+        boff[ib + 1] = boff[ib] + bsize[ib];
+        for (int r = boff[ib]; r < boff[ib + 1] && r < N; ++r)
+            colblk[r] = ib;
+    }
+    if (boff[NB] != N)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "convert: the block sizes sum to %d, N=%d", boff[NB], N);
+        return nullptr;
+    }
+    const size_t words = (size_t) (NB + 31) / 32;
+    const size_t smem = words * (sizeof(unsigned) + sizeof(int));
+    if (smem > c->smem_optin)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "convert: NB=%d block columns", NB);
+        return nullptr;
+    }
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch((size_t) (N + NB + 1) * sizeof(int) + 256));
+    int *f = eb_flags(c);
+    if (!scr || !f)
+        return nullptr;
+    int *dcolblk = reinterpret_cast<int *>(scr);
+    int *dboff = dcolblk + N;
+    if (!CUDA_OK(cudaMemcpyAsync(dcolblk, colblk.data(), sizeof(int) * N, cudaMemcpyHostToDevice, c->stream)) ||
+        !CUDA_OK(cudaMemcpyAsync(dboff, boff.data(), sizeof(int) * (NB + 1), cudaMemcpyHostToDevice, c->stream)))
+        return nullptr;
+    for (auto kern : {conv_count_kernel<double>})
+        if (!CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+            return nullptr;
+    conv_count_kernel<double><<<max(1, min(NB, c->sm_count * 4)), 256, smem, c->stream>>>(
+        E->d_nnz, E->d_index, E->ld, N, dcolblk, dboff, NB, f);
+    int hf[2] = {0, 0};
+    if (!LAUNCH_OK("conv_count_kernel") || !eb_read_flags(c, f, hf, 2))
+        return nullptr;
+    if (hf[1])
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "convert: a column index or row length out of range");
+        return nullptr;
+    }
+    const int maxcnt = hf[0];
+    int MB = maxcnt > 0 ? maxcnt : 1;
+    const int mb_state = bml_get_mb();
+    if (mb_state > MB)
+        MB = mb_state < NB ? mb_state : NB;
+    bml_matrix_ellblock_t *B = eb_alloc_blocks(prec, NB, MB, M, bsize, mode);
+    if (!B)
+        return nullptr;
+    bool ok;
+    const bool din = E->matrix_precision == double_real, dout = prec == double_real;
+    auto set_smem = [&](auto kern) {
+        return CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    };
+    if (din && dout)
+        ok = set_smem(conv_fill_kernel<double, double>) && conv_fill<double, double>(c, E, dcolblk, B, smem);
+    else if (din)
+        ok = set_smem(conv_fill_kernel<double, float>) && conv_fill<double, float>(c, E, dcolblk, B, smem);
+    else if (dout)
+        ok = set_smem(conv_fill_kernel<float, double>) && conv_fill<float, double>(c, E, dcolblk, B, smem);
+    else
+        ok = set_smem(conv_fill_kernel<float, float>) && conv_fill<float, float>(c, E, dcolblk, B, smem);
+    if (!ok)
+    {
+        eb_free(B);
+        return nullptr;
+    }
+    eb_mark_device(B);
+    return B;
+}
+
+bml_matrix_ellpack_t *ell_from_ellblock(bml_matrix_ellblock_t *A, bml_matrix_precision_t prec, int M,
+                                        bml_distribution_mode_t mode)
+{
+    B200Context *c = b200_ctx();
+    if (!c || !eb_to_device(A))
+        return nullptr;
+    const int N = A->N;
+    std::vector<int> rowblk(N);
+    for (int ib = 0, r = 0; ib < A->NB; ++ib)
+        for (int k = 0; k < A->bsize[ib]; ++k)
+            rowblk[r++] = ib;
+    int *drowblk = static_cast<int *>(b200_scratch(sizeof(int) * (size_t) N + 256));
+    int *f = eb_flags(c);
+    if (!drowblk || !f ||
+        !CUDA_OK(cudaMemcpyAsync(drowblk, rowblk.data(), sizeof(int) * N, cudaMemcpyHostToDevice, c->stream)))
+        return nullptr;
+    bml_matrix_ellpack_t *E = ell_alloc(prec, N, M, mode, true);
+    if (!E)
+        return nullptr;
+    const int grid = max(1, min(b200_ceil_div(N, 8), c->sm_count * 16));
+    const bool din = A->matrix_precision == double_real, dout = prec == double_real;
+    auto launch = [&](int count) {
+        if (din && dout)
+            conv_back_kernel<double, double><<<grid, 256, 0, c->stream>>>(
+                view<double>(A), drowblk, static_cast<double *>(E->d_value), E->d_index, E->d_nnz, E->ld, E->M, N,
+                count, f);
+        else if (din)
+            conv_back_kernel<double, float><<<grid, 256, 0, c->stream>>>(
+                view<double>(A), drowblk, static_cast<float *>(E->d_value), E->d_index, E->d_nnz, E->ld, E->M, N,
+                count, f);
+        else if (dout)
+            conv_back_kernel<float, double><<<grid, 256, 0, c->stream>>>(
+                view<float>(A), drowblk, static_cast<double *>(E->d_value), E->d_index, E->d_nnz, E->ld, E->M, N,
+                count, f);
+        else
+            conv_back_kernel<float, float><<<grid, 256, 0, c->stream>>>(
+                view<float>(A), drowblk, static_cast<float *>(E->d_value), E->d_index, E->d_nnz, E->ld, E->M, N,
+                count, f);
+        return LAUNCH_OK("conv_back_kernel");
+    };
+    int maxw = 0;
+    if (!launch(0) || !eb_read_flags(c, f, &maxw, 1))
+    {
+        ell_free(E);
+        return nullptr;
+    }
+    ell_mark_device(E);
+    if (maxw > M)
+        b200_set_error(BML_B200_ERR_ROW_OVERFLOW, "convert: a row holds %d nonzeros, M=%d", maxw, M);
+    return E;
+}
+
 bml_matrix_ellblock_t *eb_import_dense(bml_matrix_precision_t prec, bml_dense_order_t order, int N, int M,
                                        void *D, double threshold, bml_distribution_mode_t mode)
 {

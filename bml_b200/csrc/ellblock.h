@@ -25,6 +25,11 @@ void *eb_get_element(bml_matrix_ellblock_t *A, int i, int j);
 void *eb_get_row(bml_matrix_ellblock_t *A, int i);
 void *eb_get_diagonal(bml_matrix_ellblock_t *A);
 void eb_set_element(bml_matrix_ellblock_t *A, int i, int j, const void *value, bool append_new);
+// Conversions between the formats on the device (values rounded to `prec`).
+bml_matrix_ellblock_t *eb_from_ellpack(bml_matrix_ellpack_t *E, bml_matrix_precision_t prec, int M,
+                                       bml_distribution_mode_t mode);
+bml_matrix_ellpack_t *ell_from_ellblock(bml_matrix_ellblock_t *A, bml_matrix_precision_t prec, int M,
+                                        bml_distribution_mode_t mode);
 void eb_set_row(bml_matrix_ellblock_t *A, int i, const void *row, double threshold);
 void eb_set_diagonal(bml_matrix_ellblock_t *A, const void *diagonal, double threshold);
 // Matrix Market coordinate I/O on the host mirror (the header is handled by the caller).

@@ -30,9 +30,25 @@
 // into a scratch copy by the prep kernel (bitonic sort in shared memory),
 // which also validates B; the product kernel reads each row of B through a
 // per-row offset that points into B or into that copy.
+//
+// Symmetric X^2.  When A == B and X is exactly symmetric (every entry has its
+// mirror with the same bits, checked on the device each call), X^2 is
+// symmetric and C[k,i] is formed from the same products as C[i,k].  The
+// product kernel then forms only columns k >= i of each row (about half the
+// products, and half the window), into a scratch matrix U; three small
+// kernels mirror U's strictly upper entries into the rows below (count per
+// row, scatter, then per row a sort of the mirrored part and a copy of the
+// upper part), so every row of C again lists its kept entries in ascending
+// column order.  The mirrored value is the same number as the upper one, so
+// C is exactly symmetric, and the keep rule, applied to each pair once, keeps
+// both or neither.  The SP2 iterates of a symmetric Hamiltonian stay exactly
+// symmetric (X0 = (emax I - H)/(emax - emin), 2X - X^2 and X^2 all map
+// mirrored pairs to equal values).  A matrix that is not symmetric takes the
+// full product; the decision is read on the device, so no host round trip.
 #include "device_util.cuh"
 
 #include <climits>
+#include <type_traits>
 #include <cstring>
 
 using namespace b200;
@@ -46,6 +62,7 @@ struct FastFlags
     int bad_input;  // a column index or row length out of range
     int unsorted;   // rows of B that were sorted into the scratch copy
     int next_row;   // row counter of the product kernel
+    int asym;       // the symmetry check found an entry without an equal mirror
 };
 
 struct FastArgs
@@ -62,7 +79,38 @@ struct FastArgs
     int ncols;
     int tile;                        // accumulator entries per tile
     int check_pre;                   // also report rows whose touched width > Mc (A*B)
+    int sym_try;                     // X^2 of a square matrix: use the symmetric form if X is symmetric
+    void *Uv; int *Ui; int *Un; int ldu; // upper parts of the rows (symmetric form)
+    int *lcnt; int *lfill;           // mirrored entries per row: count, and placement cursor
 };
+
+// Row j of B through its offset: B itself, or its sorted copy.
+template <typename T> struct RowView
+{
+    const int *k;
+    const T *v;
+};
+template <typename T> __device__ __forceinline__ RowView<T> row_of(const FastArgs &g, int j)
+{
+    const long long o = g.roff[j];
+    return o >= 0 ? RowView<T>{g.Bi + o, static_cast<const T *>(g.Bv) + o}
+                  : RowView<T>{g.Si + (-o - 1), static_cast<const T *>(g.Sv) + (-o - 1)};
+}
+
+// First position in the ascending k[0..n) holding a column >= c.
+__device__ __forceinline__ int lower_bound(const int *k, int n, int c)
+{
+    int lo = 0, hi = n;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(k + mid) < c)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
 
 // -------------------------------------------------------------------------
 // Prep: validate B, find its unsorted rows and sort them into the copy S.
@@ -156,6 +204,50 @@ __global__ void __launch_bounds__(PREP_T) fast_prep_kernel(FastArgs g, int p2, T
 }
 
 // -------------------------------------------------------------------------
+// Symmetry check of X (A == B): every entry (i, j, v) must have a mirror
+// (j, i) holding the same bits.  One warp per row, a binary search in the
+// (sorted view of the) mirror row per entry.
+// -------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) sym_check_kernel(FastArgs g)
+{
+    using Bits = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned>::type;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    if (g.flags->bad_input)
+        return;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < g.NB; i += warps)
+    {
+        if (*(volatile int *) &g.flags->asym)
+            return;
+        const int ni = g.Bn[i];
+        const RowView<T> r = row_of<T>(g, i);
+        int bad = 0;
+        for (int p = lane; p < ni; p += 32)
+        {
+            const int j = __ldg(r.k + p);
+            const RowView<T> m = row_of<T>(g, j);
+            const int nj = g.Bn[j];
+            const int q = lower_bound(m.k, nj, i);
+            const T a = __ldg(r.v + p);
+            if (q >= nj || __ldg(m.k + q) != i)
+                bad = 1;
+            else
+            {
+                const T b = __ldg(m.v + q);
+                Bits ba, bb;
+                memcpy(&ba, &a, sizeof(T));
+                memcpy(&bb, &b, sizeof(T));
+                if (ba != bb)
+                    bad = 1;
+            }
+        }
+        if (__any_sync(FULL, bad) && lane == 0)
+            atomicExch(&g.flags->asym, 1);
+    }
+}
+
+// -------------------------------------------------------------------------
 // Product kernel.
 // Shared memory: acc[tile] (T) | touched bits[tile/32] (TOUCH) | cur[lda] (int)
 // -------------------------------------------------------------------------
@@ -208,11 +300,16 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
     const T *Av = static_cast<const T *>(g.Av);
     const T *Bv = static_cast<const T *>(g.Bv);
     const T *Sv = static_cast<const T *>(g.Sv);
-    T *Cv = static_cast<T *>(g.Cv);
 
     // the prep kernel found an input out of range: touch nothing
     if (g.flags->bad_input)
         return;
+    // symmetric form: columns k >= i only, rows written to U (the check
+    // kernel has finished; every thread reads the same flag)
+    const bool sym = g.sym_try && !g.flags->asym;
+    T *outv = static_cast<T *>(sym ? g.Uv : g.Cv);
+    int *outi = sym ? g.Ui : g.Ci;
+    const size_t ldo = sym ? (size_t) g.ldu : (size_t) g.ldc;
     for (int c = threadIdx.x; c < tile; c += W * 32)
         acc[c] = T(0);
     if (TOUCH)
@@ -257,8 +354,19 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
                     const int nj = g.Bn[j];
                     if (nj <= 0)
                         continue;
-                    const long long o = g.roff[j];
-                    const int *ki = o >= 0 ? g.Bi + o : g.Si + (-o - 1);
+                    const int *ki = row_of<T>(g, j).k;
+                    if (sym)
+                    {
+                        // the part of row j at columns >= i
+                        const int q = lower_bound(ki, nj, i);
+                        cur[jp] = q;
+                        if (q < nj)
+                        {
+                            lo = i;
+                            hi = max(hi, ki[nj - 1]);
+                        }
+                        continue;
+                    }
                     lo = min(lo, ki[0]);
                     hi = max(hi, ki[nj - 1]);
                 }
@@ -316,7 +424,7 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
                     const long long o = __shfl_sync(FULL, mo, t);
                     const int *ki = o >= 0 ? g.Bi + o : g.Si + (-o - 1);
                     const T *kv = o >= 0 ? Bv + o : Sv + (-o - 1);
-                    int pos = multi ? cur[jp] : 0;
+                    int pos = (multi || sym) ? cur[jp] : 0;
                     while (pos < nj)
                     {
                         int k[U];
@@ -413,8 +521,8 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
                 const int pos = off + __popc(bal & lanemask_lt());
                 if (keep && pos < g.Mc)
                 {
-                    g.Ci[(size_t) i * g.ldc + pos] = c0 + c;
-                    Cv[(size_t) i * g.ldc + pos] = x;
+                    outi[(size_t) i * ldo + pos] = c0 + c;
+                    outv[(size_t) i * ldo + pos] = x;
                 }
                 off += __popc(bal);
             }
@@ -434,14 +542,150 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
         if (threadIdx.x == 0)
         {
             const int ll = ms.count;
-            g.Cn[i] = min(ll, g.Mc);
-            atomicMax(&g.flags->max_width, ll);
-            if (ll > g.Mc || (g.check_pre && ms.touched > g.Mc))
-                atomicExch(&g.flags->overflow, 1);
+            if (sym)
+                g.Un[i] = ll; // the mirror kernels complete the row
+            else
+            {
+                g.Cn[i] = min(ll, g.Mc);
+                atomicMax(&g.flags->max_width, ll);
+                if (ll > g.Mc || (g.check_pre && ms.touched > g.Mc))
+                    atomicExch(&g.flags->overflow, 1);
+            }
             if (g.dA)
                 g.dA[i] = ms.dA;
             if (g.dC)
                 g.dC[i] = ms.dC;
+        }
+        __syncthreads();
+    }
+}
+
+// -------------------------------------------------------------------------
+// Symmetric form, after the product kernel: mirror U's strictly upper kept
+// entries (k, i > k) into row i.  Each kernel returns at once when the
+// product kernel took the full form.
+// -------------------------------------------------------------------------
+__device__ __forceinline__ bool sym_on(const FastArgs &g)
+{
+    return !g.flags->bad_input && g.sym_try && !g.flags->asym;
+}
+
+// lcnt[i] = number of kept entries (k, i) with k < i; one warp per row k.
+__global__ void __launch_bounds__(256) sym_count_kernel(FastArgs g)
+{
+    if (!sym_on(g))
+        return;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < g.NA; k += warps)
+    {
+        const int n = min(g.Un[k], g.Mc);
+        for (int p = lane; p < n; p += 32)
+        {
+            const int i = g.Ui[(size_t) k * g.ldu + p];
+            if (i > k)
+                atomicAdd(&g.lcnt[i], 1);
+        }
+    }
+}
+
+// Scatter of the mirrored entries into the first lcnt[i] slots of row i of C
+// (in arrival order; the finish kernel sorts them).
+template <typename T>
+__global__ void __launch_bounds__(256) sym_place_kernel(FastArgs g)
+{
+    if (!sym_on(g))
+        return;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const T *Uv = static_cast<const T *>(g.Uv);
+    T *Cv = static_cast<T *>(g.Cv);
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < g.NA; k += warps)
+    {
+        const int n = min(g.Un[k], g.Mc);
+        for (int p = lane; p < n; p += 32)
+        {
+            const size_t at = (size_t) k * g.ldu + p;
+            const int i = g.Ui[at];
+            if (i <= k)
+                continue;
+            const int q = atomicAdd(&g.lfill[i], 1);
+            if (q < g.Mc)
+            {
+                g.Ci[(size_t) i * g.ldc + q] = k;
+                Cv[(size_t) i * g.ldc + q] = Uv[at];
+            }
+        }
+    }
+}
+
+// Row i of C: its mirrored part sorted by column (bitonic sort in shared
+// memory, padded with INT_MAX keys), then its upper part copied from U; the
+// row's width, overflow and the widest row are recorded.  One CTA of 256
+// threads per row (grid-stride); shared memory: vals[p2] | keys[p2], p2 the
+// power of two >= Mc.
+template <typename T>
+__global__ void __launch_bounds__(256) sym_finish_kernel(FastArgs g, int p2)
+{
+    if (!sym_on(g))
+        return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T *sv = reinterpret_cast<T *>(smem);
+    int *sk = reinterpret_cast<int *>(smem + (size_t) p2 * sizeof(T));
+    const T *Uv = static_cast<const T *>(g.Uv);
+    T *Cv = static_cast<T *>(g.Cv);
+    for (int i = blockIdx.x; i < g.NA; i += gridDim.x)
+    {
+        const int L = g.lcnt[i];
+        const int Lk = min(L, g.Mc);
+        const int total = L + g.Un[i];
+        const size_t crow = (size_t) i * g.ldc;
+        int n2 = 1;
+        while (n2 < Lk)
+            n2 <<= 1;
+        for (int p = threadIdx.x; p < n2; p += 256)
+        {
+            sk[p] = p < Lk ? g.Ci[crow + p] : INT_MAX;
+            sv[p] = p < Lk ? Cv[crow + p] : T(0);
+        }
+        __syncthreads();
+        for (int size = 2; size <= n2; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1)
+            {
+                for (int t = threadIdx.x; t < (n2 >> 1); t += 256)
+                {
+                    const int lo = 2 * t - (t & (stride - 1));
+                    const int hi = lo + stride;
+                    const bool up = (lo & size) == 0;
+                    const int klo = sk[lo], khi = sk[hi];
+                    if ((klo > khi) == up)
+                    {
+                        sk[lo] = khi;
+                        sk[hi] = klo;
+                        const T v = sv[lo];
+                        sv[lo] = sv[hi];
+                        sv[hi] = v;
+                    }
+                }
+                __syncthreads();
+            }
+        for (int p = threadIdx.x; p < Lk; p += 256)
+        {
+            g.Ci[crow + p] = sk[p];
+            Cv[crow + p] = sv[p];
+        }
+        const int nu = min(g.Un[i], g.Mc);
+        for (int p = threadIdx.x; p < nu && L + p < g.Mc; p += 256)
+        {
+            g.Ci[crow + L + p] = g.Ui[(size_t) i * g.ldu + p];
+            Cv[crow + L + p] = Uv[(size_t) i * g.ldu + p];
+        }
+        if (threadIdx.x == 0)
+        {
+            g.Cn[i] = min(total, g.Mc);
+            atomicMax(&g.flags->max_width, total);
+            if (total > g.Mc)
+                atomicExch(&g.flags->overflow, 1);
         }
         __syncthreads();
     }
@@ -466,6 +710,9 @@ constexpr int FX_W = B200_FX_W, FX_U = B200_FX_U, FX_MINB = B200_FX_MINB;
 constexpr size_t FX_SMALL = 16384;
 
 bool g_x2_exact = false;
+// The symmetric form of X^2 (on by default; off only to measure the full form).
+bool g_x2_symmetric = true;
+bool g_last_symmetric = false;
 
 // Dynamic shared memory a product CTA may take: its share of the SM's
 // 228 KiB (less the 1 KiB the SM reserves per CTA), within the per-block
@@ -490,13 +737,25 @@ bool fast_multiply_typed(FastArgs g, double *trace, int *required_M, bool touch)
     if (!c)
         return false;
     const int N = g.NA;
-    // scratch: roff[NB] | sorted copy of B (values, columns) | diag arrays
+    // the symmetric form's row sort holds a row of C in shared memory
+    int p2c = 1;
+    while (p2c < g.Mc)
+        p2c <<= 1;
+    const size_t smemF = (size_t) p2c * (sizeof(T) + sizeof(int));
+    if (touch || smemF > c->smem_optin)
+        g.sym_try = 0;
+    // scratch: roff[NB] | sorted copy of B (values, columns) | diag arrays |
+    // (symmetric form) U values, U columns, U widths, lcnt, lfill
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t nbe = (size_t) g.NB * g.ldb;
+    const size_t nue = g.sym_try ? (size_t) N * g.ldc : 0;
     const size_t off_sv = al((size_t) g.NB * sizeof(long long));
     const size_t off_si = al(off_sv + nbe * sizeof(T));
     const size_t off_diag = al(off_si + nbe * sizeof(int));
-    const size_t total = al(off_diag + (size_t) 2 * N * sizeof(double));
+    const size_t off_uv = al(off_diag + (size_t) 2 * N * sizeof(double));
+    const size_t off_ui = al(off_uv + nue * sizeof(T));
+    const size_t off_un = al(off_ui + nue * sizeof(int));
+    const size_t total = al(off_un + (g.sym_try ? (size_t) 3 * N * sizeof(int) : 0));
     unsigned char *scr = static_cast<unsigned char *>(b200_scratch(total));
     if (!scr)
         return false;
@@ -508,6 +767,17 @@ bool fast_multiply_typed(FastArgs g, double *trace, int *required_M, bool touch)
     g.Sv = Sv;
     g.Si = Si;
     g.roff = roff;
+    if (g.sym_try)
+    {
+        g.Uv = scr + off_uv;
+        g.Ui = reinterpret_cast<int *>(scr + off_ui);
+        g.Un = reinterpret_cast<int *>(scr + off_un);
+        g.lcnt = g.Un + N;
+        g.lfill = g.lcnt + N;
+        g.ldu = g.ldc;
+        if (!CUDA_OK(cudaMemsetAsync(g.lcnt, 0, (size_t) 2 * N * sizeof(int), c->stream)))
+            return false;
+    }
 
     unsigned char *small = static_cast<unsigned char *>(c->d_small) + FX_SMALL;
     FastFlags *flags = reinterpret_cast<FastFlags *>(small);
@@ -534,6 +804,13 @@ bool fast_multiply_typed(FastArgs g, double *trace, int *required_M, bool touch)
     fast_prep_kernel<T><<<pgrid, PREP_T, smemP, c->stream>>>(g, p2, Sv, Si, roff);
     if (!LAUNCH_OK("fast_prep_kernel"))
         return false;
+    const int wgrid = max(1, min(b200_ceil_div(N, 8), c->sm_count * 16));
+    if (g.sym_try)
+    {
+        sym_check_kernel<T><<<wgrid, 256, 0, c->stream>>>(g);
+        if (!LAUNCH_OK("sym_check_kernel"))
+            return false;
+    }
 
     // product kernel: the accumulator window takes the shared memory left
     // after the cursors (and the touched bitmap)
@@ -563,6 +840,23 @@ bool fast_multiply_typed(FastArgs g, double *trace, int *required_M, bool touch)
     kern<<<c->sm_count * occ, FX_W * 32, smemK, c->stream>>>(g);
     if (!LAUNCH_OK("fast_x2_kernel"))
         return false;
+    if (g.sym_try)
+    {
+        sym_count_kernel<<<wgrid, 256, 0, c->stream>>>(g);
+        if (!LAUNCH_OK("sym_count_kernel"))
+            return false;
+        sym_place_kernel<T><<<wgrid, 256, 0, c->stream>>>(g);
+        if (!LAUNCH_OK("sym_place_kernel"))
+            return false;
+        if (!CUDA_OK(cudaFuncSetAttribute(sym_finish_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int) smemF)))
+            return false;
+        int occF = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occF, sym_finish_kernel<T>, 256, smemF);
+        sym_finish_kernel<T><<<max(1, min(N, c->sm_count * max(occF, 1))), 256, smemF, c->stream>>>(g, p2c);
+        if (!LAUNCH_OK("sym_finish_kernel"))
+            return false;
+    }
     if (trace)
     {
         b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(diagA, diagC, N, dtrace);
@@ -576,6 +870,7 @@ bool fast_multiply_typed(FastArgs g, double *trace, int *required_M, bool touch)
         return false;
     const FastFlags *hf = reinterpret_cast<const FastFlags *>(pin);
     const double *ht = reinterpret_cast<const double *>(pin + 64);
+    g_last_symmetric = g.sym_try && !hf->asym && !hf->bad_input;
     if (required_M)
         *required_M = hf->max_width;
     if (hf->bad_input)
@@ -624,11 +919,28 @@ bool ell_multiply_unordered(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bm
     g.thr = threshold;
     g.check_pre = check_pre ? 1 : 0;
     g.ncols = B->N > C->N ? B->N : C->N;
+    // X^2 of a square matrix: the symmetric form runs if X proves symmetric
+    g.sym_try = (A == B && A->N == C->N && g_x2_symmetric) ? 1 : 0;
     // a touched-column bitmap is needed where untouched zeros could pass the
     // keep rule (threshold < 0 or NaN) or the pre-threshold width is checked
     const bool touch = check_pre || !(threshold >= 0.0);
     return A->matrix_precision == double_real ? fast_multiply_typed<double>(g, trace, required_M, touch)
                                               : fast_multiply_typed<float>(g, trace, required_M, touch);
+}
+
+// Allows (1, the default) or forbids (0) the symmetric form of the unordered
+// X^2; returns the previous setting.
+extern "C" BML_B200_API int bml_b200_set_x2_symmetric(int allow)
+{
+    const int old = g_x2_symmetric ? 1 : 0;
+    g_x2_symmetric = allow != 0;
+    return old;
+}
+
+// 1 when the last unordered product took the symmetric form.
+extern "C" BML_B200_API int bml_b200_last_x2_symmetric(void)
+{
+    return g_last_symmetric ? 1 : 0;
 }
 
 // Selects the ordered (bit-identical to the reference) or the unordered

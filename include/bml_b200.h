@@ -317,6 +317,16 @@ BML_B200_API int bml_b200_set_x2_tiers(int mask);
  * the ordered tiers.  Returns the previous choice.  No reference counterpart. */
 BML_B200_API int bml_b200_set_x2_exact(int exact);
 
+/* The unordered X^2 of an exactly symmetric matrix (each entry's mirror holds
+ * the same bits, checked on the device every call) forms only the columns
+ * k >= i of each row and mirrors them: half the products, the same result
+ * bound, and an exactly symmetric X^2.  set_x2_symmetric(0) forbids that form
+ * (the full product runs); returns the previous setting (default 1).
+ * last_x2_symmetric() is 1 when the last unordered product took it.  No
+ * reference counterpart. */
+BML_B200_API int bml_b200_set_x2_symmetric(int allow);
+BML_B200_API int bml_b200_last_x2_symmetric(void);
+
 /* Device-memory budget, in bytes, for the accumulator slabs of the exact
  * ELLBLOCK products (bml_multiply_x2, bml_multiply_AB, bml_multiply): every
  * CTA holds a slot for each block column a row can touch, NB of them, when

@@ -90,6 +90,7 @@ def ref():
             "bml_set_block_sizes": (None, [C.POINTER(i), i, i]),
             "bml_get_N": (i, [vp]),
             "bml_get_M": (i, [vp]),
+            "bml_convert": (vp, [vp, i, i, i, i]),
             "bml_write_bml_matrix": (None, [vp, C.c_char_p]),
             "bml_read_bml_matrix": (None, [vp, C.c_char_p]),
         }

@@ -9,7 +9,7 @@ checked against
     library) and differentiated by torch autograd; compared on H's pattern
     to 1e-8 relative to the largest entry;
   - central finite differences (step 1e-6) of the library's own forward
-    solve, on the entries with the largest gradients, to 1e-5 relative.
+    solve, on 32 entries, to 1e-6 relative.
 Checkpoint intervals of 1, 4 and the full count must give the same gradient."""
 import ctypes as C
 
@@ -142,18 +142,58 @@ def test_adjoint_matches_dense_autograd(iters, every):
     assert np.abs(g[mask] - ref_on_pattern).max() <= 1e-8 * scale
 
 
+def _loss_and_pattern(hv, ix, nz, vv, N, M, iters):
+    H = B.Ellpack.from_arrays(hv, ix, nz, N, M)
+    V = B.Ellpack.from_arrays(vv, ix, nz, N, M)
+    D = B.Ellpack(N, M)
+    info = (C.c_double * 6)()
+    assert B.lib.bml_b200_sp2(H.h, D.h, THR, N / 2.0, iters, -1.0, 0, info) == B.OK
+    val = B.lib.bml_trace_mult(D.h, V.h)
+    _, dix, dnz = D.download()
+    for m in (H, V, D):
+        m.free()
+    keys = set()
+    for i in range(N):
+        keys.update(i * N + c for c in dix[i * M:i * M + dnz[i]].tolist())
+    return val, keys
+
+
 def test_adjoint_matches_finite_differences():
+    """Central differences (step 1e-6, the differentiable configuration's
+    step) of the library's forward SP2 against the adjoint, to 1e-6
+    relative, on 32 entries of H's pattern: the 16 largest gradient entries
+    and 16 drawn at random.  The adjoint holds the thresholds fixed, so an
+    entry whose +-h perturbation moves the retained pattern of D (an entry
+    crossing the threshold, which makes L jump) is not compared; at most 4
+    of the 32 may be skipped so."""
     N, M, v, ix, nz, vv, _ = _problem(seed=1)
     iters, h = 10, 1e-6
     _, (g, _, _) = _loss_and_grad(v, ix, nz, vv, N, M, iters, 3)
     mask = np.flatnonzero((np.arange(M)[None, :] < nz[:, None]).reshape(-1))
-    picks = mask[np.argsort(-np.abs(g[mask]))[:8]]
+    top = mask[np.argsort(-np.abs(g[mask]))[:16]]
+    rest = np.setdiff1d(mask, top)
+    picks = np.concatenate([top, np.random.default_rng(5).choice(rest, 16, replace=False)])
+    _, base = _loss_and_pattern(v, ix, nz, vv, N, M, iters)
+    gscale = np.abs(g[mask]).max()
+    skipped, worst = 0, 0.0
     for q in picks:
         vp, vm = v.copy(), v.copy()
         vp[q] += h
         vm[q] -= h
-        fd = (_loss_only(vp, ix, nz, vv, N, M, iters) - _loss_only(vm, ix, nz, vv, N, M, iters)) / (2 * h)
-        assert fd == pytest.approx(g[q], rel=1e-5), (q, fd, g[q])
+        lp, pp = _loss_and_pattern(vp, ix, nz, vv, N, M, iters)
+        lm, pm = _loss_and_pattern(vm, ix, nz, vv, N, M, iters)
+        if pp != base or pm != base:
+            skipped += 1
+            continue
+        fd = (lp - lm) / (2 * h)
+        # relative to the entry, with a floor of 1e-3 of the largest entry
+        # for gradient entries near zero (where the differences' rounding,
+        # about 1e-16 |L| / h, would dominate)
+        err = abs(fd - g[q]) / max(abs(g[q]), 1e-3 * gscale)
+        worst = max(worst, err)
+        assert err <= 1e-6, (q, fd, g[q])
+    assert skipped <= 4, skipped
+    print("finite differences: worst relative error %.2e, %d of %d skipped" % (worst, skipped, len(picks)))
 
 
 def test_adjoint_single_precision_close_to_double():

@@ -250,3 +250,86 @@ def _dense(arr, N, M):
         n = nz[i]
         np.add.at(D[i], ix[i * M:i * M + n], v[i * M:i * M + n])
     return D
+
+
+def _dense_of(arrs, N, M):
+    v, ix, nz = arrs
+    D = np.zeros((N, N))
+    for i in range(N):
+        n = nz[i]
+        D[i, ix[i * M:i * M + n]] = v[i * M:i * M + n]
+    return D
+
+
+def test_x2_symmetric_form(oracle_mod):
+    """A symmetric X takes the symmetric form (upper half formed, mirrored):
+    the result is exactly symmetric, within the bound of the reference's,
+    and within the bound of the full form's."""
+    O = oracle_mod
+    N, M = 12 ** 3, 160
+    v, ix, nz = B.gen_lattice(12, 3, N, M, 0)
+    M2 = N
+    ref, tr_ref = _ref_x2(O, v, ix, nz, N, M, 1e-5, M2)
+    S = _absum(O, v, ix, nz, N, M, M2)
+    got, tr = _gpu_x2(v, ix, nz, N, M, M2, 1e-5)
+    assert B.lib.bml_b200_last_x2_symmetric() == 1
+    D = _dense_of(got, N, M2)
+    assert np.array_equal(D, D.T), "the symmetric form's X^2 is not exactly symmetric"
+    x2check.compare(got, ref, S, M2, M2, M2, 1e-5, 1e-12)
+    assert x2check.rows_sorted(got, M2)
+    old = B.lib.bml_b200_set_x2_symmetric(0)
+    try:
+        full, trf = _gpu_x2(v, ix, nz, N, M, M2, 1e-5)
+        assert B.lib.bml_b200_last_x2_symmetric() == 0
+    finally:
+        B.lib.bml_b200_set_x2_symmetric(old)
+    x2check.compare(got, full, S, M2, M2, M2, 1e-5, 1e-12)
+    assert tr[1] == pytest.approx(trf[1], rel=1e-12)
+
+
+def test_x2_nonsymmetric_input_takes_full_form(oracle_mod):
+    """One entry off its mirror by one ulp: the check finds it and the full
+    product runs, still within the bound of the reference's."""
+    O = oracle_mod
+    N, M = 12 ** 3, 160
+    v, ix, nz = B.gen_lattice(12, 3, N, M, 0)
+    v = v.copy()
+    v[100 * M + 5] = np.nextafter(v[100 * M + 5], np.inf)
+    M2 = N
+    ref, _ = _ref_x2(O, v, ix, nz, N, M, 1e-5, M2)
+    S = _absum(O, v, ix, nz, N, M, M2)
+    got, _ = _gpu_x2(v, ix, nz, N, M, M2, 1e-5)
+    assert B.lib.bml_b200_last_x2_symmetric() == 0
+    x2check.compare(got, ref, S, M2, M2, M2, 1e-5, 1e-12)
+
+
+def test_sp2_unordered_against_ordered():
+    """SP2 on the 12^3 lattice (threshold 1e-5, 12 iterations): the iterates
+    stay exactly symmetric, every X^2 takes the symmetric form, and the result
+    agrees with the ordered (reference-identical) solve: trace and band
+    energy to 1e-10 relative, ||D - D_ordered||_F / ||D_ordered||_F to 1e-9
+    (entries at the threshold may fall either way)."""
+    import ctypes as C
+    N, M = 12 ** 3, 12 ** 3
+    v, ix, nz = B.gen_lattice(12, 3, N, 160, 0)
+    pad = lambda a: np.pad(a.reshape(N, 160), ((0, 0), (0, M - 160))).reshape(-1)
+    H = B.Ellpack.from_arrays(pad(v), pad(ix), nz, N, M)
+    out = {}
+    for exact in (1, 0):
+        old = B.lib.bml_b200_set_x2_exact(exact)
+        try:
+            D = B.Ellpack(N, M)
+            info = (C.c_double * 6)()
+            assert B.lib.bml_b200_sp2(H.h, D.h, 1e-5, N / 2.0, 12, -1.0, 0, info) == B.OK
+            out[exact] = (D, list(info), B.lib.bml_b200_last_x2_symmetric())
+        finally:
+            B.lib.bml_b200_set_x2_exact(old)
+    (Do, io, _), (Du, iu, symu) = out[1], out[0]
+    assert symu == 1
+    Dd = _dense_of(Du.download(), N, M)
+    assert np.array_equal(Dd, Dd.T)
+    assert iu[2] == pytest.approx(io[2], rel=1e-10)
+    eo, eu = B.lib.bml_trace_mult(Do.h, H.h), B.lib.bml_trace_mult(Du.h, H.h)
+    assert eu == pytest.approx(eo, rel=1e-10)
+    assert B.lib.bml_fnorm2(Du.h, Do.h) <= 1e-9 * B.lib.bml_fnorm(Do.h)
+    B.check()
