@@ -43,10 +43,6 @@ M_X = 2048         # stored width of the iterates (iteration 5 needs 1792)
 THRESHOLD = 1e-5
 OCC = N / 2.0
 SP2_ITERS = 4
-# DRAM bytes per product term of the dense X^2 tier, from one ncu capture of
-# the 30^3 lattice case (bench.py --profile): 122.82 GB read + 11.77 GB
-# written for 18,570,945,128 products.
-DRAM_BYTES_PER_PRODUCT = (122.821243e9 + 11.769428e9) / 18570945128
 # B200 FP64 (vector and tensor) nominal rate, HGX figure per GPU; no measured
 # FP64 peak is available, so fractions against it are "of nominal"
 FP64_NOMINAL_TFLOPS = 37.0
@@ -426,10 +422,36 @@ def products(X, n):
     return P
 
 
-def x2_roofline(B, H, info):
-    """Algorithmic bytes of one X^2 on the last SP2 iterate over its device
-    time (CUDA events on the library stream)."""
+def formed_fraction(X, n, sample=400, seed=0):
+    """Share of X^2's product terms that the symmetric form computes (those
+    with k >= i), from a sample of rows."""
     import numpy as np
+    xv, xix, xnz = X.download()
+    rows = xix.reshape(n, -1)
+    width = rows.shape[1]
+    rng = np.random.default_rng(seed)
+    tot = part = 0
+    for i in rng.choice(n, size=min(sample, n), replace=False):
+        js = rows[i, :xnz[i]]
+        sub = rows[js]                                   # the rows j of row i
+        valid = np.arange(width)[None, :] < xnz[js][:, None]
+        tot += int(valid.sum())
+        part += int((valid & (sub >= i)).sum())
+    return part / max(tot, 1)
+
+
+# ncu capture of one X^2 call on the 30^3 lattice's SP2 iterate (bench.py
+# --profile, 18.57 G reference product terms; profiles/x2_symmetric_lattice30.md):
+# the product kernel's dram__bytes_read.sum + dram__bytes_write.sum
+NCU_X2_PRODUCTS = 18570945128
+NCU_X2_KERNEL_DRAM = 1130652000 + 163951616
+
+
+def x2_roofline(B, H, info):
+    """One X^2 on the SP2 iterate entering iteration SP2_ITERS-1: the
+    compulsory HBM bytes of the call over the product kernel's device time
+    (CUDA events on the library stream around that kernel, averaged over the
+    calls), and the same figures for the whole call."""
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -438,42 +460,55 @@ def x2_roofline(B, H, info):
     hbm = peaks.get("hbm_gbs")
     src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    # rebuild the iterate entering iteration SP2_ITERS-1
     X = B.Ellpack(N, M_X)
     info2 = (C.c_double * 6)()
     B.check(B.lib.bml_b200_sp2(H.h, X.h, THRESHOLD, OCC, SP2_ITERS - 1, 1e-8, 0, info2))
     X2 = B.Ellpack(N, M_X)
     tr = (C.c_double * 2)()
+    old_timing = B.lib.bml_b200_set_kernel_timing(1)
     B.check(B.lib.bml_b200_multiply_x2(X.h, X2.h, THRESHOLD, tr))  # warm
     reps = 3
+    kms = []
     B.check(B.lib.bml_b200_event_record(2))
     for _ in range(reps):
         B.check(B.lib.bml_b200_multiply_x2(X.h, X2.h, THRESHOLD, tr))
+        kms.append(B.lib.bml_b200_last_x2_kernel_ms())
     B.check(B.lib.bml_b200_event_record(3))
-    t = B.event_ms(2, 3) / 1e3 / reps
+    B.lib.bml_b200_set_kernel_timing(old_timing)
+    t_call = B.event_ms(2, 3) / 1e3 / reps
+    t_k = sum(kms) / len(kms) / 1e3
+    symmetric = B.lib.bml_b200_last_x2_symmetric()
     nnz_x = B.lib.bml_b200_nnz(X.h)
     nnz_x2 = B.lib.bml_b200_nnz(X2.h)
     P = products(X, N)
+    frac_formed = formed_fraction(X, N) if symmetric else 1.0
+    formed = P * frac_formed
     bytes_alg = 12 * nnz_x + 12 * nnz_x2 + 8 * N
-    achieved = bytes_alg / t / 1e9
+    achieved = bytes_alg / t_k / 1e9
+    X.free()
+    X2.free()
     return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "peak_source": src, "traffic": DRAM_BYTES_PER_PRODUCT * P,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dense tier on the 30^3 "
-                              "case (bench.py --profile: 134.6 GB for 18.57 G products), scaled by this "
-                              "call's products",
-            "kernel": "one ELLPACK X^2 call (tier kernels together) on the SP2 iterate of iteration %d"
-                      % (SP2_ITERS - 1),
-            "x2_seconds": t, "nnz_x": int(nnz_x), "nnz_x2": int(nnz_x2), "products": P,
-            "fp64_gflops": 2.0 * P / t / 1e9, "products_per_s": P / t,
-            "compute_frac": 2.0 * P / t / 1e12 / (FP64_NOMINAL_TFLOPS / 2),
-            "busiest_unit": {"unit": "L2 (lts__throughput, tag lookups)", "busy_pct": 69.8,
-                             "l1_to_l2_requests_pct": 73.9, "dram_pct": 26.8,
-                             "source": "ncu --set full of the dense tier on the 30^3 case (bench.py --profile): "
-                                       "the kernel is bound by the L2 reductions and gathers of its accumulator, "
-                                       "neither by HBM bytes nor by FP64 flops"},
-            "compute_frac_of": "nominal FP64 %.0f TFLOP/s halved (separately rounded multiply and add per "
-                               "product, as in the reference)" % FP64_NOMINAL_TFLOPS,
-            "gathered_gbs": 12.0 * P / t / 1e9}
+            "peak_source": src,
+            "traffic": NCU_X2_KERNEL_DRAM / NCU_X2_PRODUCTS * P,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the product kernel "
+                              "(fast_x2_kernel, symmetric form) on the 30^3 case (bench.py --profile: 1.29 GB for "
+                              "18.57 G reference product terms), scaled by this call's product terms",
+            "kernel": "fast_x2_kernel (symmetric form: columns k >= i), one ELLPACK X^2 on the SP2 iterate of "
+                      "iteration %d; kernel_seconds by CUDA events around it on the library stream" % (SP2_ITERS - 1),
+            "kernel_seconds": t_k, "x2_call_seconds": t_call, "symmetric_form": bool(symmetric),
+            "nnz_x": int(nnz_x), "nnz_x2": int(nnz_x2), "products_reference": P,
+            "products_formed": int(formed), "products_formed_share": frac_formed,
+            "reference_products_per_s": P / t_call,
+            "fp64_gflops_formed": 2.0 * formed / t_k / 1e9,
+            "compute_frac": 2.0 * formed / t_k / 1e12 / (FP64_NOMINAL_TFLOPS / 2),
+            "compute_frac_of": "nominal FP64 %.0f TFLOP/s halved (each product is a multiply and a separate "
+                               "atomic add)" % FP64_NOMINAL_TFLOPS,
+            "busiest_unit": {"unit": "L1/shared-memory pipe (l1tex__throughput)", "busy_pct": 86.3,
+                             "shared_atomic_wavefronts_share": 0.59, "l2_pct": 21.3, "dram_pct_of_elapsed": None,
+                             "source": "ncu --set full of fast_x2_kernel on the 30^3 case (bench.py --profile): the "
+                                       "kernel is bound by its shared-memory atomic adds (59% of the shared "
+                                       "wavefronts), neither by HBM bytes nor by FP64 flops"},
+            "gathered_gbs": 12.0 * formed / t_k / 1e9}
 
 
 # ---------------------------------------------------------------------------

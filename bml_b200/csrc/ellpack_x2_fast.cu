@@ -713,6 +713,11 @@ bool g_x2_exact = false;
 // The symmetric form of X^2 (on by default; off only to measure the full form).
 bool g_x2_symmetric = true;
 bool g_last_symmetric = false;
+// CUDA events around the product kernel (when timing is on), on the library
+// stream; the last duration in ms, or -1.
+bool g_time_kernel = false;
+cudaEvent_t g_kev[2] = {nullptr, nullptr};
+float g_last_kernel_ms = -1.0f;
 
 // Dynamic shared memory a product CTA may take: its share of the SM's
 // 228 KiB (less the 1 KiB the SM reserves per CTA), within the per-block
@@ -837,8 +842,14 @@ bool fast_multiply_typed(FastArgs g, double *trace, int *required_M, bool touch)
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply: the unordered kernel does not fit the device");
         return false;
     }
+    const bool timed = g_time_kernel && (g_kev[0] || (CUDA_OK(cudaEventCreate(&g_kev[0])) &&
+                                                        CUDA_OK(cudaEventCreate(&g_kev[1]))));
+    if (timed && !CUDA_OK(cudaEventRecord(g_kev[0], c->stream)))
+        return false;
     kern<<<c->sm_count * occ, FX_W * 32, smemK, c->stream>>>(g);
     if (!LAUNCH_OK("fast_x2_kernel"))
+        return false;
+    if (timed && !CUDA_OK(cudaEventRecord(g_kev[1], c->stream)))
         return false;
     if (g.sym_try)
     {
@@ -871,6 +882,9 @@ bool fast_multiply_typed(FastArgs g, double *trace, int *required_M, bool touch)
     const FastFlags *hf = reinterpret_cast<const FastFlags *>(pin);
     const double *ht = reinterpret_cast<const double *>(pin + 64);
     g_last_symmetric = g.sym_try && !hf->asym && !hf->bad_input;
+    g_last_kernel_ms = -1.0f;
+    if (timed && !CUDA_OK(cudaEventElapsedTime(&g_last_kernel_ms, g_kev[0], g_kev[1])))
+        return false;
     if (required_M)
         *required_M = hf->max_width;
     if (hf->bad_input)
@@ -935,6 +949,22 @@ extern "C" BML_B200_API int bml_b200_set_x2_symmetric(int allow)
     const int old = g_x2_symmetric ? 1 : 0;
     g_x2_symmetric = allow != 0;
     return old;
+}
+
+// Times the product kernel of later unordered products with CUDA events on
+// the library stream (on = 1); returns the previous setting.
+extern "C" BML_B200_API int bml_b200_set_kernel_timing(int on)
+{
+    const int old = g_time_kernel ? 1 : 0;
+    g_time_kernel = on != 0;
+    return old;
+}
+
+// Device time of the last unordered product's product kernel in ms (-1 when
+// it was not timed).
+extern "C" BML_B200_API double bml_b200_last_x2_kernel_ms(void)
+{
+    return (double) g_last_kernel_ms;
 }
 
 // 1 when the last unordered product took the symmetric form.

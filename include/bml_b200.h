@@ -327,6 +327,14 @@ BML_B200_API int bml_b200_set_x2_exact(int exact);
 BML_B200_API int bml_b200_set_x2_symmetric(int allow);
 BML_B200_API int bml_b200_last_x2_symmetric(void);
 
+/* Diagnostics: with set_kernel_timing(1), later unordered products time
+ * their product kernel (the kernel that forms and sums the products) with
+ * CUDA events on the library stream; last_x2_kernel_ms() returns that time
+ * for the last product, or -1.  set_kernel_timing returns the previous
+ * setting.  No reference counterpart. */
+BML_B200_API int bml_b200_set_kernel_timing(int on);
+BML_B200_API double bml_b200_last_x2_kernel_ms(void);
+
 /* Device-memory budget, in bytes, for the accumulator slabs of the exact
  * ELLBLOCK products (bml_multiply_x2, bml_multiply_AB, bml_multiply): every
  * CTA holds a slot for each block column a row can touch, NB of them, when
