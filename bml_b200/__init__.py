@@ -126,6 +126,8 @@ _PROTOS = {
     "bml_b200_set_x2_symmetric": (_i, [_i]),
     "bml_b200_last_x2_symmetric": (_i, []),
     "bml_b200_set_kernel_timing": (_i, [_i]),
+    "bml_b200_set_dense_tier": (_i, [_i]),
+    "bml_b200_last_x2_dense": (_i, []),
     "bml_b200_last_x2_kernel_ms": (_d, []),
     "bml_getNRanks": (_i, []),
     "bml_getMyRank": (_i, []),

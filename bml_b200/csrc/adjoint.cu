@@ -17,8 +17,10 @@
 // threshold, so no gradient reaches them).  The products are the library's
 // sparse products (threshold 0); the restrictions are one kernel.
 // Memory: X is checkpointed every `every` iterations in the forward pass and
-// each segment is recomputed (bit-identically) before its backward steps, so
-// at most K/every + every iterates are held.
+// each segment is recomputed before its backward steps (bit-identically with
+// the ordered products and on the dense tier; the unordered sparse products
+// may add in another order, so a recomputed iterate can differ from the first
+// pass in the last bits), so at most K/every + every iterates are held.
 // Finally dL/dH = -G_0/d + a * d(emax)/dH + b * d(emin)/dH, with d = emax -
 // emin, a = (tr G_0 - <G_0, X0>)/d and b = <G_0, X0>/d; emax = h_k + r_k of
 // its maximising row k (diagonal + sum of |off-diagonals|), so d(emax)/dH is

@@ -2586,12 +2586,20 @@ bool ell_multiply_AB(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matri
         return false;
     if (C->mirror == MIRROR_HOST_NEWER)
         C->mirror = MIRROR_SYNCED;
-    if (!ell_x2_exact() && ell_unordered_fits(A) && ell_unordered_fits(B))
+    if (!ell_x2_exact())
     {
-        const bool ok = ell_multiply_unordered(A, B, C, threshold, trace, required_M,
-                                               A != B && !x2_rows);
-        ell_mark_device(C);
-        return ok;
+        bool taken = false;
+        bool ok = ell_multiply_dense_tier(A, B, C, threshold, trace, required_M, &taken);
+        if (!taken && ell_unordered_fits(A) && ell_unordered_fits(B))
+        {
+            taken = true;
+            ok = ell_multiply_unordered(A, B, C, threshold, trace, required_M, A != B && !x2_rows);
+        }
+        if (taken)
+        {
+            ell_mark_device(C);
+            return ok;
+        }
     }
     MulArgs g{};
     g.Av = A->d_value; g.Ai = A->d_index; g.An = A->d_nnz; g.lda = A->ld; g.NA = A->N;

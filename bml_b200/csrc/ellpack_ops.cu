@@ -790,6 +790,14 @@ bool ell_add(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double alpha, dou
     const size_t smem = (size_t) (A->ld + B->ld) * (sz + 4) + ((size_t) 2 << logts) * 4 + 8 * 4 + 64;
     if (smem > c->smem_optin)
     {
+        // rows too wide for the hash: through a dense image of the row sums
+        // (unordered form; rows come out in ascending column order)
+        if (!ell_x2_exact() && threshold >= 0.0)
+        {
+            const bool ok = ell_add_wide(A, B, alpha, beta, threshold);
+            ell_mark_device(A);
+            return ok;
+        }
         b200_set_error(BML_B200_ERR_UNSUPPORTED, "add: rows of width %d/%d exceed shared memory",
                        A->M, B->M);
         return false;
@@ -1022,10 +1030,7 @@ bool ell_trace_mult(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *tr
         smem >>= 1;
     }
     if (smem > c->smem_optin)
-    {
-        b200_set_error(BML_B200_ERR_UNSUPPORTED, "trace_mult: B rows of width %d too wide", B->M);
-        return false;
-    }
+        return ell_trace_mult_wide(A, B, trace);
     const int grid = min(b200_ceil_div(A->N, warps_per_block), c->sm_count * 16);
     if (A->matrix_precision == double_real)
     {
@@ -1323,10 +1328,7 @@ bool ell_fnorm2(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *result
         ++logts;
     const size_t smem = (size_t) 4 * (1 << logts) * sizeof(int);
     if (smem > c->smem_optin)
-    {
-        b200_set_error(BML_B200_ERR_UNSUPPORTED, "fnorm2: rows of width %d are too wide", A->M);
-        return false;
-    }
+        return ell_fnorm2_wide(A, B, result);
     double *rows = static_cast<double *>(b200_scratch((size_t) A->N * sizeof(double)));
     if (!rows)
         return false;
@@ -1486,8 +1488,9 @@ bool ell_restrict(bml_matrix_ellpack_t *S, bml_matrix_ellpack_t *P, bml_matrix_e
     const size_t smem = (size_t) 2 * (1 << logts) * sizeof(int);
     if (smem > c->smem_optin)
     {
-        b200_set_error(BML_B200_ERR_UNSUPPORTED, "restrict: pattern rows of %d entries are too wide", maxrow);
-        return false;
+        const bool ok = ell_restrict_wide(S, P, O);
+        ell_mark_device(O);
+        return ok;
     }
     const int grid = max(1, min(S->N, c->sm_count * 8));
     if (S->matrix_precision == double_real)

@@ -713,6 +713,7 @@ bool g_x2_exact = false;
 // The symmetric form of X^2 (on by default; off only to measure the full form).
 bool g_x2_symmetric = true;
 bool g_last_symmetric = false;
+bool g_last_dense = false;
 // CUDA events around the product kernel (when timing is on), on the library
 // stream; the last duration in ms, or -1.
 bool g_time_kernel = false;
@@ -913,6 +914,21 @@ bool ell_x2_exact()
     return g_x2_exact;
 }
 
+// The dense tier, when the operands' rows fill in (its A*B width check counts
+// the nonzero entries of the product, which are the touched ones unless
+// products cancel to an exact zero).
+bool ell_multiply_dense_tier(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C,
+                             double threshold, double *trace, int *required_M, bool *taken)
+{
+    *taken = false;
+    if (!ell_dense_fits(A, B, C, threshold))
+        return false;
+    *taken = true;
+    g_last_symmetric = false;
+    g_last_dense = true;
+    return ell_multiply_dense(A, B, C, threshold, trace, required_M);
+}
+
 bool ell_unordered_fits(const bml_matrix_ellpack_t *A)
 {
     B200Context *c = b200_ctx();
@@ -926,6 +942,7 @@ bool ell_unordered_fits(const bml_matrix_ellpack_t *A)
 bool ell_multiply_unordered(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C,
                             double threshold, double *trace, int *required_M, bool check_pre)
 {
+    g_last_dense = false;
     FastArgs g{};
     g.Av = A->d_value; g.Ai = A->d_index; g.An = A->d_nnz; g.lda = A->ld; g.NA = A->N;
     g.Bv = B->d_value; g.Bi = B->d_index; g.Bn = B->d_nnz; g.ldb = B->ld; g.NB = B->N;
@@ -965,6 +982,12 @@ extern "C" BML_B200_API int bml_b200_set_kernel_timing(int on)
 extern "C" BML_B200_API double bml_b200_last_x2_kernel_ms(void)
 {
     return (double) g_last_kernel_ms;
+}
+
+// 1 when the last unordered product ran on the dense tier.
+extern "C" BML_B200_API int bml_b200_last_x2_dense(void)
+{
+    return g_last_dense ? 1 : 0;
 }
 
 // 1 when the last unordered product took the symmetric form.

@@ -148,6 +148,21 @@ bool ell_x2_exact();
 bool ell_unordered_fits(const bml_matrix_ellpack_t *A);
 bool ell_multiply_unordered(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C,
                             double threshold, double *trace, int *required_M, bool check_pre);
+// The dense tier of the unordered product (ellpack_dense.cu): a GEMM on dense
+// images when both operands' rows fill at least 40 % of their columns.
+bool ell_dense_fits(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C, double threshold);
+// Runs the dense tier when it applies (*taken); the result is the product's
+// status then.
+bool ell_multiply_dense_tier(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C,
+                             double threshold, double *trace, int *required_M, bool *taken);
+bool ell_multiply_dense(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C, double threshold,
+                        double *trace, int *required_M);
+// Wide-row forms (ellpack_wide.cu) of the operations whose shared-memory
+// hash cannot hold a row: through a dense image of one operand.
+bool ell_add_wide(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double alpha, double beta, double threshold);
+bool ell_trace_mult_wide(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *trace);
+bool ell_fnorm2_wide(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, double *result);
+bool ell_restrict_wide(bml_matrix_ellpack_t *S, bml_matrix_ellpack_t *P, bml_matrix_ellpack_t *O);
 // A view of rows [r0, r1) of A: the same storage, N = r1 - r0 (columns keep
 // their global numbering).  Operations on the view touch only those rows.
 bml_matrix_ellpack_t ell_row_view(const bml_matrix_ellpack_t *A, int r0, int r1);

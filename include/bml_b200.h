@@ -332,6 +332,15 @@ BML_B200_API int bml_b200_last_x2_symmetric(void);
  * CUDA events on the library stream; last_x2_kernel_ms() returns that time
  * for the last product, or -1.  set_kernel_timing returns the previous
  * setting.  No reference counterpart. */
+/* The dense tier of the unordered product: when both operands' rows fill at
+ * least 40 % of their columns on average (and the dense images fit 64 GiB),
+ * A and B are scattered into dense images, multiplied by a register-tiled
+ * GEMM and compacted with the same keep rule, rows in ascending column
+ * order.  set_dense_tier(0) forbids it (default 1; returns the previous
+ * setting); last_x2_dense() is 1 when the last unordered product ran on it.
+ * No reference counterpart. */
+BML_B200_API int bml_b200_set_dense_tier(int allow);
+BML_B200_API int bml_b200_last_x2_dense(void);
 BML_B200_API int bml_b200_set_kernel_timing(int on);
 BML_B200_API double bml_b200_last_x2_kernel_ms(void);
 
