@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--profile-eb", action="store_true",
                     help="run the small exact ELLBLOCK case for an ncu capture (10^3 block lattice)")
     ap.add_argument("--no-ellblock", action="store_true", help="skip the ELLBLOCK tensor-core leg")
+    ap.add_argument("--step-only", action="store_true",
+                    help="time the SP2 steps only (no e2e, roofline, mixed, chain, ELLBLOCK or CPU legs), for a "
+                         "launch-list capture; the timed steps run inside an NVTX range \"step\"")
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: 30^3 lattice, 3 SP2 iterations then one X^2")
     ap.add_argument("--profile-ops", action="store_true",
@@ -224,8 +227,11 @@ def run_b200(args, rank, world, local):
     launches0 = B.lib.bml_b200_launch_count()
     B.check(B.lib.bml_b200_event_record(0))
     step_ev = []
+    nvtx = _nvtx()
     for k in range(args.steps):
+        nvtx.range_push("step")
         step()
+        nvtx.range_pop()
         if k < 32:
             slot = 16 + k
             B.check(B.lib.bml_b200_event_record(slot))
@@ -239,6 +245,15 @@ def run_b200(args, rank, world, local):
     ms = max_over_ranks(ms)
     sec_per_step = ms / 1e3 / args.steps
     value = sec_per_step  # one solve, split over the ranks when world > 1
+    if args.step_only:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms,
+                "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "config": bench_config(world), "gpu_launches": int(B.lib.bml_b200_launch_count() - launches0),
+                "note": "--step-only: the SP2 steps alone"} if rank == 0 else None
 
     # end-to-end through the C ABI with host buffers
     barrier()
@@ -633,7 +648,10 @@ def run_profile_ops():
     B.check(B.lib.bml_b200_multiply_x2(X.h, X2.h, THRESHOLD, tr))
     nnz = lambda m: int(B.lib.bml_b200_nnz(m.h))
     n_x, n_x2 = nnz(X), nnz(X2)
-    # the operations, in launch order
+    # the operations, in launch order, inside an NVTX range "ops" (ncu
+    # --nvtx --nvtx-include "ops/" captures only these)
+    nvtx = _nvtx()
+    nvtx.range_push("ops")
     S = B.Ellpack(Np, Mp)
     B.lib.bml_copy(X.h, S.h)                       # copy_kernel: X -> S
     B.lib.bml_add(S.h, X2.h, 2.0, -1.0, THRESHOLD)  # add_kernel: S = 2 S - X2
@@ -649,11 +667,28 @@ def run_profile_ops():
     B.lib.bml_free_memory(eb)
     Xt = B.lib.bml_transpose_new(X2.h)             # transpose_scatter_kernel + row_sort_kernel
     B.check()
+    nvtx.range_pop()
     hh = C.c_void_p(Xt)
     B.lib.bml_deallocate(C.byref(hh))
     print(json.dumps({"profile_case": "one-pass ELLPACK operations on the 30^3 lattice's SP2 iterate X and X^2",
                       "N": Np, "M": Mp, "nnz_x": n_x, "nnz_x2": n_x2, "nnz_add": n_add, "nnz_threshold": n_thr,
                       "trace": trace}))
+
+
+def _nvtx():
+    """NVTX range markers (torch's bindings), for the ncu captures of the
+    profile cases; no-ops where torch has none."""
+    try:
+        import torch
+        return torch.cuda.nvtx
+    except (ImportError, AttributeError):
+        class _Nop:
+            def range_push(self, _):
+                pass
+
+            def range_pop(self):
+                pass
+        return _Nop()
 
 
 class _StdoutToStderr:
@@ -748,7 +783,9 @@ def run_profile_eb_ops(L=7):
     B.check()
     blocks = lambda h: int(B.lib.bml_b200_nnz(h)) // 1024
     n_h, n_x2 = blocks(H), blocks(X2)
-    # the operations, in launch order
+    # the operations, in launch order, inside an NVTX range "ops"
+    nvtx = _nvtx()
+    nvtx.range_push("ops")
     B.lib.bml_copy(X2, S)                                   # eb_copy_kernel: X2 -> S
     B.lib.bml_add(S, H, C.c_double(2.0), C.c_double(-1.0), C.c_double(1e-6))  # eb_add_kernel: S = 2 S - H
     n_add = blocks(S)
@@ -763,6 +800,7 @@ def run_profile_eb_ops(L=7):
     Xt = B.lib.bml_transpose_new(X2)                        # eb_transpose_kernel
     tm = B.lib.bml_trace_mult(X2, H)                        # eb_trace_mult_kernel
     B.check()
+    nvtx.range_pop()
     for h in (X2, S, T, Xt, H):
         hh = C.c_void_p(h)
         B.lib.bml_deallocate(C.byref(hh))

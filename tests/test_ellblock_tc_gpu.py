@@ -218,3 +218,31 @@ def test_ellblock_sp2_mixed_against_fp64():
         free(H)
     finally:
         B.lib.bml_b200_reset_block_sizes()
+
+
+@pytest.mark.xfail(reason="the tensor cores accumulate in FP32: the mixed ELLBLOCK SP2 is about 3e-5 from the "
+                          "exact solve in trace (5e-6 in band energy); FP64 folding of the partial tiles is not built",
+                   strict=False)
+def test_ellblock_sp2_mixed_meets_the_1e6_target():
+    """The mixed form's target (trace and band energy within 1e-6 of the
+    exact solve) on the 4^3 block lattice, 8 tensor-core + 2 exact
+    iterations: an expected failure while the accumulation is FP32."""
+    L, radius, iters, nclose, thr = 4, 2.0, 10, 2, 1e-6
+    Hd = block_lattice(L, radius, seed=3)
+    nb, N = L ** 3, Hd.shape[0]
+    set_partition(nb, nb)
+    try:
+        H = from_dense(Hd)
+        res = {}
+        for name, nc in (("exact", iters), ("mixed", nclose)):
+            D = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+            info = (C.c_double * 8)()
+            assert B.lib.bml_b200_ellblock_sp2_mixed(H, D, thr, N / 2.0, iters, -1.0, 0, nc, info) == B.OK
+            res[name] = to_dense(D, N)
+            free(D)
+        free(H)
+        De, Dm = res["exact"], res["mixed"]
+        assert abs(np.trace(Dm) - np.trace(De)) <= 1e-6 * abs(np.trace(De))
+        assert abs(np.sum(Dm * Hd.T) - np.sum(De * Hd.T)) <= 1e-6 * abs(np.sum(De * Hd.T))
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
