@@ -695,15 +695,18 @@ __global__ void __launch_bounds__(256) sym_finish_kernel(FastArgs g, int p2)
 
 namespace {
 
-// Warps per CTA and chunks in flight per lane of the product kernel.
+// Warps per CTA, chunks in flight per lane and CTAs per SM of the product
+// kernel.  Two CTAs of 16 warps with 8 chunks per lane were the fastest of
+// the shapes measured on the 30^3 lattice iterate (X^2 in 60.8 ms FP64,
+// 43.4 ms FP32; one CTA of 32 warps with 4 chunks: 63.4 and 52.1 ms).
 #ifndef B200_FX_W
-#define B200_FX_W 32
+#define B200_FX_W 16
 #endif
 #ifndef B200_FX_U
-#define B200_FX_U 4
+#define B200_FX_U 8
 #endif
 #ifndef B200_FX_MINB
-#define B200_FX_MINB 1
+#define B200_FX_MINB 2
 #endif
 constexpr int FX_W = B200_FX_W, FX_U = B200_FX_U, FX_MINB = B200_FX_MINB;
 // Offsets in the context's small device/pinned buffers.
