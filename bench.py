@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--profile-eb", action="store_true",
                     help="run the small exact ELLBLOCK case for an ncu capture (10^3 block lattice)")
     ap.add_argument("--no-ellblock", action="store_true", help="skip the ELLBLOCK tensor-core leg")
+    ap.add_argument("--exchange", default="gather", choices=["gather", "halo"],
+                    help="with --gpus > 1: all-gather the iterate after each update, or send each rank only "
+                         "the rows its next X^2 reads")
     ap.add_argument("--step-only", action="store_true",
                     help="time the SP2 steps only (no e2e, roofline, mixed, chain, ELLBLOCK or CPU legs), for a "
                          "launch-list capture; the timed steps run inside an NVTX range \"step\"")
@@ -142,12 +145,13 @@ def inputs():
     return B.gen_lattice(L, RADIUS, N, M_H, SEED)
 
 
-def bench_config(world):
+def bench_config(world, exchange="gather"):
     """The `config` object of the JSON line, the same in both arms."""
+    how = {"gather": "NCCL all-gather of the iterate",
+           "halo": "NCCL point-to-point rows within each rank's column range"}[exchange]
     return {"workload": WORKLOAD, "N": N, "M": M_X, "threshold": THRESHOLD,
             "sp2_iterations": SP2_ITERS,
-            "parallelism": ("rows sharded over %d GPUs (NCCL all-gather of the iterate)" % world)
-            if world > 1 else "1 GPU",
+            "parallelism": ("rows sharded over %d GPUs (%s)" % (world, how)) if world > 1 else "1 GPU",
             "l2": "inputs larger than L2 (iterates ~0.8-1.3 GB)"}
 
 
@@ -187,7 +191,7 @@ def run_b200(args, rank, world, local):
         # traces are summed and the new iterate's rows all-gathered (NCCL).
         from bml_b200.sharded import GpuOps, ShardedSP2
         ops = GpuOps(B.lib, H.h, M_X, THRESHOLD, pg, torch)
-        sharded = ShardedSP2(ops, pg, rank, world)
+        sharded = ShardedSP2(ops, pg, rank, world, args.exchange)
 
     def step():
         if sharded is not None:
@@ -252,7 +256,7 @@ def run_b200(args, rank, world, local):
         return {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms,
                 "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
-                "config": bench_config(world), "gpu_launches": int(B.lib.bml_b200_launch_count() - launches0),
+                "config": bench_config(world, args.exchange), "gpu_launches": int(B.lib.bml_b200_launch_count() - launches0),
                 "note": "--step-only: the SP2 steps alone"} if rank == 0 else None
 
     # end-to-end through the C ABI with host buffers
@@ -284,7 +288,7 @@ def run_b200(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "step_ms": step_ms, "higher_is_better": False,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded splitmix64 lattice Hamiltonian, generated on the host)",
-        "config": bench_config(world),
+        "config": bench_config(world, args.exchange),
         # the transfers move each row's columns up to the widest row
         "e2e": {"value": e2e, "unit": "s",
                 "h2d_bytes_per_step": int(N * int(nz.max()) * (v.itemsize + ix.itemsize) + nz.nbytes),
@@ -600,7 +604,7 @@ def run_reference(args, rank, world):
             "steps": steps, "warmup": warm, "ms_per_step": dt * 1e3, "higher_is_better": False,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded splitmix64 lattice Hamiltonian)",
-            "config": bench_config(world),
+            "config": bench_config(world, args.exchange),
             "cpu_baseline": {"value": dt, "unit": "s", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": dt, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -10,6 +10,16 @@ GPUs) before the next product.  Every rank therefore holds the same X after
 each iteration, as in the single-GPU solve, and the trajectory is the same
 up to the order in which the partial traces are summed.
 
+With exchange="halo" the iterate is not all-gathered.  A row of X^2 reads
+only the rows of X named by its columns, so after each update every rank
+publishes the range [lo, hi) of the columns of its own rows (two integers,
+all-gathered), and each rank sends to every other the rows of its block that
+fall in that rank's range (point-to-point).  Rows outside a rank's range go
+stale on it and are never read; one all-gather at the end gives every rank
+the whole result.  On a banded iterate (the 1-D chain, or the first
+iterations on a lattice) this moves a band of rows per neighbour instead of
+the whole matrix; the trajectory is the same as with the all-gather.
+
 The loop is written against a small set of operations so that its
 collective logic can be exercised on CPU ranks (gloo) with a host
 implementation of those operations; `GpuOps` is the implementation that
@@ -32,18 +42,52 @@ def row_blocks(n, world):
     return out
 
 
+def _overlap(a, b):
+    """Intersection of the half-open ranges a and b, or None."""
+    lo, hi = max(a[0], b[0]), min(a[1], b[1])
+    return (lo, hi) if lo < hi else None
+
+
 class ShardedSP2:
     """SP2 with rows split over the ranks of `dist` (torch.distributed).
 
     ops must provide: n (rows), start() (X0 on this rank, whole), x2_rows(r0,
     r1) -> (trX, trX2) partial traces, update_rows(branch, r0, r1),
     gather(blocks) (every rank receives every block of X), reduce_sum(array)
-    (sum over ranks), trace() (tr X, whole).
+    (sum over ranks), trace() (tr X, whole); for exchange="halo" also
+    column_range(r0, r1) -> (lo, hi) (the columns of rows r0..r1 of X, hi
+    exclusive; (0, 0) for no entries), allgather_ints(list) -> array of one
+    row per rank, and exchange(sends, recvs) with (peer, row0, row1)
+    entries (rows row0..row1 of X sent to or received from peer).
     """
 
-    def __init__(self, ops, dist, rank, world):
+    def __init__(self, ops, dist, rank, world, exchange="gather"):
+        if exchange not in ("gather", "halo"):
+            raise ValueError("exchange must be 'gather' or 'halo'")
         self.ops, self.dist, self.rank, self.world = ops, dist, rank, world
+        self.exchange = exchange
         self.blocks = row_blocks(ops.n, world)
+        self.rows_received = 0
+
+    def _halo(self):
+        """Send every rank the rows of this block that its next X^2 reads,
+        receive the rows this block's X^2 reads from the others."""
+        ops, me = self.ops, self.rank
+        r0, r1 = self.blocks[me]
+        lo, hi = ops.column_range(r0, r1)
+        ranges = np.asarray(ops.allgather_ints([lo, hi]), dtype=np.int64).reshape(self.world, 2)
+        sends, recvs = [], []
+        for peer in range(self.world):
+            if peer == me:
+                continue
+            out = _overlap(self.blocks[me], ranges[peer])
+            if out:
+                sends.append((peer, out[0], out[1]))
+            inc = _overlap(self.blocks[peer], ranges[me])
+            if inc:
+                recvs.append((peer, inc[0], inc[1]))
+        ops.exchange(sends, recvs)
+        self.rows_received += sum(b - a for _, a, b in recvs)
 
     def run(self, occupation, maxiter, tol=-1.0, stall=0):
         ops = self.ops
@@ -58,7 +102,11 @@ class ShardedSP2:
             branch = 0 if abs(t2 - occupation) <= abs(2.0 * t - t2 - occupation) else 1
             branches.append(branch)
             ops.update_rows(branch, r0, r1)
-            ops.gather(self.blocks)
+            if self.exchange == "halo":
+                self._halo()
+            else:
+                ops.gather(self.blocks)
+                self.rows_received += ops.n - (r1 - r0)
             it += 1
             if last < tol:
                 rule = 1
@@ -71,8 +119,10 @@ class ShardedSP2:
                     if since >= stall:
                         rule = 2
                         break
+        if self.exchange == "halo":
+            ops.gather(self.blocks)  # every rank ends with the whole iterate
         return {"iterations": it, "rule": rule, "trace": ops.trace(), "idempotency": last,
-                "branches": branches}
+                "branches": branches, "rows_received": self.rows_received}
 
 
 class _CudaArrayView:
@@ -156,6 +206,46 @@ class GpuOps:
                 for src, (a, b) in enumerate(blocks):
                     chunk = full[a * width:b * width]
                     self.dist.broadcast(chunk, src=src)
+        self.torch.cuda.synchronize()
+
+    def column_range(self, r0, r1):
+        self._check(self.lib.bml_b200_synchronize())
+        if r1 <= r0:
+            return 0, 0
+        t = self.torch
+        _, idx, nnz = self._device_views()
+        ld = self.ld
+        cols = idx[r0 * ld:r1 * ld].view(r1 - r0, ld)
+        live = t.arange(ld, device=cols.device)[None, :] < nnz[r0:r1, None]
+        if not bool(live.any()):
+            return 0, 0
+        lo = int(t.where(live, cols, t.full_like(cols, self.n)).min())
+        hi = int(t.where(live, cols, t.full_like(cols, -1)).max()) + 1
+        return lo, hi
+
+    def allgather_ints(self, vals):
+        t = self.torch
+        mine = t.tensor(vals, dtype=t.int64, device="cuda")
+        parts = [t.empty_like(mine) for _ in range(self.dist.get_world_size())]
+        self.dist.all_gather(parts, mine)
+        return t.stack(parts).cpu().numpy()
+
+    def exchange(self, sends, recvs):
+        # the library's stream must be done with X before NCCL reads it, and
+        # NCCL done before the library's next kernels read the received rows
+        self._check(self.lib.bml_b200_synchronize())
+        val, idx, nnz = self._device_views()
+        ld, d = self.ld, self.dist
+        p2p = []
+        for peer, a, b in sends:
+            for full, width in ((val, ld), (idx, ld), (nnz, 1)):
+                p2p.append(d.P2POp(d.isend, full[a * width:b * width], peer))
+        for peer, a, b in recvs:
+            for full, width in ((val, ld), (idx, ld), (nnz, 1)):
+                p2p.append(d.P2POp(d.irecv, full[a * width:b * width], peer))
+        if p2p:
+            for req in d.batch_isend_irecv(p2p):
+                req.wait()
         self.torch.cuda.synchronize()
 
     def trace(self):

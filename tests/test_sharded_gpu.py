@@ -22,7 +22,8 @@ def _free_port():
     return port
 
 
-def test_sharded_world1_matches_single_call(oracle_mod):
+@pytest.mark.parametrize("exchange", ["gather", "halo"])
+def test_sharded_world1_matches_single_call(oracle_mod, exchange):
     import torch
     import torch.distributed as dist
     from bml_b200.sharded import GpuOps, ShardedSP2
@@ -39,7 +40,11 @@ def test_sharded_world1_matches_single_call(oracle_mod):
     dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % _free_port(), rank=0, world_size=1)
     try:
         ops = GpuOps(B.lib, H.h, M, thr, dist, torch)
-        res = ShardedSP2(ops, dist, 0, 1).run(N / 2.0, iters)
+        res = ShardedSP2(ops, dist, 0, 1, exchange).run(N / 2.0, iters)
+        if exchange == "halo":
+            # the column range of all rows of the iterate: the whole lattice
+            assert ops.column_range(0, N) == (0, N)
+            assert res["rows_received"] == 0
         X = B.Ellpack(N, M, handle=ops.X)
         got = X.download()
         assert res["iterations"] == iters

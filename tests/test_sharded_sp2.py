@@ -90,21 +90,48 @@ class HostOps:
         return t.numpy()
 
     def gather(self, blocks):
-        rank = dist.get_rank()
         for a, wd in zip(self.X, (M, M, 1)):
-            r0, r1 = blocks[rank]
-            mine = torch.from_numpy(a[r0 * wd:r1 * wd].copy())
-            parts = [torch.empty_like(mine) for _ in blocks]
-            dist.all_gather(parts, mine)
-            for (s0, s1), p in zip(blocks, parts):
-                a[s0 * wd:s1 * wd] = p.numpy()
+            # blocks of unequal length (gloo's all_gather wants equal ones):
+            # one broadcast per block
+            for src, (s0, s1) in enumerate(blocks):
+                buf = torch.from_numpy(a[s0 * wd:s1 * wd].copy())
+                dist.broadcast(buf, src=src)
+                a[s0 * wd:s1 * wd] = buf.numpy()
+
+    def column_range(self, r0, r1):
+        _, ix, nz = self.X
+        cols = np.concatenate([ix[i * M:i * M + nz[i]] for i in range(r0, r1)] + [np.zeros(0, np.int32)])
+        return (int(cols.min()), int(cols.max()) + 1) if cols.size else (0, 0)
+
+    def allgather_ints(self, vals):
+        mine = torch.tensor(vals, dtype=torch.int64)
+        parts = [torch.empty_like(mine) for _ in range(dist.get_world_size())]
+        dist.all_gather(parts, mine)
+        return torch.stack(parts).numpy()
+
+    def exchange(self, sends, recvs):
+        reqs, inbox = [], []
+        # one tag per array (gloo matches a message by peer and tag), far
+        # from the small tags gloo's own collectives count up through
+        for peer, a, b in sends:
+            for k, (arr, wd) in enumerate(zip(self.X, (M, M, 1))):
+                reqs.append(dist.isend(torch.from_numpy(arr[a * wd:b * wd].copy()), peer, tag=1000000 + k))
+        for peer, a, b in recvs:
+            for k, (arr, wd) in enumerate(zip(self.X, (M, M, 1))):
+                buf = torch.from_numpy(np.empty((b - a) * wd, arr.dtype))
+                reqs.append(dist.irecv(buf, peer, tag=1000000 + k))
+                inbox.append((arr, a * wd, b * wd, buf))
+        for r in reqs:
+            r.wait()
+        for arr, a, b, buf in inbox:
+            arr[a:b] = buf.numpy()
 
     def trace(self):
         v, ix, nz = self.X
         return float(sum(v[i * M:i * M + nz[i]][ix[i * M:i * M + nz[i]] == i].sum() for i in range(N)))
 
 
-def _rank_main(rank, world, port, out_dir):
+def _rank_main(rank, world, port, out_dir, exchange="gather"):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, root)
@@ -114,9 +141,10 @@ def _rank_main(rank, world, port, out_dir):
     try:
         v, ix, nz = _chain(N, M)
         ops = HostOps(O, v, ix, nz)
-        res = ShardedSP2(ops, dist, rank, world).run(N / 2.0, ITERS)
+        res = ShardedSP2(ops, dist, rank, world, exchange).run(N / 2.0, ITERS)
         np.savez(os.path.join(out_dir, "rank%d.npz" % rank), v=ops.X[0], ix=ops.X[1], nz=ops.X[2],
-                 trace=res["trace"], iterations=res["iterations"], branches=np.array(res["branches"]))
+                 trace=res["trace"], iterations=res["iterations"], branches=np.array(res["branches"]),
+                 rows_received=res["rows_received"])
     finally:
         dist.destroy_process_group()
 
@@ -134,6 +162,67 @@ def test_sharded_sp2_two_ranks_matches_oracle(oracle_mod, tmp_path):
     assert int(r[0]["iterations"]) == int(info[0]) == ITERS
     assert O.same_rows_exact((r[0]["v"], r[0]["ix"], r[0]["nz"]), (dv, dix, dnz), M, M)
     assert float(r[0]["trace"]) == pytest.approx(info[2], rel=1e-12)
+
+
+def test_sharded_sp2_halo_three_ranks_matches_oracle(oracle_mod, tmp_path):
+    """The halo exchange (point-to-point rows within each rank's column
+    range, one all-gather at the end) on three gloo ranks, the middle one
+    with two neighbours: the same density matrix, bit for bit, as the
+    single-process oracle SP2, with far fewer rows moved than all-gathers
+    of the whole iterate would move."""
+    O = oracle_mod
+    port = _free_port()
+    world = 3
+    mp.spawn(_rank_main, args=(world, port, str(tmp_path), "halo"), nprocs=world, join=True)
+    r = [np.load(tmp_path / ("rank%d.npz" % k)) for k in range(world)]
+    for k in range(1, world):
+        for key in ("v", "ix", "nz", "branches"):
+            assert np.array_equal(r[0][key], r[k][key]), key
+    v, ix, nz = _chain(N, M)
+    (dv, dix, dnz), info = O.rest_sp2(v, ix, nz, N, M, THR, N / 2.0, ITERS, -1.0, 0)
+    assert int(r[0]["iterations"]) == int(info[0]) == ITERS
+    assert O.same_rows_exact((r[0]["v"], r[0]["ix"], r[0]["nz"]), (dv, dix, dnz), M, M)
+    assert float(r[0]["trace"]) == pytest.approx(info[2], rel=1e-12)
+    # rows received by the middle rank: its two bands, against the
+    # all-gather's N - N/3 rows per iteration
+    from bml_b200.sharded import row_blocks
+    b0, b1 = row_blocks(N, world)[1]
+    got = int(r[1]["rows_received"])
+    assert 0 < got < 0.5 * ITERS * (N - (b1 - b0))
+
+
+def test_halo_ranges_are_symmetric():
+    """What rank s sends to rank d is exactly what d receives from s."""
+    from bml_b200.sharded import ShardedSP2
+
+    class Fake:
+        n = 100
+
+        def __init__(self, me, ranges):
+            self.me, self.ranges, self.sent = me, ranges, None
+
+        def column_range(self, r0, r1):
+            return self.ranges[self.me]
+
+        def allgather_ints(self, vals):
+            return np.array(self.ranges)
+
+        def exchange(self, sends, recvs):
+            self.sent, self.recv = sends, recvs
+
+    ranges = [(0, 40), (20, 75), (60, 100), (0, 0)]
+    fakes = [Fake(k, ranges) for k in range(4)]
+    for k, f in enumerate(fakes):
+        ShardedSP2(f, None, k, 4, "halo")._halo()
+    for s_, fs in enumerate(fakes):
+        for peer, a, b in fs.sent:
+            assert (s_, a, b) in fakes[peer].recv
+    for d_, fd in enumerate(fakes):
+        for peer, a, b in fd.recv:
+            assert (d_, a, b) in fakes[peer].sent
+    # rank 3 (no entries) receives nothing; rank 1 receives rows 20..25 and 50..75
+    assert fakes[3].recv == []
+    assert sorted(fakes[1].recv) == [(0, 20, 25), (2, 50, 75)]
 
 
 def test_row_blocks_cover_rows():
