@@ -853,8 +853,8 @@ def ellblock_sp2_leg(iters=5, nclose=2):
             "iterations": iters, "closing_fp64": nclose, "fp64": e, "mixed": m, "speedup": e["s"] / m["s"],
             "trace_rel_err": abs(m["trace"] - e["trace"]) / abs(e["trace"]),
             "energy_rel_err": abs(m["energy_trDH"] - e["energy_trDH"]) / abs(e["energy_trDH"]),
-            "note": "bulk X^2 run on the tensor cores where a group of four block rows fits the kernel's "
-                    "capacities (here only X0^2); wider iterates run on the exact FP64 product"}
+            "note": "bulk X^2 on the tensor cores (FP16 hi/lo split, FP32 accumulation), the closing "
+                    "iterations on the exact FP64 block product"}
 
 
 def ellblock_leg(reps=3):

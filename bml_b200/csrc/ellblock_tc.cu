@@ -12,13 +12,18 @@
 // result is written back in the matrix precision; blocks are kept as in the
 // reference (kb == ib, or max |x| > threshold), the traces are FP64 sums.
 //
-// Work: persistent CTAs, claiming from a counter groups of four consecutive block rows
-// ib0..ib0+3, which share most of their block columns jb on a lattice.  For
-// the group, with M = 128 = 4 x 32 rows:
+// Work: persistent CTAs claim from a counter groups of four consecutive
+// block rows ib0..ib0+3, which share most of their block columns jb on a
+// lattice.  For the group, with M = 128 = 4 x 32 rows:
 //   D[kb] (128 x 32, FP32, in TMEM) += [X[ib0,jb]; ..; X[ib0+3,jb]] X[jb,kb]
 // over the union J of the rows' block columns (missing blocks are zero), for
-// every output block column kb; 16 output tiles of 32 TMEM columns are live
-// at once (a wave), so the group's outputs are made in waves.
+// every output block column kb in K; 8 output tiles of 32 TMEM columns are
+// live at once (a wave), so the group's outputs are made in waves.
+// The group's tables (J, K, the output tile of every pair (jb, kb), and the
+// pairs sorted by wave with a stable counting sort, so that the pairs of one
+// jb stay together and share one left operand) are built by the CTA in global
+// memory, one set per CTA, sized before the launch by a counting kernel for
+// the largest group: the kernel takes groups of any size.
 // Operands are staged into shared memory in the UMMA canonical K-major
 // no-swizzle layout (8-row x 16-byte core matrices).  A split kernel first
 // writes every block of X in that layout, as the left operand (rows x k) and
@@ -26,18 +31,20 @@
 // 2 KB image each, so staging is one bulk copy (cp.async.bulk, completing on
 // an mbarrier) per block, issued by one producer thread into rings of left
 // and right operand buffers.  One thread issues the MMAs and releases each
-// buffer with tcgen05.commit on its "empty" mbarrier.  Everything either
-// thread needs per pair is precomputed by the whole CTA when the wave's pair
-// list is built (the new-left-operand flag, the rows each tile touches), so
-// their loops hold only the waits, the copies and the MMAs.  Every wait is
-// bounded.
+// buffer with tcgen05.commit on its "empty" mbarrier.  A sorted pair's record
+// holds everything either thread needs (the new-left-operand flag, the
+// positions of the left blocks, the right operand's slot, the tile), so their
+// loops hold only one record load, the waits, the copies and the MMAs.  Every
+// wait is bounded.
 #include "device_util.cuh"
 #include "ellblock.h"
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -51,25 +58,29 @@ constexpr int TC_THREADS = 128;   // 4 warps; warp q owns TMEM lanes 32q..32q+31
 constexpr int TC_GROUP = 4;       // block rows per group (M = 128)
 constexpr int IMG = TB * TB;      // 16-bit elements per block image (2 KB)
 constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
-// Two shapes of the kernel: a small one with two CTAs per SM (8 live tiles,
-// 256 TMEM columns each, so one CTA's set-up and epilogue overlap the
-// other's MMAs) that takes groups up to its capacities, and a large one with
-// one CTA per SM that the host falls back to when a group exceeds them.
-// ABUF/BBUF: left/right operand buffers; JCAP: union of block columns per
-// group; KCAP: output block columns per group; LCAP: product pairs per wave;
-// PCAP: product pairs per group.
-template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int JCAP_, int KCAP_, int LCAP_, int PCAP_> struct TcCfg
+// Shape of the kernel: TILES output tiles live per CTA (a wave), CTAS CTAs
+// per SM (two, so that one CTA's set-up and epilogue overlap the other's
+// MMAs), ABUF and BBUF buffers in the left and right operand rings, ACC
+// accumulators of 32 TMEM columns per tile: with 1, hi*hi, hi*lo and lo*hi
+// all add into one; with 2, the small cross terms hi*lo + lo*hi add into a
+// second one, so the large sum takes a third of the accumulation steps.
+template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int ACC_> struct TcCfg
 {
-    static constexpr int TILES = TILES_, CTAS = CTAS_, ABUF = ABUF_, BBUF = BBUF_;
-    static constexpr int JCAP = JCAP_, KCAP = KCAP_, LCAP = LCAP_, PCAP = PCAP_;
-    static_assert(CTAS * TILES * 32 <= 512, "tensor memory holds 512 columns per SM");
+    static constexpr int TILES = TILES_, CTAS = CTAS_, ABUF = ABUF_, BBUF = BBUF_, ACC = ACC_;
+    static_assert(CTAS * TILES * 32 * ACC <= 512, "tensor memory holds 512 columns per SM");
     static_assert(TILES <= 16, "tile numbers take 4 bits of a pair");
+    static_assert(ACC == 1 || ACC == 2, "one or two accumulators per tile");
 };
-#ifndef B200_TCS_SHAPE
-#define B200_TCS_SHAPE 8, 2, 3, 8, 512, 1024, 1024, 4096
+#ifndef B200_TC_TILES
+#define B200_TC_TILES 8
 #endif
-using TcSmall = TcCfg<B200_TCS_SHAPE>;
-using TcBig = TcCfg<16, 1, 6, 12, 1024, 4096, 2048, 8192>;
+#ifndef B200_TC_CTAS
+#define B200_TC_CTAS 2
+#endif
+#ifndef B200_TC_ACC
+#define B200_TC_ACC 1
+#endif
+using TcShape = TcCfg<B200_TC_TILES, B200_TC_CTAS, 3, 8, B200_TC_ACC>;
 
 // Operand type of the split: FP16 (11-bit significands: hi and lo carry
 // about 22 bits, the dropped lo*lo about 2^-22 of a product) with the whole
@@ -283,28 +294,21 @@ template <class Cfg> struct TcSmem
             int jpre[TC_NWCAP];       // J entries before each bitmap word: index = rank of jb
             unsigned kbits[TC_NWCAP]; // output block columns of the group (bitmap over NB)
             int kpre[TC_NWCAP];       // tiles before each bitmap word: tile = rank of kb
-        } su; // the group's set-up, while the left-operand ring is idle
+        } su;                         // the group's set-up, while the left-operand ring is idle
+        int wpos[4 * TC_NWCAP];       // then the next free place of every wave in the sorted pairs
     };
     union
     {
-        tc_t b[Cfg::BBUF][2][IMG]; // right operands, hi and lo: 32 x 32 (2 KB each)
+        tc_t b[Cfg::BBUF][2][IMG];         // right operands, hi and lo: 32 x 32 (2 KB each)
         float stage[TC_GROUP][TB][TB + 1]; // epilogue transpose (the ring is idle then)
     };
     uint64_t full_a[Cfg::ABUF], full_b[Cfg::BBUF]; // bulk copies landed
-    uint64_t empty_b[Cfg::BBUF];            // MMAs reading a B buffer (and all before) done
-    uint64_t empty_a[Cfg::ABUF];            // MMAs reading an A buffer's fill (and all before) done
-    uint64_t done;                        // all MMAs of a wave done
+    uint64_t empty_b[Cfg::BBUF];                   // MMAs reading a B buffer (and all before) done
+    uint64_t empty_a[Cfg::ABUF];                   // MMAs reading an A buffer's fill (and all before) done
+    uint64_t done;                                 // all MMAs of a wave done
     unsigned tmem;
-    int nJ, nK, npairs, ok, dead, grp;
-    int jb[Cfg::JCAP];             // union of the group's block columns
-    short jslot[Cfg::JCAP][TC_GROUP]; // position of X[ib0+q, jb] in row ib0+q, or -1
-    int klist[Cfg::KCAP];          // kb of each output tile
-    int jcnt[Cfg::JCAP];           // pairs of the current wave per J entry, then their start
-    int list[Cfg::LCAP];           // pairs of the current wave: j << 20 | tile << 16 | kp
-    int jstart[Cfg::JCAP + 1];     // first pair of each J entry in ptile
-    unsigned short ptile[Cfg::PCAP]; // output tile of every pair (j, kp) of the group
-    unsigned char jmask[Cfg::JCAP];  // rows q of the group holding X[ib0+q, jb]
-    int touched[Cfg::TILES];         // rows q of the group with a product in the tile
+    int nJ, nK, npairs, dead, grp;
+    int scratch[TC_THREADS / 32];
 };
 
 template <typename T> struct TcView
@@ -323,27 +327,27 @@ template <typename T> struct TcOut
     long long slot;
 };
 
-// Slot of key k in an open-addressing table of size 2*cap (cap a power of 2).
-__device__ __forceinline__ int tc_find(int *keys, int cap2, int k, bool &found)
+// A group's tables, in global memory: one set per CTA, each sized for the
+// largest group (tc_count_kernel).  A pair (j, kp) is the product of the
+// group's left operand for J entry j with the right operand X[jb_j, kb],
+// kb the kp-th block column of row jb_j.  Records of the sorted pairs:
+//   x = tile within the wave (bits 0-3) | j << 4 | a new left operand << 31,
+//   y = slot of the right operand, jb * MB + kp,
+//   z, w = position jp of X[ib0+q, jb] in row ib0+q for q = 0..3, 16 bits
+//          each (z: q = 0, 1; w: q = 2, 3), 0xFFFF where the row lacks jb.
+struct TcTab
 {
-    unsigned h = ((unsigned) k * 2654435761u) & (unsigned) (cap2 - 1);
-    for (int p = 0; p < cap2; ++p)
-    {
-        if (keys[h] == k)
-        {
-            found = true;
-            return (int) h;
-        }
-        if (keys[h] == B200_EMPTY_KEY)
-        {
-            found = false;
-            return (int) h;
-        }
-        h = (h + 1) & (unsigned) (cap2 - 1);
-    }
-    found = false;
-    return -1;
-}
+    int *jb;              // [jcap] J: the group's block columns, ascending
+    uint2 *jslot;         // [jcap] positions of X[ib0+q, jb], as z, w above
+    unsigned char *jmask; // [jcap] rows q holding jb
+    int *jstart;          // [jcap + 1] first pair of each J entry, pairs in (j, kp) order
+    int *klist;           // [kcap] K: the output block columns, ascending (tile = rank)
+    int *ttouch;          // [kcap] rows q with a product in each tile
+    int *ptile;           // [pcap] output tile of every pair, in (j, kp) order
+    uint4 *list;          // [pcap] the pairs sorted by wave, in (j, kp) order within a wave
+    int *wstart;          // [wcap + 1] first pair of each wave in list
+    int jcap, kcap, pcap, wcap;
+};
 
 // Rank of the set bits of bits[0..nwords): pre[w] = set bits before word w,
 // list[rank] = bit position (up to cap entries), *total = bits set.  All
@@ -386,24 +390,140 @@ __device__ void rank_bits(const unsigned *bits, int *pre, int *list, int cap, in
         *total = run;
 }
 
-// flags: [0] row overflow, [1] widest kept row, [2] group over capacity,
-// [3] a tensor-core wait timed out, [4] next group to claim
+// Sizes of every group's tables: |J|, |K| and its pairs sum_{jb in J}
+// nnzb[jb].  Their maxima over the groups go to flags[5], [6] and [7], a
+// block column outside 0..NB-1 to flags[2].  One group per CTA at a time;
+// the rows of J are walked one per warp.
+template <typename T>
+__global__ void __launch_bounds__(TC_THREADS) tc_count_kernel(TcView<T> X, int *flags)
+{
+    __shared__ unsigned jbits[TC_NWCAP], kbits[TC_NWCAP];
+    __shared__ long long red[TC_THREADS / 32][3];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ngroups = (X.NB + TC_GROUP - 1) / TC_GROUP;
+    const int nwords = (X.NB + 31) >> 5;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x)
+    {
+        for (int w = tid; w < nwords; w += TC_THREADS)
+        {
+            jbits[w] = 0u;
+            kbits[w] = 0u;
+        }
+        __syncthreads();
+        const int row = g * TC_GROUP + warp;
+        int bad = 0;
+        if (row < X.NB)
+            for (int jp = lane; jp < X.nnzb[row]; jp += 32)
+            {
+                const int jb = X.indexb[(size_t) row * X.MB + jp];
+                if (jb < 0 || jb >= X.NB)
+                    bad = 1;
+                else
+                    atomicOr(&jbits[jb >> 5], 1u << (jb & 31));
+            }
+        __syncthreads();
+        long long pairs = 0, nj = 0, nk = 0;
+        // warp-strided words of the J bitmap; each set bit's row is walked
+        // by the whole warp
+        for (int w0 = warp * 32; w0 < nwords; w0 += TC_THREADS)
+        {
+            const int w = w0 + lane;
+            unsigned b = w < nwords ? jbits[w] : 0u;
+            nj += __popc(b);
+            for (;;)
+            {
+                const unsigned live = __ballot_sync(FULL, b != 0u);
+                if (!live)
+                    break;
+                const int src = __ffs(live) - 1;
+                const unsigned bsrc = __shfl_sync(FULL, b, src);
+                const int jb = ((w0 + src) << 5) + __ffs(bsrc) - 1;
+                if (lane == src)
+                    b &= b - 1;
+                const int n = X.nnzb[jb];
+                if (lane == 0)
+                    pairs += n;
+                for (int kp = lane; kp < n; kp += 32)
+                {
+                    const int kb = X.indexb[(size_t) jb * X.MB + kp];
+                    if (kb < 0 || kb >= X.NB)
+                        bad = 1;
+                    else
+                        atomicOr(&kbits[kb >> 5], 1u << (kb & 31));
+                }
+            }
+        }
+        __syncthreads();
+        for (int w = tid; w < nwords; w += TC_THREADS)
+            nk += __popc(kbits[w]);
+        for (int o = 16; o; o >>= 1)
+        {
+            pairs += __shfl_xor_sync(FULL, pairs, o);
+            nj += __shfl_xor_sync(FULL, nj, o);
+            nk += __shfl_xor_sync(FULL, nk, o);
+        }
+        if (lane == 0)
+        {
+            red[warp][0] = pairs;
+            red[warp][1] = nj;
+            red[warp][2] = nk;
+        }
+        if (__syncthreads_or(bad) && tid == 0)
+            atomicExch(&flags[2], 1);
+        if (tid == 0)
+        {
+            long long s[3] = {0, 0, 0};
+            for (int w = 0; w < TC_THREADS / 32; ++w)
+                for (int k = 0; k < 3; ++k)
+                    s[k] += red[w][k];
+            atomicMax(&flags[5], (int) s[1]);
+            atomicMax(&flags[6], (int) s[2]);
+            atomicMax(&flags[7], (int) min(s[0], (long long) INT_MAX));
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// Position of X[ib0+q, jb] in row ib0+q from a record's z, w (0xFFFF: none).
+__device__ __forceinline__ unsigned rec_slot(const uint4 &r, int q)
+{
+    const unsigned v = q < 2 ? r.z : r.w;
+    return (v >> ((q & 1) * 16)) & 0xFFFFu;
+}
+
+// flags: [0] row overflow, [1] widest kept row, [2] a group's tables outside
+// their sizes, [3] a tensor-core wait timed out, [4] next group to claim,
+// [8] max |x| of X (the split's scale)
 template <typename T, class Cfg>
 __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
-    tc_x2_kernel(TcView<T> X, TcOut<T> C, const tc_t *img, const tc_t *zimg, double thr,
+    tc_x2_kernel(TcView<T> X, TcOut<T> C, TcTab G, const tc_t *img, const tc_t *zimg, double thr,
                  double *dA, double *dC, int *flags)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    constexpr int TC_TILES = Cfg::TILES, TC_ABUF = Cfg::ABUF, TC_BBUF = Cfg::BBUF, TC_JCAP = Cfg::JCAP;
-    constexpr int TC_KCAP = Cfg::KCAP, TC_LCAP = Cfg::LCAP, TC_PCAP = Cfg::PCAP;
+    constexpr int TC_TILES = Cfg::TILES, TC_ABUF = Cfg::ABUF, TC_BBUF = Cfg::BBUF;
+    static_assert(TC_TILES >= 8, "wave counters: NB / TILES <= 4 * TC_NWCAP");
     TcSmem<Cfg> &S = *reinterpret_cast<TcSmem<Cfg> *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ngroups = (X.NB + TC_GROUP - 1) / TC_GROUP;
+    {
+        const size_t cb = blockIdx.x;
+        G.jb += cb * G.jcap;
+        G.jslot += cb * G.jcap;
+        G.jmask += cb * G.jcap;
+        G.jstart += cb * (G.jcap + 1);
+        G.klist += cb * G.kcap;
+        G.ttouch += cb * G.kcap;
+        G.ptile += cb * G.pcap;
+        G.list += cb * G.pcap;
+        G.wstart += cb * (G.wcap + 1);
+    }
 
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&S.tmem)),
-                     "r"(TC_TILES * 32)
+                     "r"(TC_TILES * 32 * Cfg::ACC)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -452,8 +572,6 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             S.su.jbits[s2] = 0u;
             S.su.kbits[s2] = 0u;
         }
-        if (tid == 0)
-            S.ok = 1;
         __syncthreads();
         int bad = 0;
         if (myrow < X.NB)
@@ -471,41 +589,41 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                 atomicExch(&flags[2], 1);
             continue;
         }
-        rank_bits(S.su.jbits, S.su.jpre, S.jb, TC_JCAP, nwords, S.jcnt, &S.nJ, tid, lane, warp);
+        rank_bits(S.su.jbits, S.su.jpre, G.jb, G.jcap, nwords, S.scratch, &S.nJ, tid, lane, warp);
         __syncthreads();
-        if (S.nJ > TC_JCAP)
+        const int nJ = S.nJ;
+        if (nJ > G.jcap)
         {
             if (tid == 0)
                 atomicExch(&flags[2], 1);
             continue;
         }
-        for (int j = tid; j < S.nJ; j += TC_THREADS)
-            for (int q = 0; q < TC_GROUP; ++q)
-                S.jslot[j][q] = -1;
+        for (int j = tid; j < nJ; j += TC_THREADS)
+            G.jslot[j] = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
         __syncthreads();
         if (myrow < X.NB)
             for (int jp = lane; jp < X.nnzb[myrow]; jp += 32)
             {
                 const int jb = X.indexb[(size_t) myrow * X.MB + jp];
                 const int j = S.su.jpre[jb >> 5] + __popc(S.su.jbits[jb >> 5] & ((1u << (jb & 31)) - 1u));
-                S.jslot[j][warp] = (short) jp;
+                reinterpret_cast<unsigned short *>(G.jslot + j)[warp] = (unsigned short) jp;
             }
         __syncthreads();
-        for (int j = tid; j < S.nJ; j += TC_THREADS)
+        for (int j = tid; j < nJ; j += TC_THREADS)
         {
+            const uint2 s = G.jslot[j];
+            const uint4 r = make_uint4(0u, 0u, s.x, s.y);
             unsigned char m = 0;
             for (int q = 0; q < TC_GROUP; ++q)
-                if (S.jslot[j][q] >= 0)
+                if (rec_slot(r, q) != 0xFFFFu)
                     m |= (unsigned char) (1u << q);
-            S.jmask[j] = m;
+            G.jmask[j] = m;
         }
-        __syncthreads();
-        const int nJ = S.nJ;
         // ---- output block columns K: a bitmap over NB, tiles by rank ----
         int badk = 0;
-        for (int j = warp; j < nJ && S.ok; j += TC_THREADS / 32)
+        for (int j = warp; j < nJ; j += TC_THREADS / 32)
         {
-            const int jb = S.jb[j];
+            const int jb = G.jb[j];
             for (int kp = lane; kp < X.nnzb[jb]; kp += 32)
             {
                 const int kb = X.indexb[(size_t) jb * X.MB + kp];
@@ -518,21 +636,18 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
         if (__syncthreads_or(badk))
         {
             if (tid == 0)
-                S.ok = 0;
+                atomicExch(&flags[2], 1);
+            continue;
         }
-        __syncthreads();
-        rank_bits(S.su.kbits, S.su.kpre, S.klist, TC_KCAP, nwords, S.jcnt, &S.nK, tid, lane, warp);
-        __syncthreads();
-        if (tid == 0 && S.nK > TC_KCAP)
-            S.ok = 0;
-        __syncthreads();
+        rank_bits(S.su.kbits, S.su.kpre, G.klist, G.kcap, nwords, S.scratch, &S.nK, tid, lane, warp);
         if (warp == 0)
         {
+            // first pair of every J entry: pairs in (j, kp) order
             int run = 0;
             for (int j0 = 0; j0 < nJ; j0 += 32)
             {
                 const int j = j0 + lane;
-                const int n = j < nJ ? X.nnzb[S.jb[j]] : 0;
+                const int n = j < nJ ? X.nnzb[G.jb[j]] : 0;
                 int incl = n;
                 for (int o = 1; o < 32; o <<= 1)
                 {
@@ -541,40 +656,113 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         incl += y;
                 }
                 if (j < nJ)
-                    S.jstart[j] = run + incl - n;
+                    G.jstart[j] = run + incl - n;
                 run += __shfl_sync(FULL, incl, 31);
             }
             if (lane == 0)
             {
-                S.jstart[nJ] = run;
-                if (run > TC_PCAP)
-                    S.ok = 0;
+                G.jstart[nJ] = run;
+                S.npairs = run;
             }
         }
         __syncthreads();
-        if (!S.ok)
+        const int nK = S.nK, npairs = S.npairs;
+        const int nW = (nK + TC_TILES - 1) / TC_TILES;
+        if (nK > G.kcap || npairs > G.pcap || nW > G.wcap || nW > 4 * TC_NWCAP)
         {
             if (tid == 0)
                 atomicExch(&flags[2], 1);
             continue;
         }
-        // the output tile of every pair (j, kp), once per group
+        for (int t = tid; t < nK; t += TC_THREADS)
+            G.ttouch[t] = 0;
+        __syncthreads();
+        // the output tile of every pair (j, kp), and the rows each tile touches
         for (int j = warp; j < nJ; j += TC_THREADS / 32)
         {
-            const int jb = S.jb[j];
+            const int jb = G.jb[j], ps = G.jstart[j];
+            const int m = G.jmask[j];
             for (int kp = lane; kp < X.nnzb[jb]; kp += 32)
             {
                 const int kb = X.indexb[(size_t) jb * X.MB + kp];
-                S.ptile[S.jstart[j] + kp] =
-                    (unsigned short) (S.su.kpre[kb >> 5] + __popc(S.su.kbits[kb >> 5] & ((1u << (kb & 31)) - 1u)));
+                const int t = S.su.kpre[kb >> 5] + __popc(S.su.kbits[kb >> 5] & ((1u << (kb & 31)) - 1u));
+                G.ptile[ps + kp] = t;
+                atomicOr(&G.ttouch[t], m);
             }
         }
-        // the set-up area is the left-operand ring: order its generic
-        // accesses before the bulk copies that refill it
-        proxy_fence();
         __syncthreads();
-        const int nK = S.nK;
-        const int nW = (nK + TC_TILES - 1) / TC_TILES;
+        // ---- the pairs sorted by wave (a stable counting sort) ----
+        for (int w = tid; w < nW; w += TC_THREADS)
+            S.wpos[w] = 0;
+        __syncthreads();
+        for (int p = tid; p < npairs; p += TC_THREADS)
+            atomicAdd(&S.wpos[G.ptile[p] / TC_TILES], 1);
+        __syncthreads();
+        if (warp == 0)
+        {
+            int run = 0;
+            for (int w0 = 0; w0 < nW; w0 += 32)
+            {
+                const int w = w0 + lane;
+                const int n = w < nW ? S.wpos[w] : 0;
+                int incl = n;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o)
+                        incl += y;
+                }
+                if (w < nW)
+                {
+                    S.wpos[w] = run + incl - n;
+                    G.wstart[w] = run + incl - n;
+                }
+                run += __shfl_sync(FULL, incl, 31);
+            }
+            if (lane == 0)
+                G.wstart[nW] = run;
+            __syncwarp();
+            // one warp places the pairs in (j, kp) order: stable
+            for (int j = 0; j < nJ; ++j)
+            {
+                const int jb = G.jb[j], ps = G.jstart[j], n = G.jstart[j + 1] - ps;
+                const uint2 sl = G.jslot[j];
+                for (int k0 = 0; k0 < n; k0 += 32)
+                {
+                    const int kp = k0 + lane;
+                    const int t = kp < n ? G.ptile[ps + kp] : -1;
+                    const int w = t >= 0 ? t / TC_TILES : -1 - lane;
+                    const unsigned peers = __match_any_sync(FULL, w);
+                    const int leader = __ffs(peers) - 1;
+                    int base = 0;
+                    if (lane == leader && t >= 0)
+                    {
+                        base = S.wpos[w];
+                        S.wpos[w] = base + __popc(peers);
+                    }
+                    base = __shfl_sync(FULL, base, leader);
+                    if (t >= 0)
+                    {
+                        const int pos = base + __popc(peers & lanemask_lt());
+                        G.list[pos] = make_uint4((unsigned) (t - w * TC_TILES) | ((unsigned) j << 4),
+                                                 (unsigned) jb * (unsigned) X.MB + (unsigned) kp, sl.x, sl.y);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // a new left operand where j changes within a wave, and at every
+        // wave's first pair
+        for (int p = tid; p < npairs; p += TC_THREADS)
+        {
+            const unsigned x = G.list[p].x;
+            if (p == 0 || ((x ^ G.list[p - 1].x) & 0x7FFFFFF0u))
+                G.list[p].x = x | 0x80000000u;
+        }
+        __syncthreads();
+        for (int w = tid; w < nW; w += TC_THREADS)
+            if (G.wstart[w] < npairs) // every wave has a pair: each tile is some pair's
+                G.list[G.wstart[w]].x |= 0x80000000u;
         int kept = 0;
         double trc = 0.0;
 
@@ -600,94 +788,30 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             if (lane == 0 && dA)
                 dA[myrow] = s;
         }
+        // the set-up area is the left-operand ring: order its generic
+        // accesses before the bulk copies that refill it
+        proxy_fence();
+        __syncthreads();
 
         // ---- waves of TC_TILES output tiles ----
         for (int w = 0; w < nW && !dead; ++w)
         {
             const int t0 = w * TC_TILES;
             const int nt = min(TC_TILES, nK - t0);
-            if (tid < TC_TILES)
-                S.touched[tid] = 0;
-            __syncthreads();
-            // pairs (j, kb) of this wave, ordered by j then kp: count per j,
-            // prefix, write
-            for (int j = warp; j < nJ; j += TC_THREADS / 32)
-            {
-                const int ps = S.jstart[j], pn = S.jstart[j + 1] - ps;
-                int cnt = 0;
-                for (int k0 = 0; k0 < pn; k0 += 32)
-                {
-                    const int kp = k0 + lane;
-                    bool in = false;
-                    if (kp < pn)
-                    {
-                        const int t = S.ptile[ps + kp];
-                        in = t >= t0 && t < t0 + nt;
-                    }
-                    cnt += __popc(__ballot_sync(FULL, in));
-                }
-                if (lane == 0)
-                    S.jcnt[j] = cnt;
-            }
-            __syncthreads();
-            if (tid == 0)
-            {
-                int run = 0;
-                for (int j = 0; j < nJ; ++j)
-                {
-                    const int c = S.jcnt[j];
-                    S.jcnt[j] = run;
-                    run += c;
-                }
-                S.npairs = run;
-            }
-            __syncthreads();
-            const int p0 = 0, p1 = S.npairs;
-            if (p1 > TC_LCAP)
-            {
-                if (tid == 0)
-                    atomicExch(&flags[2], 1);
-                dead = true; // capacity, not a timeout: leave the group set
-                break;
-            }
-            for (int j = warp; j < nJ; j += TC_THREADS / 32)
-            {
-                const int ps = S.jstart[j], pn = S.jstart[j + 1] - ps;
-                int pos = S.jcnt[j];
-                for (int k0 = 0; k0 < pn; k0 += 32)
-                {
-                    const int kp = k0 + lane;
-                    bool in = false;
-                    int t = 0;
-                    if (kp < pn)
-                    {
-                        t = S.ptile[ps + kp];
-                        in = t >= t0 && t < t0 + nt;
-                    }
-                        const unsigned bal = __ballot_sync(FULL, in);
-                    if (in)
-                    {
-                        const int at = pos + __popc(bal & lanemask_lt());
-                        // bit 30: the first pair of this j in the wave (a new left operand)
-                        S.list[at] = (at == S.jcnt[j] ? 1 << 30 : 0) | (j << 20) | ((t - t0) << 16) | kp;
-                        atomicOr(&S.touched[t - t0], (int) S.jmask[j]);
-                    }
-                    pos += __popc(bal);
-                }
-            }
-            __syncthreads();
+            const int p0 = G.wstart[w], p1 = G.wstart[w + 1];
             if (tid == 0)
             {
                 // producer (thread 0): for each pair, its right operand into
-                // the next B buffer and, on a new j, the group's left operand
-                // into the next A buffer, each once the MMAs that read the
-                // buffer's previous fill are done
+                // the next B buffer and, on a new left operand, the group's
+                // four blocks of column jb into the next A buffer, each once
+                // the MMAs that read the buffer's previous fill are done
                 for (int p = p0; p < p1; ++p)
                 {
-                    const int pv = S.list[p];
-                    const int j = (pv >> 20) & 1023, kp = pv & 0xFFFF;
+                    if (((p - p0) & 7) == 0 && p + 16 < p1)
+                        prefetch_l1(G.list + p + 16);
+                    const uint4 r = G.list[p];
                     const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
-                    if (pv >> 30)
+                    if (r.x >> 31)
                     {
                         const unsigned a = ga % TC_ABUF, fa = ga / TC_ABUF;
                         if (fa >= 1 && !mbar_wait2s(&S.empty_a[a], (fa - 1) & 1))
@@ -699,12 +823,12 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
 #pragma unroll
                         for (int q = 0; q < TC_GROUP; ++q)
                         {
-                            const int jp = S.jslot[j][q];
+                            const unsigned jp = rec_slot(r, q);
 #pragma unroll
                             for (int part = 0; part < 2; ++part)
                             {
                                 const tc_t *src =
-                                    jp >= 0 ? img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG : zimg;
+                                    jp != 0xFFFFu ? img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG : zimg;
                                 bulk_copy(reinterpret_cast<unsigned char *>(S.a[a][part]) + q * 2048, src, IMG * 2,
                                           &S.full_a[a]);
                             }
@@ -720,8 +844,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                     mbar_expect(&S.full_b[b], 2 * IMG * 2);
                     // the right hi and lo images are adjacent in both places:
                     // one 4 KB copy
-                    const tc_t *bsrc = img + ((size_t) S.jb[j] * X.MB + kp) * 4 * IMG;
-                    bulk_copy(S.b[b][0], bsrc + 2 * IMG, 2 * IMG * 2, &S.full_b[b]);
+                    bulk_copy(S.b[b][0], img + (size_t) r.y * 4 * IMG + 2 * IMG, 2 * IMG * 2, &S.full_b[b]);
                     ++gp;
                 }
             }
@@ -732,10 +855,12 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                 unsigned started = 0, acur = 0;
                 for (int p = p0; p < p1; ++p)
                 {
-                    const int pv = S.list[p];
-                    const int tile = (pv >> 16) & 15;
+                    if (((p - p0) & 7) == 0 && p + 16 < p1)
+                        prefetch_l1(G.list + p + 16);
+                    const unsigned rx = G.list[p].x;
+                    const int tile = (int) (rx & 15u);
                     const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
-                    if (pv >> 30)
+                    if (rx >> 31)
                     {
                         if (p > p0)
                             umma_commit(&S.empty_a[acur]); // the previous left operand is done with
@@ -753,7 +878,8 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         break;
                     }
                     tc_fence_after();
-                    const unsigned d = tbase + (unsigned) (tile * 32);
+                    const unsigned d = tbase + (unsigned) (tile * 32 * Cfg::ACC);
+                    const unsigned dx = d + (Cfg::ACC == 2 ? 32u : 0u); // the cross terms' accumulator
                     const unsigned a0 = su32(S.a[acur][0]), a1 = su32(S.a[acur][1]);
                     const unsigned b0 = su32(S.b[b][0]), b1 = su32(S.b[b][1]);
                     unsigned acc = (started >> tile) & 1u;
@@ -767,8 +893,8 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         const uint64_t bh = smem_desc(b0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
                         const uint64_t bl = smem_desc(b1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
                         umma_f16(d, ah, bh, acc);
-                        umma_f16(d, ah, bl, 1u);
-                        umma_f16(d, al, bh, 1u);
+                        umma_f16(dx, ah, bl, Cfg::ACC == 2 ? acc : 1u);
+                        umma_f16(dx, al, bh, 1u);
                         acc = 1u;
                     }
                     umma_commit(&S.empty_b[b]);
@@ -799,12 +925,20 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             for (int t = 0; t < nt; ++t)
             {
                 float v[32];
-                tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32), v);
+                tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32 * Cfg::ACC), v);
+                if (Cfg::ACC == 2)
+                {
+                    float vx[32];
+                    tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 64 + 32), vx);
+#pragma unroll
+                    for (int c = 0; c < 32; ++c)
+                        v[c] += vx[c];
+                }
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
                     v[c] *= unscale; // undo the split's 2^s on both factors
-                const int kb = S.klist[t0 + t];
-                if (myrow >= X.NB || !((S.touched[t] >> warp) & 1))
+                const int kb = G.klist[t0 + t];
+                if (myrow >= X.NB || !((G.ttouch[t0 + t] >> warp) & 1))
                     continue;
                 float mx = 0.f, diag = 0.f;
 #pragma unroll
@@ -884,7 +1018,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TILES * 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TILES * 32 * Cfg::ACC)
                      : "memory");
 }
 
@@ -901,24 +1035,32 @@ bool tc_split(B200Context *c, const bml_matrix_ellblock_t *X, int sgrid, unsigne
     return LAUNCH_OK("tc_split_kernel");
 }
 
-template <typename T, class Cfg>
-bool tc_launch(B200Context *c, const bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, const tc_t *img,
-               const tc_t *zimg, double threshold, double *dA, double *dC, int *flags)
+template <typename T> TcView<T> tc_view(const bml_matrix_ellblock_t *X)
 {
-    const size_t smem = sizeof(TcSmem<Cfg>) + 1024;
-    auto k = tc_x2_kernel<T, Cfg>;
+    return TcView<T>{static_cast<const T *>(X->d_pool), X->d_indexb, X->d_nnzb, X->NB, X->MB, X->slot_elems};
+}
+
+template <typename T>
+bool tc_launch(B200Context *c, const bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, const TcTab &tab,
+               const tc_t *img, const tc_t *zimg, double threshold, double *dA, double *dC, int *flags, int grid)
+{
+    const size_t smem = sizeof(TcSmem<TcShape>) + 1024;
+    auto k = tc_x2_kernel<T, TcShape>;
     if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
         return false;
-    k<<<c->sm_count * Cfg::CTAS, TC_THREADS, smem, c->stream>>>(
-        TcView<T>{static_cast<const T *>(X->d_pool), X->d_indexb, X->d_nnzb, X->NB, X->MB, X->slot_elems},
-        TcOut<T>{static_cast<T *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems}, img, zimg,
-        threshold, dA, dC, flags);
+    k<<<grid, TC_THREADS, smem, c->stream>>>(
+        tc_view<T>(X), TcOut<T>{static_cast<T *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems}, tab,
+        img, zimg, threshold, dA, dC, flags);
     return LAUNCH_OK("tc_x2_kernel");
 }
 
+// Bytes of device memory the tables of one X^2 may take (all CTAs).
+constexpr size_t TC_TABLE_BUDGET = size_t(16) << 30;
+
 // X2 = X*X on the tensor cores (FP16 hi/lo split, FP32 accumulation); X and
 // X2 must have blocks of 32 throughout.  Returns false with a status set
-// (UNSUPPORTED when the partition or a group's size is outside this path).
+// (UNSUPPORTED when the partition is outside this path, or the group tables
+// would exceed TC_TABLE_BUDGET).
 bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, double threshold, double *trace)
 {
     if (!X || !X2 || X == X2 || X->NB != X2->NB || X->matrix_precision != X2->matrix_precision)
@@ -947,57 +1089,97 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     if (!c || !eb_to_device(X) || !eb_to_device(X2))
         return false;
     const int NB = X->NB, MB = X->MB;
-    const size_t n_img = (size_t) NB * MB * 4 * IMG;
+    const bool dbl = X->matrix_precision == double_real;
+    int *flags = reinterpret_cast<int *>(static_cast<unsigned char *>(c->d_small) + 32768);
+    unsigned *maxbits = reinterpret_cast<unsigned *>(flags + 8); // max |x| of X, for the split's scale
+    unsigned char *pin = static_cast<unsigned char *>(c->pinned) + 8192;
+    // sizes of the group tables
+    const int ngroups = (NB + TC_GROUP - 1) / TC_GROUP;
+    if (!CUDA_OK(cudaMemsetAsync(flags, 0, 64, c->stream)))
+        return false;
+    const int cgrid = std::min(ngroups, c->sm_count * 8);
+    if (dbl)
+        tc_count_kernel<double><<<cgrid, TC_THREADS, 0, c->stream>>>(tc_view<double>(X), flags);
+    else
+        tc_count_kernel<float><<<cgrid, TC_THREADS, 0, c->stream>>>(tc_view<float>(X), flags);
+    if (!LAUNCH_OK("tc_count_kernel"))
+        return false;
+    int hf[8];
+    if (!CUDA_OK(cudaMemcpyAsync(pin, flags, sizeof(hf), cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+        return false;
+    memcpy(hf, pin, sizeof(hf));
+    if (hf[2])
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "multiply_x2_tc: a block column outside 0..NB-1");
+        return false;
+    }
+    const int grid = c->sm_count * TcShape::CTAS;
+    TcTab tab{};
+    tab.jcap = std::max(hf[5], 1);
+    tab.kcap = std::max(hf[6], 1);
+    tab.pcap = std::max(hf[7], 1);
+    tab.wcap = (tab.kcap + TcShape::TILES - 1) / TcShape::TILES;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t J = tab.jcap, K = tab.kcap, P = tab.pcap, W = tab.wcap, g = grid;
+    const size_t sz[9] = {g * J * 4, g * J * 8, g * J, g * (J + 1) * 4, g * K * 4, g * K * 4,
+                          g * P * 4, g * P * 16, g * (W + 1) * 4};
+    size_t tab_bytes = 0;
+    for (size_t s : sz)
+        tab_bytes += al(s);
+    if (hf[7] == INT_MAX || tab_bytes > TC_TABLE_BUDGET)
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply_x2_tc: group tables of %zu bytes above the budget",
+                       tab_bytes);
+        return false;
+    }
+    const size_t n_img = (size_t) NB * MB * 4 * IMG;
     const size_t off_tr = al(n_img * sizeof(tc_t));
-    const size_t off_flags = al(off_tr + (size_t) 2 * NB * sizeof(double));
-    const size_t off_zero = al(off_flags + 64);
-    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_zero + IMG * sizeof(tc_t)));
+    const size_t off_zero = al(off_tr + (size_t) 2 * NB * sizeof(double));
+    const size_t off_tab = al(off_zero + IMG * sizeof(tc_t));
+    unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_tab + tab_bytes));
     if (!scr)
         return false;
     tc_t *img = reinterpret_cast<tc_t *>(scr);
     double *dA = reinterpret_cast<double *>(scr + off_tr);
     double *dC = dA + NB;
-    int *flags = reinterpret_cast<int *>(scr + off_flags);
-    unsigned *maxbits = reinterpret_cast<unsigned *>(flags + 8); // max |x| of X, for the split's scale
     tc_t *zimg = reinterpret_cast<tc_t *>(scr + off_zero);
+    {
+        unsigned char *p = scr + off_tab;
+        auto take = [&](int i) {
+            unsigned char *q = p;
+            p += al(sz[i]);
+            return q;
+        };
+        tab.jb = reinterpret_cast<int *>(take(0));
+        tab.jslot = reinterpret_cast<uint2 *>(take(1));
+        tab.jmask = take(2);
+        tab.jstart = reinterpret_cast<int *>(take(3));
+        tab.klist = reinterpret_cast<int *>(take(4));
+        tab.ttouch = reinterpret_cast<int *>(take(5));
+        tab.ptile = reinterpret_cast<int *>(take(6));
+        tab.list = reinterpret_cast<uint4 *>(take(7));
+        tab.wstart = reinterpret_cast<int *>(take(8));
+    }
     if (!CUDA_OK(cudaMemsetAsync(flags, 0, 64, c->stream)) ||
         !CUDA_OK(cudaMemsetAsync(zimg, 0, IMG * sizeof(tc_t), c->stream)) ||
         !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)))
         return false;
-    const int sgrid = (int) min((long long) NB * MB, (long long) c->sm_count * 32);
-    bool ok = X->matrix_precision == double_real
-                  ? tc_split<double>(c, X, sgrid, maxbits, img)
-                  : tc_split<float>(c, X, sgrid, maxbits, img);
+    const int sgrid = (int) std::min((long long) NB * MB, (long long) c->sm_count * 32);
+    bool ok = dbl ? tc_split<double>(c, X, sgrid, maxbits, img) : tc_split<float>(c, X, sgrid, maxbits, img);
     if (!ok)
         return false;
-    // the two-CTA shape first; the one-CTA shape if a group exceeded it
-    unsigned char *pin = static_cast<unsigned char *>(c->pinned) + 8192;
-    int hf[4];
-    for (int shape = 0; shape < 2; ++shape)
-    {
-        if (shape == 1 && !CUDA_OK(cudaMemsetAsync(flags, 0, 20, c->stream)))
-            return false;
-        if (X->matrix_precision == double_real)
-            ok = shape == 0 ? tc_launch<double, TcSmall>(c, X, X2, img, zimg, threshold, dA, dC, flags)
-                            : tc_launch<double, TcBig>(c, X, X2, img, zimg, threshold, dA, dC, flags);
-        else
-            ok = shape == 0 ? tc_launch<float, TcSmall>(c, X, X2, img, zimg, threshold, dA, dC, flags)
-                            : tc_launch<float, TcBig>(c, X, X2, img, zimg, threshold, dA, dC, flags);
-        if (!ok)
-            return false;
-        if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
-            return false;
-        memcpy(hf, pin, sizeof(hf));
-        if (!hf[2] || hf[3])
-            break; // fitted (or timed out: reported below)
-    }
+    ok = dbl ? tc_launch<double>(c, X, X2, tab, img, zimg, threshold, dA, dC, flags, grid)
+             : tc_launch<float>(c, X, X2, tab, img, zimg, threshold, dA, dC, flags, grid);
+    if (!ok)
+        return false;
     double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 256);
     b200_sum_rows_kernel<<<1, 1024, 0, c->stream>>>(dA, dC, NB, out);
     if (!LAUNCH_OK("b200_sum_rows_kernel"))
         return false;
-    if (!CUDA_OK(cudaMemcpyAsync(pin + 64, out, 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
+    if (!CUDA_OK(cudaMemcpyAsync(pin, flags, 16, cudaMemcpyDeviceToHost, c->stream)) ||
+        !CUDA_OK(cudaMemcpyAsync(pin + 64, out, 16, cudaMemcpyDeviceToHost, c->stream)) || !b200_sync())
         return false;
+    memcpy(hf, pin, 4 * sizeof(int));
     X2->mirror = MIRROR_DEVICE_NEWER;
     if (trace)
         memcpy(trace, pin + 64, 2 * sizeof(double));
@@ -1008,7 +1190,7 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     }
     if (hf[2])
     {
-        b200_set_error(BML_B200_ERR_UNSUPPORTED, "multiply_x2_tc: a group of block rows exceeds the kernel's capacity");
+        b200_set_error(BML_B200_ERR_INVALID, "multiply_x2_tc: a group's tables differ from their counted sizes");
         return false;
     }
     if (hf[0])
@@ -1084,8 +1266,8 @@ extern "C" int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, dou
         bool ok = false, on_tc = false;
         if (!closing)
         {
-            // Blocks other than 32 x 32, or a group beyond the tensor-core
-            // kernel's capacities, are an expected outcome here: that
+            // Blocks other than 32 x 32, or a partition beyond the
+            // tensor-core kernel's limits, are an expected outcome here: that
             // iteration runs on the exact product, noted as information.
             const int verbose = b200_swap_verbose(0);
             ok = on_tc = eb_multiply_x2_tc(static_cast<bml_matrix_ellblock_t *>(D),
@@ -1096,7 +1278,7 @@ extern "C" int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, dou
                 bml_b200_clear_error();
                 if (verbose)
                     fprintf(stderr, "[bml_b200 info] ellblock_sp2_mixed: iteration %d runs on the exact block "
-                                    "product (outside the tensor-core kernel's capacities)\n", it);
+                                    "product (outside the tensor-core kernel's limits)\n", it);
             }
             else if (!on_tc)
                 b200_set_error(b200_get_error(), "ellblock_sp2_mixed: tensor-core X^2 failed in iteration %d", it);

@@ -438,8 +438,9 @@ BML_B200_API int bml_b200_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double thr
  * precision; blocks are kept as by bml_multiply_x2 (kb == ib
  * or max |x| > threshold).  trace (may be NULL) receives {tr X, tr X2}.  Every
  * block of X and X2 must be 32 x 32 (bml_set_block_sizes); otherwise
- * UNSUPPORTED.  Blocks of a row come out in first-touch order over the four
- * block rows the kernel handles together, not row by row. */
+ * UNSUPPORTED; so are NB > 65536, MB > 32767, and inputs whose per-group
+ * tables would take more than 16 GiB of device memory.  Blocks of a row come
+ * out in ascending block column. */
 BML_B200_API int bml_b200_ellblock_multiply_x2_tc(bml_matrix_t *X, bml_matrix_t *X2, double threshold,
     double *trace);
 
@@ -448,7 +449,7 @@ BML_B200_API int bml_b200_ellblock_multiply_x2_tc(bml_matrix_t *X, bml_matrix_t 
  * iterations the matrix-precision X^2 of bml_multiply_x2; adds, copies, the
  * branch choice and the stop tests as bml_b200_sp2.  A bulk iteration that
  * the tensor-core X^2 rejects as UNSUPPORTED (blocks other than 32 x 32, or
- * four block rows together beyond its capacities) runs on the exact X^2.
+ * a partition beyond its limits) runs on the exact X^2.
  * info as for bml_b200_sp2_mixed ([4] is 0; [6] and [7] count the
  * iterations that ran on the tensor cores). */
 BML_B200_API int bml_b200_ellblock_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double threshold,

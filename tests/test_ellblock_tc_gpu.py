@@ -67,7 +67,7 @@ def free(h):
 
 @pytest.mark.parametrize("prec", [DOUBLE, SINGLE])
 # (6, 2.24): 57 block neighbours, about 7000 block products per group of four
-# block rows, more than the two-CTA shape takes: the one-CTA shape runs
+# block rows
 @pytest.mark.parametrize("L,radius", [(3, 1.0), (4, 2.0), (6, 2.24)])
 def test_tc_x2_matches_block_product(prec, L, radius):
     H = block_lattice(L, radius)
@@ -166,6 +166,59 @@ def test_tc_x2_against_fp64_dense(L, radius):
         B.lib.bml_b200_reset_block_sizes()
 
 
+@pytest.mark.parametrize("L,radius", [(6, 2.0), (8, 2.0)])
+def test_tc_x2_of_a_filled_iterate(L, radius):
+    """X^2 of X1 = H^2 (the exact block product at 1e-6), whose rows hold up
+    to every block of a radius-4 neighbourhood: groups of four block rows
+    with hundreds of block columns and tens of thousands of block pairs, as
+    in the later SP2 iterations.  Against the FP64 dense product of X1, with
+    the bound grown with the number of FP32 accumulation steps per tile
+    (measured at 6^3: 4.4e-5 of S with rows of 152 blocks)."""
+    import torch
+    thr = 1e-6
+    H = block_lattice(L, radius, seed=5)
+    nb, N = L ** 3, H.shape[0]
+    set_partition(nb, nb)
+    try:
+        X = from_dense(H)
+        X1 = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+        Xt = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+        B.check()
+        B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(X, X1, C.c_double(thr))))
+        B.check()
+        X1d = to_dense(X1, N)
+        widest = int((X1d.reshape(nb, 32, nb, 32).any(axis=(1, 3))).sum(axis=1).max())
+        trt = (C.c_double * 2)()
+        st = B.lib.bml_b200_ellblock_multiply_x2_tc(X1, Xt, thr, trt)
+        assert st == B.OK, B.lib.bml_b200_error_string(st)
+        want, S, keep = _fp64_block_x2(X1d, nb, thr)
+        got = torch.from_numpy(to_dense(Xt, N)).to(want.device)
+        gkeep = got.reshape(nb, 32, nb, 32).abs().amax(dim=(1, 3)) > 0
+        both = (gkeep & keep)[:, None, :, None].expand(nb, 32, nb, 32).reshape(N, N)
+        err = torch.where(both, (got - want).abs(), torch.zeros((), dtype=torch.float64, device=want.device))
+        ratio = float((err / S.clamp_min(1e-300)).max())
+        # an output tile accumulates up to `widest` pairs, six FP32 steps
+        # each (two K = 16 halves of hi*hi, hi*lo and lo*hi), each step
+        # within one unit in the last place (2^-23) of the running sum <= S
+        eps = 6 * widest * 2.0 ** -23
+        print("tc X^2 of X1 at %d^3 (widest row of X1: %d blocks): max |err|/S %.2e (bound %.2e)"
+              % (L, widest, ratio, eps))
+        assert widest > 100
+        assert ratio <= eps
+        differ = gkeep ^ keep
+        if bool(differ.any()):
+            norm = want.reshape(nb, 32, nb, 32).abs().amax(dim=(1, 3))
+            smax = S.reshape(nb, 32, nb, 32).amax(dim=(1, 3))
+            assert bool(((norm[differ] - thr).abs() <= eps * smax[differ]).all())
+        assert trt[1] == pytest.approx(float(torch.trace(want)), rel=eps)
+        for h in (X, X1, Xt):
+            free(h)
+        del want, S, got, err
+        torch.cuda.empty_cache()
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
+
+
 def test_tc_rejects_other_block_sizes():
     set_partition(16, 16, bs=8)
     try:
@@ -186,8 +239,8 @@ def test_ellblock_sp2_mixed_against_fp64():
     """bml_b200_ellblock_sp2_mixed: bulk SP2 iterations on the tensor-core X^2,
     the last two on the matrix-precision block product, against the same
     solve with every iteration exact (nclose = maxiter).  On the 4^3 block
-    lattice (N = 2048, radius 2) the iterates stay within the group limits
-    of the tensor-core path for all ten iterations.  Tolerances: trace,
+    lattice (N = 2048, radius 2), all eight bulk iterations run on the
+    tensor cores.  Tolerances: trace,
     band energy tr(DH) and ||D - D_exact||_F / ||D_exact||_F within 1e-4
     (the split carries about 1e-5 relative per X^2)."""
     L, radius, iters, nclose, thr = 4, 2.0, 10, 2, 1e-6
