@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-tc", action="store_true",
                     help="run the small tensor-core ELLBLOCK case for an ncu capture (10^3 block lattice)")
+    ap.add_argument("--profile-tc-wide", action="store_true",
+                    help="the same for X1 = H^2 (block rows of a later SP2 iteration)")
     ap.add_argument("--profile-eb-ops", action="store_true",
                     help="the one-pass ELLBLOCK operations, once each, for an ncu capture (7^3 block lattice)")
     ap.add_argument("--eb-ops-L", type=int, default=7, help="block lattice side for --profile-eb-ops")
@@ -728,15 +730,31 @@ def ellblock_case(L):
     return H, nb * 32
 
 
-def run_profile_tc():
-    """Three tensor-core X^2 calls on the 10^3 block lattice (N = 32000)."""
+def run_profile_tc(wide=False):
+    """Three tensor-core X^2 calls on the 10^3 block lattice (N = 32000): of
+    H, or (wide) of X1 = H^2 by the exact block product, whose block rows are
+    those of a later SP2 iteration; the three calls run inside the NVTX range
+    "tc"."""
     import bml_b200 as B
     H, n = ellblock_case(10)
+    X = H
+    if wide:
+        X = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+        B.check()
+        B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(H, X, C.c_double(1e-6))))
+        B.check()
     X2 = B.lib.bml_zero_matrix(3, 2, n, n, 0)
     tr = (C.c_double * 2)()
+    B.check(B.lib.bml_b200_synchronize())
+    nvtx = _nvtx()
+    nvtx.range_push("tc")
     for _ in range(3):
-        B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, X2, 1e-6, tr))
-    print(json.dumps({"profile_case": "10^3 block lattice, tensor-core X^2", "trace": list(tr)}))
+        B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(X, X2, 1e-6, tr))
+    B.check(B.lib.bml_b200_synchronize())
+    nvtx.range_pop()
+    print(json.dumps({"profile_case": "10^3 block lattice, tensor-core X^2 of %s" % ("X1 = H^2" if wide else "H"),
+                      "trace": list(tr), "blocks_x": int(B.lib.bml_b200_nnz(X)) // 1024,
+                      "blocks_x2": int(B.lib.bml_b200_nnz(X2)) // 1024}))
 
 
 def block_lattice_products(L, radius):
@@ -919,8 +937,8 @@ def main():
     if args.profile:
         run_profile_case()
         return
-    if args.profile_tc:
-        run_profile_tc()
+    if args.profile_tc or args.profile_tc_wide:
+        run_profile_tc(wide=args.profile_tc_wide)
         return
     if args.profile_ops:
         run_profile_ops()

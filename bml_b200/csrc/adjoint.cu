@@ -15,7 +15,11 @@
 // where Q_n keeps the entries of G on the pattern of T(X_n^2) and P_n keeps
 // the pattern of X_n (entries outside it were dropped by an earlier
 // threshold, so no gradient reaches them).  The products are the library's
-// sparse products (threshold 0); the restrictions are one kernel.
+// sparse products; where the unordered kernel takes them, their masked form
+// forms only the entries on X_n's pattern (the rest would be dropped by P_n),
+// so no product wider than X_n is ever stored; otherwise (the ordered form,
+// or rows the dense tier takes) they are formed at threshold 0 and then
+// restricted, one kernel.
 // Memory: X is checkpointed every `every` iterations in the forward pass and
 // each segment is recomputed before its backward steps (bit-identically with
 // the ordered products and on the dense tier; the unordered sparse products
@@ -101,6 +105,20 @@ Mat product(bml_matrix_t *A, bml_matrix_t *B, int M0)
     return Mat();
 }
 
+// A*B at P's pattern (C with P's M), through the masked form of the unordered
+// product; an empty Mat with no status set where that form does not apply.
+Mat masked_product(bml_matrix_t *A, bml_matrix_t *B, bml_matrix_t *P)
+{
+    Mat C = zero(bml_get_precision(A), bml_get_N(A), bml_get_M(P));
+    if (!C.m)
+        return Mat();
+    bool taken = false;
+    if (!ell_multiply_masked(static_cast<bml_matrix_ellpack_t *>(A), static_cast<bml_matrix_ellpack_t *>(B),
+                             static_cast<bml_matrix_ellpack_t *>(P), C.e(), &taken))
+        return Mat();
+    return C;
+}
+
 // One SP2 step X -> X_next (X2 is scratch of X's shape); returns the branch
 // (0: X^2, 1: 2X - X^2).  Same calls, in the same order, as bml_b200_sp2.
 int sp2_step(bml_matrix_t *X, bml_matrix_t *X2, double threshold, double occupation)
@@ -143,20 +161,39 @@ Mat step_back(bml_matrix_t *Xn, const Mat &G, int branch, double threshold, bml_
         float minus1f = -1.0f;
         bml_scale_inplace(prec == double_real ? (void *) &minus1 : (void *) &minus1f, Gh.m);
     }
-    Mat T1 = product(Gh.m, Xt.m, 2 * M);
-    if (!T1.m)
+    // on X_n's pattern where the masked form applies, else whole
+    Mat T1 = masked_product(Gh.m, Xt.m, Xn);
+    Mat T2 = T1.m ? masked_product(Xt.m, Gh.m, Xn) : Mat();
+    if (err())
         return Mat();
-    Mat T2 = product(Xt.m, Gh.m, bml_get_M(T1.m));
-    if (!T2.m)
-        return Mat();
-    int MS = bml_get_M(T1.m) + bml_get_M(T2.m) + (branch ? bml_get_M(G.m) : 0);
+    const bool on_pattern = T1.m && T2.m;
+    if (!on_pattern)
+    {
+        T1 = product(Gh.m, Xt.m, 2 * M);
+        if (!T1.m)
+            return Mat();
+        T2 = product(Xt.m, Gh.m, bml_get_M(T1.m));
+        if (!T2.m)
+            return Mat();
+    }
+    // T1 + T2 (+ 2G).  On X_n's pattern T1 and T2 share it, and G is first
+    // restricted to it, so the sum is no wider than X_n.
+    Mat Gr;
+    if (on_pattern && branch)
+    {
+        Gr = zero(prec, N, M);
+        if (!Gr.m || !ell_restrict(static_cast<bml_matrix_ellpack_t *>(G.m), static_cast<bml_matrix_ellpack_t *>(Xn),
+                                   Gr.e()))
+            return Mat();
+    }
+    int MS = on_pattern ? M : bml_get_M(T1.m) + bml_get_M(T2.m) + (branch ? bml_get_M(G.m) : 0);
     MS = MS < N ? MS : N;
     Mat S = copy_of(T1.m, MS);
     if (!S.m || err())
         return Mat();
     bml_add(S.m, T2.m, 1.0, 1.0, 0.0);
     if (branch)
-        bml_add(S.m, G.m, 1.0, 2.0, 0.0);
+        bml_add(S.m, on_pattern ? Gr.m : G.m, 1.0, 2.0, 0.0);
     if (err())
         return Mat();
     Mat Gn = zero(prec, N, M);

@@ -82,6 +82,8 @@ struct FastArgs
     int sym_try;                     // X^2 of a square matrix: use the symmetric form if X is symmetric
     void *Uv; int *Ui; int *Un; int ldu; // upper parts of the rows (symmetric form)
     int *lcnt; int *lfill;           // mirrored entries per row: count, and placement cursor
+    const int *Pi; const int *Pn; int ldp; // masked form: row i of C takes exactly P's row i pattern
+    int masked;
 };
 
 // Row j of B through its offset: B itself, or its sorted copy.
@@ -260,6 +262,7 @@ struct FastMisc
     double dA;        // sum of A's diagonal entries in the row
     double dC;        // pre-threshold diagonal of C (when touched)
     int lo, hi;       // column span of the row
+    int plo, phi;     // masked form: column span of P's row
     int count;        // kept entries written so far
     int touched;      // touched columns so far (TOUCH)
     int diag_touched;
@@ -315,6 +318,7 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
     if (TOUCH)
         for (int c = threadIdx.x; c < tile / 32; c += W * 32)
             tbits[c] = 0u;
+    const bool masked = g.masked != 0;
 
     for (;;)
     {
@@ -329,6 +333,8 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
             ms.touched = 0;
             ms.diag_touched = 0;
             ms.bad = 0;
+            ms.plo = INT_MAX;
+            ms.phi = -1;
         }
         __syncthreads();
         const int i = ms.row;
@@ -336,6 +342,42 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
             break;
         const int ni = g.An[i];
         const size_t arow = (size_t) i * g.lda;
+        // masked form: P's row, written with zero values (the tiles below
+        // overwrite the columns they form), and its column span
+        const int np = masked ? g.Pn[i] : 0;
+        if (masked)
+        {
+            int plo = INT_MAX, phi = -1, bad = (np < 0 || np > g.ldp || np > g.Mc) ? 1 : 0;
+            if (!bad)
+                for (int q = threadIdx.x; q < np; q += W * 32)
+                {
+                    const int col = g.Pi[(size_t) i * g.ldp + q];
+                    if (col < 0 || col >= g.ncols)
+                        bad = 1;
+                    plo = min(plo, col);
+                    phi = max(phi, col);
+                    outi[(size_t) i * ldo + q] = col;
+                    outv[(size_t) i * ldo + q] = T(0);
+                }
+            for (int o = 16; o; o >>= 1)
+            {
+                plo = min(plo, __shfl_xor_sync(FULL, plo, o));
+                phi = max(phi, __shfl_xor_sync(FULL, phi, o));
+                bad |= __shfl_xor_sync(FULL, bad, o);
+            }
+            if (lane == 0)
+            {
+                if (bad)
+                    ms.bad = 1;
+                if (phi >= 0)
+                {
+                    atomicMin(&ms.plo, plo);
+                    atomicMax(&ms.phi, phi);
+                }
+            }
+            __syncthreads();
+        }
+        const int plo = masked ? ms.plo : 0;
         // span of the row, A's diagonal, validation of A's row
         {
             int lo = INT_MAX, hi = -1, bad = (ni < 0 || ni > g.lda) ? 1 : 0;
@@ -355,6 +397,18 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
                     if (nj <= 0)
                         continue;
                     const int *ki = row_of<T>(g, j).k;
+                    if (masked)
+                    {
+                        // the part of row j at columns >= the start of P's row
+                        const int q = lower_bound(ki, nj, plo);
+                        cur[jp] = q;
+                        if (q < nj)
+                        {
+                            lo = min(lo, ki[q]);
+                            hi = max(hi, ki[nj - 1]);
+                        }
+                        continue;
+                    }
                     if (sym)
                     {
                         // the part of row j at columns >= i
@@ -394,7 +448,7 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
             __syncthreads();
             continue;
         }
-        const int lo = ms.lo, hi = ms.hi;
+        const int lo = ms.lo, hi = masked ? min(ms.hi, ms.phi) : ms.hi;
         const bool multi = hi - lo + 1 > tile;
         for (int c0 = lo; c0 <= hi; c0 += tile)
         {
@@ -424,7 +478,7 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
                     const long long o = __shfl_sync(FULL, mo, t);
                     const int *ki = o >= 0 ? g.Bi + o : g.Si + (-o - 1);
                     const T *kv = o >= 0 ? Bv + o : Sv + (-o - 1);
-                    int pos = (multi || sym) ? cur[jp] : 0;
+                    int pos = (multi || sym || masked) ? cur[jp] : 0;
                     while (pos < nj)
                     {
                         int k[U];
@@ -470,6 +524,27 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
                 }
             }
             __syncthreads();
+            if (masked)
+            {
+                // P's columns in this tile take their sums (0 where nothing
+                // was added); then the window is zeroed
+                for (int q = threadIdx.x; q < np; q += W * 32)
+                {
+                    const int col = g.Pi[(size_t) i * g.ldp + q];
+                    if (col >= c0 && col < cend)
+                    {
+                        const T x = acc[col - c0];
+                        outv[(size_t) i * ldo + q] = x;
+                        if (col == i)
+                            ms.dC = (double) x;
+                    }
+                }
+                __syncthreads();
+                for (int c = threadIdx.x; c < len; c += W * 32)
+                    acc[c] = T(0);
+                __syncthreads();
+                continue;
+            }
             // Scan of the window in column order: count per warp, prefix over
             // warps, then write the kept entries and zero the window.
             const int per = (((len + W - 1) / W) + 31) & ~31;
@@ -541,7 +616,7 @@ __global__ void __launch_bounds__(W * 32, MINB) fast_x2_kernel(FastArgs g)
         }
         if (threadIdx.x == 0)
         {
-            const int ll = ms.count;
+            const int ll = masked ? np : ms.count;
             if (sym)
                 g.Un[i] = ll; // the mirror kernels complete the row
             else
@@ -960,6 +1035,39 @@ bool ell_multiply_unordered(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bm
     const bool touch = check_pre || !(threshold >= 0.0);
     return A->matrix_precision == double_real ? fast_multiply_typed<double>(g, trace, required_M, touch)
                                               : fast_multiply_typed<float>(g, trace, required_M, touch);
+}
+
+bool ell_multiply_masked(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *P,
+                         bml_matrix_ellpack_t *C, bool *taken)
+{
+    *taken = false;
+    if (!A || !B || !P || !C || C == A || C == B || C == P || A->matrix_precision != B->matrix_precision ||
+        A->matrix_precision != C->matrix_precision || A->N != C->N || P->N != C->N || P->M > C->M)
+    {
+        b200_set_error(BML_B200_ERR_INVALID, "masked multiply: operands of one precision, C distinct, "
+                                             "P and C with A's rows, C at least as wide as P");
+        return false;
+    }
+    if (g_x2_exact || !ell_unordered_fits(A) || !ell_unordered_fits(B) || ell_dense_fits(A, B, C, 0.0))
+        return false;
+    if (!ell_to_device(A) || (B != A && !ell_to_device(B)) || (P != A && P != B && !ell_to_device(P)) ||
+        !ell_to_device(C))
+        return false;
+    if (C->mirror == MIRROR_HOST_NEWER)
+        C->mirror = MIRROR_SYNCED;
+    *taken = true;
+    g_last_dense = false;
+    FastArgs g{};
+    g.Av = A->d_value; g.Ai = A->d_index; g.An = A->d_nnz; g.lda = A->ld; g.NA = A->N;
+    g.Bv = B->d_value; g.Bi = B->d_index; g.Bn = B->d_nnz; g.ldb = B->ld; g.NB = B->N;
+    g.Cv = C->d_value; g.Ci = C->d_index; g.Cn = C->d_nnz; g.ldc = C->ld; g.Mc = C->M;
+    g.Pi = P->d_index; g.Pn = P->d_nnz; g.ldp = P->ld; g.masked = 1;
+    g.thr = 0.0;
+    g.ncols = B->N > C->N ? B->N : C->N;
+    const bool ok = A->matrix_precision == double_real ? fast_multiply_typed<double>(g, nullptr, nullptr, false)
+                                                       : fast_multiply_typed<float>(g, nullptr, nullptr, false);
+    ell_mark_device(C);
+    return ok;
 }
 
 // Allows (1, the default) or forbids (0) the symmetric form of the unordered

@@ -148,6 +148,13 @@ bool ell_x2_exact();
 bool ell_unordered_fits(const bml_matrix_ellpack_t *A);
 bool ell_multiply_unordered(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C,
                             double threshold, double *trace, int *required_M, bool check_pre);
+// C = A*B at P's pattern (the masked form of the unordered product): row i
+// of C lists P's row i columns in P's order with the sums of their products
+// (0 where there are none), no threshold.  *taken is false, with no status
+// set, where the form does not apply (the ordered form selected, rows too
+// wide for the kernel, or operands the dense tier takes); C needs P's M.
+bool ell_multiply_masked(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *P,
+                         bml_matrix_ellpack_t *C, bool *taken);
 // The dense tier of the unordered product (ellpack_dense.cu): a GEMM on dense
 // images when both operands' rows fill at least 40 % of their columns.
 bool ell_dense_fits(bml_matrix_ellpack_t *A, bml_matrix_ellpack_t *B, bml_matrix_ellpack_t *C, double threshold);

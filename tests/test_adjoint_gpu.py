@@ -143,6 +143,32 @@ def test_adjoint_matches_dense_autograd(iters, every):
     assert np.abs(g[mask] - ref_on_pattern).max() <= 1e-8 * scale
 
 
+@pytest.mark.unordered
+@pytest.mark.parametrize("every", [4, 1])
+def test_adjoint_unordered_matches_dense_autograd(every):
+    """The unordered form, whose backward products are formed only on the
+    iterates' patterns (the masked products): against the dense FP64
+    autograd reference to the same 1e-8, and against the ordered form's
+    gradient to 1e-10 of the largest entry (the two add products in other
+    orders)."""
+    iters = 12
+    N, M, v, ix, nz, vv, Vd = _problem()
+    loss_u, (g_u, _, _) = _loss_and_grad(v, ix, nz, vv, N, M, iters, every)
+    old = B.lib.bml_b200_set_x2_exact(1)
+    try:
+        loss_o, (g_o, _, _) = _loss_and_grad(v, ix, nz, vv, N, M, iters, every)
+    finally:
+        B.lib.bml_b200_set_x2_exact(old)
+    ref_loss, ref_grad = _dense_reference_grad(_dense(v, ix, nz, N, M), Vd, iters)
+    assert loss_u == pytest.approx(ref_loss, rel=1e-10)
+    mask = (np.arange(M)[None, :] < nz[:, None]).reshape(-1)
+    rows = np.repeat(np.arange(N), M)
+    ref_on_pattern = ref_grad[rows[mask], ix[mask]]
+    scale = np.abs(ref_on_pattern).max()
+    assert np.abs(g_u[mask] - ref_on_pattern).max() <= 1e-8 * scale
+    assert np.abs(g_u[mask] - g_o[mask]).max() <= 1e-10 * scale
+
+
 def _loss_and_pattern(hv, ix, nz, vv, N, M, iters):
     H = B.Ellpack.from_arrays(hv, ix, nz, N, M)
     V = B.Ellpack.from_arrays(vv, ix, nz, N, M)
