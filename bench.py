@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--profile-tc", action="store_true",
                     help="run the small tensor-core ELLBLOCK case for an ncu capture (10^3 block lattice)")
     ap.add_argument("--profile-tc-wide", action="store_true",
-                    help="the same for X1 = H^2 (block rows of a later SP2 iteration)")
+                    help="the same for the SP2 iterate after one iteration (the second iteration's product)")
     ap.add_argument("--profile-eb-ops", action="store_true",
                     help="the one-pass ELLBLOCK operations, once each, for an ncu capture (7^3 block lattice)")
     ap.add_argument("--eb-ops-L", type=int, default=7, help="block lattice side for --profile-eb-ops")
@@ -465,7 +465,7 @@ def formed_fraction(X, n, sample=400, seed=0):
 # --profile, 18.57 G reference product terms; profiles/x2_symmetric_lattice30.md):
 # the product kernel's dram__bytes_read.sum + dram__bytes_write.sum
 NCU_X2_PRODUCTS = 18570945128
-NCU_X2_KERNEL_DRAM = 1130652000 + 163951616
+NCU_X2_KERNEL_DRAM = 1111612672 + 169511936
 
 
 def x2_roofline(B, H, info):
@@ -512,7 +512,7 @@ def x2_roofline(B, H, info):
             "peak_source": src,
             "traffic": NCU_X2_KERNEL_DRAM / NCU_X2_PRODUCTS * P,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the product kernel "
-                              "(fast_x2_kernel, symmetric form) on the 30^3 case (bench.py --profile: 1.29 GB for "
+                              "(fast_x2_kernel, symmetric form) on the 30^3 case (bench.py --profile: 1.28 GB for "
                               "18.57 G reference product terms), scaled by this call's product terms",
             "kernel": "fast_x2_kernel (symmetric form: columns k >= i), one ELLPACK X^2 on the SP2 iterate of "
                       "iteration %d; kernel_seconds by CUDA events around it on the library stream" % (SP2_ITERS - 1),
@@ -732,17 +732,17 @@ def ellblock_case(L):
 
 def run_profile_tc(wide=False):
     """Three tensor-core X^2 calls on the 10^3 block lattice (N = 32000): of
-    H, or (wide) of X1 = H^2 by the exact block product, whose block rows are
-    those of a later SP2 iteration; the three calls run inside the NVTX range
-    "tc"."""
+    H, or (wide) of X1, the iterate after one exact SP2 iteration from H
+    (the product of the second SP2 iteration); the three calls run inside the
+    NVTX range "tc"."""
     import bml_b200 as B
     H, n = ellblock_case(10)
     X = H
     if wide:
         X = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+        info = (C.c_double * 8)()
         B.check()
-        B.lib.bml_free_memory(C.c_void_p(B.lib.bml_multiply_x2(H, X, C.c_double(1e-6))))
-        B.check()
+        B.check(B.lib.bml_b200_ellblock_sp2_mixed(H, X, 1e-6, n / 2.0, 1, -1.0, 0, 1, info))
     X2 = B.lib.bml_zero_matrix(3, 2, n, n, 0)
     tr = (C.c_double * 2)()
     B.check(B.lib.bml_b200_synchronize())
@@ -752,7 +752,7 @@ def run_profile_tc(wide=False):
         B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(X, X2, 1e-6, tr))
     B.check(B.lib.bml_b200_synchronize())
     nvtx.range_pop()
-    print(json.dumps({"profile_case": "10^3 block lattice, tensor-core X^2 of %s" % ("X1 = H^2" if wide else "H"),
+    print(json.dumps({"profile_case": "10^3 block lattice, tensor-core X^2 of %s" % ("the SP2 iterate X1" if wide else "H"),
                       "trace": list(tr), "blocks_x": int(B.lib.bml_b200_nnz(X)) // 1024,
                       "blocks_x2": int(B.lib.bml_b200_nnz(X2)) // 1024}))
 

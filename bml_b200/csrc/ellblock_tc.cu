@@ -58,18 +58,16 @@ constexpr int TC_THREADS = 128;   // 4 warps; warp q owns TMEM lanes 32q..32q+31
 constexpr int TC_GROUP = 4;       // block rows per group (M = 128)
 constexpr int IMG = TB * TB;      // 16-bit elements per block image (2 KB)
 constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
-// Shape of the kernel: TILES output tiles live per CTA (a wave), CTAS CTAs
-// per SM (two, so that one CTA's set-up and epilogue overlap the other's
-// MMAs), ABUF and BBUF buffers in the left and right operand rings, ACC
-// accumulators of 32 TMEM columns per tile: with 1, hi*hi, hi*lo and lo*hi
-// all add into one; with 2, the small cross terms hi*lo + lo*hi add into a
-// second one, so the large sum takes a third of the accumulation steps.
-template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int ACC_> struct TcCfg
+// Shape of the kernel: TILES output tiles of 32 TMEM columns live per CTA (a
+// wave), CTAS CTAs per SM (two, so that one CTA's set-up and epilogue overlap
+// the other's MMAs), ABUF and BBUF buffers in the left and right operand
+// rings.  Measured on the 16^3 block lattice's X^2: 8 tiles x 2 CTAs 6.9 ms,
+// 16 tiles x 1 CTA 10.0 ms.
+template <int TILES_, int CTAS_, int ABUF_, int BBUF_> struct TcCfg
 {
-    static constexpr int TILES = TILES_, CTAS = CTAS_, ABUF = ABUF_, BBUF = BBUF_, ACC = ACC_;
-    static_assert(CTAS * TILES * 32 * ACC <= 512, "tensor memory holds 512 columns per SM");
+    static constexpr int TILES = TILES_, CTAS = CTAS_, ABUF = ABUF_, BBUF = BBUF_;
+    static_assert(CTAS * TILES * 32 <= 512, "tensor memory holds 512 columns per SM");
     static_assert(TILES <= 16, "tile numbers take 4 bits of a pair");
-    static_assert(ACC == 1 || ACC == 2, "one or two accumulators per tile");
 };
 #ifndef B200_TC_TILES
 #define B200_TC_TILES 8
@@ -77,10 +75,7 @@ template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int ACC_> struct TcCfg
 #ifndef B200_TC_CTAS
 #define B200_TC_CTAS 2
 #endif
-#ifndef B200_TC_ACC
-#define B200_TC_ACC 1
-#endif
-using TcShape = TcCfg<B200_TC_TILES, B200_TC_CTAS, 3, 8, B200_TC_ACC>;
+using TcShape = TcCfg<B200_TC_TILES, B200_TC_CTAS, 3, 8>;
 
 // Operand type of the split: FP16 (11-bit significands: hi and lo carry
 // about 22 bits, the dropped lo*lo about 2^-22 of a product) with the whole
@@ -523,7 +518,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&S.tmem)),
-                     "r"(TC_TILES * 32 * Cfg::ACC)
+                     "r"(TC_TILES * 32)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -878,8 +873,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         break;
                     }
                     tc_fence_after();
-                    const unsigned d = tbase + (unsigned) (tile * 32 * Cfg::ACC);
-                    const unsigned dx = d + (Cfg::ACC == 2 ? 32u : 0u); // the cross terms' accumulator
+                    const unsigned d = tbase + (unsigned) (tile * 32);
                     const unsigned a0 = su32(S.a[acur][0]), a1 = su32(S.a[acur][1]);
                     const unsigned b0 = su32(S.b[b][0]), b1 = su32(S.b[b][1]);
                     unsigned acc = (started >> tile) & 1u;
@@ -893,8 +887,8 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         const uint64_t bh = smem_desc(b0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
                         const uint64_t bl = smem_desc(b1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
                         umma_f16(d, ah, bh, acc);
-                        umma_f16(dx, ah, bl, Cfg::ACC == 2 ? acc : 1u);
-                        umma_f16(dx, al, bh, 1u);
+                        umma_f16(d, ah, bl, 1u);
+                        umma_f16(d, al, bh, 1u);
                         acc = 1u;
                     }
                     umma_commit(&S.empty_b[b]);
@@ -925,15 +919,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             for (int t = 0; t < nt; ++t)
             {
                 float v[32];
-                tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32 * Cfg::ACC), v);
-                if (Cfg::ACC == 2)
-                {
-                    float vx[32];
-                    tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 64 + 32), vx);
-#pragma unroll
-                    for (int c = 0; c < 32; ++c)
-                        v[c] += vx[c];
-                }
+                tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32), v);
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
                     v[c] *= unscale; // undo the split's 2^s on both factors
@@ -1018,7 +1004,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TILES * 32 * Cfg::ACC)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TILES * 32)
                      : "memory");
 }
 
