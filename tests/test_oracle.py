@@ -164,8 +164,12 @@ def test_restatement_ellblock_x2_matches_reference(ref, prec, thr):
     assert np.array_equal(rnz, onz)
     for ib in range(nb):
         assert np.array_equal(rix[ib * s2.MB:ib * s2.MB + rnz[ib]], oix[ib * nb:ib * nb + onz[ib]])
-    assert tr[0] == pytest.approx(rtr[0], rel=1e-12 if prec == O.DOUBLE else 1e-6)
-    assert tr[1] == pytest.approx(rtr[1], rel=1e-12 if prec == O.DOUBLE else 1e-6)
+    # the reference sums the traces in an OpenMP reduction, whose order
+    # follows the thread count: compare within the rounding of the sum,
+    # relative to the sum of the magnitudes (tr X can cancel)
+    eps = 1e-12 if prec == O.DOUBLE else 1e-6
+    assert abs(tr[0] - rtr[0]) <= eps * np.abs(np.diag(D).astype(np.float64)).sum()
+    assert abs(tr[1] - rtr[1]) <= eps * np.abs(np.diag(d2).astype(np.float64)).sum()
 
 
 def test_restatement_on_example_hamiltonian(oracle_mod):
