@@ -1401,7 +1401,11 @@ __device__ __forceinline__ void eb_wait(uint64_t *bar, unsigned parity, int *fla
         atomicExch(flag, 1);
 }
 
-template <typename T>
+// FUSED: each block product's inner sums by fused multiply-adds (one
+// rounding per step, half the FP64 instructions; the unordered form of the
+// library), or, as the restatement and the reference's -std=c99 build, by a
+// separately rounded product and sum (the ordered form, bit for bit).
+template <typename T, bool FUSED>
 __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, EbView<T> B, EbView<T> C, double thr,
                                                                   int use_norm_inf_fast, int cap, T *slab,
                                                                   int *lists, int *marks, double *dA, double *dC,
@@ -1577,8 +1581,14 @@ __global__ void __launch_bounds__(EB32_THREADS, 4) eb_mul32_kernel(EbView<T> A, 
 #pragma unroll
                             for (int c = 0; c < 8; ++c)
                             {
-                                const T p = mul_rn(lrow[l], V::at(bv[c / NV], c % NV));
-                                s[c] = l == 0 ? p : add_rn(s[c], p);
+                                if (FUSED)
+                                    s[c] = l == 0 ? lrow[l] * V::at(bv[c / NV], c % NV)
+                                                  : fma(lrow[l], V::at(bv[c / NV], c % NV), s[c]);
+                                else
+                                {
+                                    const T p = mul_rn(lrow[l], V::at(bv[c / NV], c % NV));
+                                    s[c] = l == 0 ? p : add_rn(s[c], p);
+                                }
                             }
                         }
 #pragma unroll
@@ -1794,7 +1804,7 @@ bool eb_multiply_typed(bml_matrix_ellblock_t *A, bml_matrix_ellblock_t *B, bml_m
         if (bs32)
         {
             const size_t smem = sizeof(EbS32<T>);
-            auto k = eb_mul32_kernel<T>;
+            auto k = ell_x2_exact() ? eb_mul32_kernel<T, false> : eb_mul32_kernel<T, true>;
             if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
                 return false;
             k<<<grid, EB32_THREADS, smem, c->stream>>>(view<T>(A), view<T>(B), view<T>(C), thr, fast_norm ? 1 : 0,

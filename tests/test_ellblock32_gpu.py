@@ -229,3 +229,52 @@ def full_lists(H, nb, bs):
         indexb[ib * nb:ib * nb + len(cols)] = cols
         nnzb[ib] = len(cols)
     return indexb, nnzb, nb
+
+
+@pytest.mark.unordered
+@pytest.mark.parametrize("prec", [DOUBLE, SINGLE], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("L,radius", [(4, 2.0), (6, 2.24)])
+def test_x2_blocks32_fused_within_bound(prec, L, radius):
+    """The unordered form of the 32 x 32 block product, whose inner sums are
+    fused multiply-adds, against the FP64 dense product: every entry of a
+    block kept by both within 1e-12 of its product magnitude sum S (FP32:
+    2 n 2^-24 S, n = 32 x the widest block row), blocks kept by one side
+    only at the threshold; the same block pattern and traces otherwise."""
+    import torch
+    from test_ellblock_tc_gpu import _fp64_block_x2, free, from_dense, set_partition, to_dense
+    thr = 1e-6
+    H = block_lattice(L, radius)
+    nb, N = L ** 3, H.shape[0]
+    set_partition(nb, nb)
+    try:
+        X = from_dense(H, prec)
+        X2 = B.lib.bml_zero_matrix(ELLBLOCK, prec, N, N, 0)
+        B.check()
+        p = B.lib.bml_multiply_x2(X, X2, C.c_double(thr))
+        B.check()
+        tr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(2,)).copy()
+        B.lib.bml_free_memory(C.c_void_p(p))
+        Hq = H.astype(np.float32).astype(np.float64) if prec == SINGLE else H
+        want, S, keep = _fp64_block_x2(Hq, nb, thr)
+        got = torch.from_numpy(to_dense(X2, N, prec)).to(want.device)
+        widest = int((Hq.reshape(nb, 32, nb, 32) != 0).any(axis=(1, 3)).sum(axis=1).max())
+        eps = 1e-12 if prec == DOUBLE else 2.0 * 32 * widest * 2.0 ** -24
+        gkeep = got.reshape(nb, 32, nb, 32).abs().amax(dim=(1, 3)) > 0
+        both = (gkeep & keep)[:, None, :, None].expand(nb, 32, nb, 32).reshape(N, N)
+        err = torch.where(both, (got - want).abs(), torch.zeros((), dtype=torch.float64, device=want.device))
+        ratio = float((err / S.clamp_min(1e-300)).max())
+        print("fused block X^2 %d^3 %s: max |err|/S %.2e (bound %.2e)"
+              % (L, "fp64" if prec == DOUBLE else "fp32", ratio, eps))
+        assert ratio <= eps
+        differ = gkeep ^ keep
+        if bool(differ.any()):
+            norm = want.reshape(nb, 32, nb, 32).abs().amax(dim=(1, 3))
+            smax = S.reshape(nb, 32, nb, 32).amax(dim=(1, 3))
+            assert bool(((norm[differ] - thr).abs() <= eps * smax[differ]).all())
+        assert tr[1] == pytest.approx(float(torch.trace(want)), rel=eps)
+        for h in (X, X2):
+            free(h)
+        del want, S, got, err
+        torch.cuda.empty_cache()
+    finally:
+        B.lib.bml_b200_reset_block_sizes()
