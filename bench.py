@@ -835,9 +835,11 @@ def run_profile_eb_ops(L=7):
 def ellblock_sp2_leg(iters=5, nclose=2):
     """The mixed ELLBLOCK SP2 configuration on the 16^3 block lattice (4096
     block rows of 32, N = 131072, threshold 1e-6, occupation N/2): the first
-    `iters` iterations from X0, every X^2 exact (FP64) against bulk X^2 on the
-    tensor cores and the last `nclose` exact, with their errors.  Device time
-    by CUDA events on the library stream."""
+    `iters` iterations from X0, every X^2 in FP64 against bulk X^2 on the
+    tensor cores and the last `nclose` in FP64, with their errors, for both
+    splits of the tensor-core X^2 (FP16 hi/lo with FP32 accumulation, and
+    8-bit slices with exact INT32 accumulation).  Device time by CUDA events
+    on the library stream."""
     import bml_b200 as B
     H, n = ellblock_case(16)
     # warm-up: the exact and tensor-core X^2 size their device scratch once
@@ -848,10 +850,17 @@ def ellblock_sp2_leg(iters=5, nclose=2):
     hh = C.c_void_p(W)
     B.lib.bml_deallocate(C.byref(hh))
     out = {}
-    for name, nc in (("fp64", iters), ("mixed", nclose)):
+    old_split = B.lib.bml_b200_set_tc_split(0)
+    for name, nc, split in (("fp64", iters, 0), ("mixed", nclose, 0), ("mixed_8bit", nclose, 1)):
         D = B.lib.bml_zero_matrix(3, 2, n, n, 0)
         B.check()
         info = (C.c_double * 8)()
+        B.lib.bml_b200_set_tc_split(split)
+        if split:  # size the 8-bit split's scratch outside the timed call
+            Wm = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+            B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, Wm, 1e-6, None))
+            hh = C.c_void_p(Wm)
+            B.lib.bml_deallocate(C.byref(hh))
         with _StdoutToStderr():
             B.check(B.lib.bml_b200_synchronize())
             B.check(B.lib.bml_b200_event_record(6))
@@ -862,17 +871,23 @@ def ellblock_sp2_leg(iters=5, nclose=2):
                      "idempotency_t_minus_t2": info[3], "tc_iterations": int(info[6]), "nnz": int(B.lib.bml_b200_nnz(D))}
         hh = C.c_void_p(D)
         B.lib.bml_deallocate(C.byref(hh))
+    B.lib.bml_b200_set_tc_split(old_split)
     hh = C.c_void_p(H)
     B.lib.bml_deallocate(C.byref(hh))
     B.lib.bml_b200_reset_block_sizes()
-    e, m = out["fp64"], out["mixed"]
+    e, m, m8 = out["fp64"], out["mixed"], out["mixed_8bit"]
+    rel = lambda a, b: abs(a - b) / abs(b)
+    m8.update({"speedup": e["s"] / m8["s"], "trace_rel_err": rel(m8["trace"], e["trace"]),
+               "energy_rel_err": rel(m8["energy_trDH"], e["energy_trDH"]),
+               "split": "8-bit slices (5 per entry), exact INT32 accumulation, FP64 recombination"})
     return {"workload": "SP2 on the 16^3 block lattice Hamiltonian (4096 block rows of 32x32, N=131072, radius 2, "
                         "thr 1e-6, occ N/2), first %d iterations from X0" % iters,
             "iterations": iters, "closing_fp64": nclose, "fp64": e, "mixed": m, "speedup": e["s"] / m["s"],
-            "trace_rel_err": abs(m["trace"] - e["trace"]) / abs(e["trace"]),
-            "energy_rel_err": abs(m["energy_trDH"] - e["energy_trDH"]) / abs(e["energy_trDH"]),
-            "note": "bulk X^2 on the tensor cores (FP16 hi/lo split, FP32 accumulation), the closing "
-                    "iterations on the exact FP64 block product"}
+            "trace_rel_err": rel(m["trace"], e["trace"]),
+            "energy_rel_err": rel(m["energy_trDH"], e["energy_trDH"]),
+            "mixed_8bit": m8,
+            "note": "bulk X^2 on the tensor cores (mixed: FP16 hi/lo split, FP32 accumulation; mixed_8bit: "
+                    "8-bit slices, exact INT32 accumulation), the closing iterations on the FP64 block product"}
 
 
 def ellblock_leg(reps=3):
@@ -902,7 +917,12 @@ def ellblock_leg(reps=3):
         B.check()
 
     te = timed(exact)
+    old_split = B.lib.bml_b200_set_tc_split(1)
+    t8 = timed(lambda: B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, Xt, 1e-6, tr)))
+    tr8 = B.lib.bml_trace(Xt)
+    B.lib.bml_b200_set_tc_split(0)
     tt = timed(lambda: B.check(B.lib.bml_b200_ellblock_multiply_x2_tc(H, Xt, 1e-6, tr)))
+    B.lib.bml_b200_set_tc_split(old_split)
     tre, trt = B.lib.bml_trace(Xe), B.lib.bml_trace(Xt)
     nnz_h = B.lib.bml_b200_nnz(H)
     P = block_lattice_products(16, 2.0)
@@ -915,6 +935,7 @@ def ellblock_leg(reps=3):
     tc_peak = peaks.get("bf16_tflops") or 1590.0
     res = {"workload": "X^2 of H, 16^3 block lattice, 4096 block rows of 32x32 (N=131072), radius 2, thr 1e-6",
            "tc_s": tt, "fp64_s": te, "speedup": te / tt, "trace_rel_err": abs(trt - tre) / abs(tre),
+           "tc_8bit_s": t8, "tc_8bit_trace_rel_err": abs(tr8 - tre) / abs(tre),
            "nnz_h": int(nnz_h), "nnz_x2": int(B.lib.bml_b200_nnz(Xt)), "block_products": P,
            "fp64_tflops": flops / te / 1e12,
            "fp64_ceiling_tflops": FP64_NOMINAL_TFLOPS,

@@ -115,6 +115,7 @@ _PROTOS = {
     "bml_b200_multiply_x2_rows": (_i, [_vp, _vp, _d, _i, _i, _dp]),
     "bml_b200_sp2_update_rows": (_i, [_vp, _vp, _d, _i, _i, _i]),
     "bml_b200_ellblock_multiply_x2_tc": (_i, [_vp, _vp, _d, _dp]),
+    "bml_b200_set_tc_split": (_i, [_i]),
     "bml_b200_gen_block_lattice": (_vp, [_i, _d, _i, C.c_ulonglong, _i]),
     "bml_b200_ellblock_sp2_mixed": (_i, [_vp, _vp, _d, _d, _i, _d, _i, _i, _dp]),
     "bml_b200_gen_chain": (_i, [_i, _i, C.c_ulonglong, _dp, _ip, _ip]),

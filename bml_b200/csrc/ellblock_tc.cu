@@ -63,9 +63,10 @@ constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
 // the other's MMAs), ABUF and BBUF buffers in the left and right operand
 // rings.  Measured on the 16^3 block lattice's X^2: 8 tiles x 2 CTAs 6.9 ms,
 // 16 tiles x 1 CTA 10.0 ms.
-template <int TILES_, int CTAS_, int ABUF_, int BBUF_> struct TcCfg
+template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int ABYTES_ = 16384, int BBYTES_ = 4096> struct TcCfg
 {
     static constexpr int TILES = TILES_, CTAS = CTAS_, ABUF = ABUF_, BBUF = BBUF_;
+    static constexpr int ABYTES = ABYTES_, BBYTES = BBYTES_; // one left / right operand buffer
     static_assert(CTAS * TILES * 32 <= 512, "tensor memory holds 512 columns per SM");
     static_assert(TILES <= 16, "tile numbers take 4 bits of a pair");
 };
@@ -169,6 +170,128 @@ __global__ void tc_split_kernel(const T *pool, const int *nnzb, int NB, int MB, 
     }
 }
 
+// --- exact mode: 8-bit slices with INT32 accumulation (kind::i8) --------
+// Every entry x of scalar row r, as a left operand, is written
+//   x = sigma_r 2^-6 (a1 + 2^-7 a2 + 2^-14 a3 + 2^-21 a4 + 2^-28 a5) + e,
+// |a_s| <= 64 (signed 8-bit), |e| <= 2^-35 sigma_r, with sigma_r = 2^e_r the
+// power of two just above the row's largest entry; as a right operand the
+// same with tau_c of its scalar column.  A product of two entries is then
+// 2^-12 sigma_r tau_c sum_{s,t} a_s b_t 2^-7(s+t-2); the terms with
+// s + t <= 6 (15 MMAs per block pair, each K = 32) are kept, the others are
+// below 2^-33 sigma_r tau_c.  Each level L = s + t sums in its own INT32
+// accumulator in TMEM, exactly (no rounding at all: a term is at most
+// 64 x 64 x 32 = 2^17 per level and pair, five terms at L = 6, so up to
+// 3276 pairs per tile fit in 2^31), and the epilogue combines the five
+// levels in FP64, exactly.  The result differs from the exact product only
+// by the slicing, about 2^-33 sigma_r tau_c per product term, without the
+// FP32 accumulation error of the FP16 form.  (Four slices, 2^-27 per term,
+// left SP2's trace 1.6e-5 from the exact solve: the error is relative to the
+// row and column maxima, not to each entry.)
+constexpr int TC8_SLICES = 5;
+constexpr int TC8_LEVELS = TC8_SLICES;  // s + t = 2..6
+constexpr int TC8_IMG = TB * TB;        // bytes per 8-bit slice image of a block (1 KB)
+constexpr int TC8_BLOCK_BYTES = 2 * TC8_SLICES * TC8_IMG; // left slices | right slices
+constexpr int TC16_BLOCK_BYTES = 8 * IMG;                 // left hi, lo | right hi, lo
+constexpr int TC8_MAX_COLS = 3276;      // block columns per group the level sums hold
+constexpr unsigned TC8_LBO = 128, TC8_SBO = 256;
+
+// Byte offset of element (row, k) in an 8-bit K-major no-swizzle image:
+// 16-byte rows of 16 k, 8-row core matrices of 128 bytes, the two k-chunks
+// of an 8-row group side by side (LBO = 128 B), row groups at SBO = 256 B.
+__device__ __forceinline__ int img8_off(int row, int k)
+{
+    return (row >> 3) * 256 + (k >> 4) * 128 + (row & 7) * 16 + (k & 15);
+}
+
+// Exponent e with 2^e > m >= 0 (m given by its bits; 0 for m = 0).
+__device__ __forceinline__ int tc8_exp(unsigned long long bits)
+{
+    const double m = __longlong_as_double((long long) bits);
+    if (!(m > 0.0))
+        return 0;
+    int e = 0;
+    frexp(m, &e); // m in [2^(e-1), 2^e)
+    return e;
+}
+
+// Largest |x| of every scalar row (rowmax) and column (colmax) of X, as
+// the bits of non-negative doubles (which order like the values).  One warp
+// per stored block: lane = column, a loop over the block's rows.
+template <typename T>
+__global__ void tc8_max_kernel(const T *pool, const int *indexb, const int *nnzb, int NB, int MB, long long slot_elems,
+                               unsigned long long *rowmax, unsigned long long *colmax)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long) gridDim.x * blockDim.x) >> 5;
+    for (long long s = ((long long) blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < (long long) NB * MB; s += warps)
+    {
+        const int ib = (int) (s / MB), jp = (int) (s % MB);
+        if (jp >= nnzb[ib])
+            continue;
+        const int jb = indexb[s];
+        const T *x = pool + s * slot_elems;
+        double cm = 0.0;
+        for (int r = 0; r < TB; ++r)
+        {
+            const double v = fabs((double) x[r * TB + lane]);
+            cm = fmax(cm, v);
+            double rm = v;
+            for (int o = 16; o; o >>= 1)
+                rm = fmax(rm, __shfl_xor_sync(FULL, rm, o));
+            if (lane == 0)
+                atomicMax(&rowmax[(size_t) ib * TB + r], (unsigned long long) __double_as_longlong(rm));
+        }
+        atomicMax(&colmax[(size_t) jb * TB + lane], (unsigned long long) __double_as_longlong(cm));
+    }
+}
+
+// The slices a1..a4 of u (|u| < 1), each in [-64, 64].
+__device__ __forceinline__ void tc8_slices(double u, signed char (&a)[TC8_SLICES])
+{
+    double y = u * 64.0;
+#pragma unroll
+    for (int s = 0; s < TC8_SLICES; ++s)
+    {
+        const double q = rint(y);
+        a[s] = (signed char) (int) q;
+        y = (y - q) * 128.0; // exact: y - q is y's fraction, scaled by a power of two
+    }
+}
+
+// Slice every stored block of X into its 8-bit images at img + slot * 8 KB:
+// left slices 1..4 (element (r, k) of the block, scaled by sigma of scalar
+// row r) at +0, +1 KB, +2 KB, +3 KB, right slices 1..4 (element (n, k) =
+// block (k, n), scaled by tau of scalar column n) at +4 KB ... +7 KB.
+template <typename T>
+__global__ void tc8_split_kernel(const T *pool, const int *indexb, const int *nnzb, int NB, int MB,
+                                 long long slot_elems, const unsigned long long *rowmax,
+                                 const unsigned long long *colmax, signed char *img)
+{
+    for (long long s = blockIdx.x; s < (long long) NB * MB; s += gridDim.x)
+    {
+        const int ib = (int) (s / MB), jp = (int) (s % MB);
+        if (jp >= nnzb[ib])
+            continue;
+        const int jb = indexb[s];
+        const T *x = pool + s * slot_elems;
+        signed char *o = img + s * TC8_BLOCK_BYTES;
+        for (int e = threadIdx.x; e < IMG; e += blockDim.x)
+        {
+            const int r = e >> 5, c = e & 31;
+            const double v = (double) x[e];
+            signed char a[TC8_SLICES];
+            tc8_slices(ldexp(v, -tc8_exp(rowmax[(size_t) ib * TB + r])), a);
+#pragma unroll
+            for (int q = 0; q < TC8_SLICES; ++q)
+                o[q * TC8_IMG + img8_off(r, c)] = a[q];
+            tc8_slices(ldexp(v, -tc8_exp(colmax[(size_t) jb * TB + c])), a);
+#pragma unroll
+            for (int q = 0; q < TC8_SLICES; ++q)
+                o[(TC8_SLICES + q) * TC8_IMG + img8_off(c, r)] = a[q];
+        }
+    }
+}
+
 // --- tcgen05 / mbarrier primitives ---------------------------------------
 __device__ __forceinline__ unsigned su32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
 
@@ -192,6 +315,20 @@ __device__ __forceinline__ void umma_f16(unsigned tmem_d, uint64_t adesc, uint64
                  "setp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
                  ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u),
+                   "r"(0u), "r"(0u)
+                 : "memory");
+}
+
+// kind::i8 instruction descriptor: D S32 (2), A and B signed 8-bit (1),
+// both K-major, N = 32, M = 128.
+constexpr uint32_t TC8_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, unsigned accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                 ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(TC8_IDESC), "r"(accumulate), "r"(0u), "r"(0u),
                    "r"(0u), "r"(0u)
                  : "memory");
 }
@@ -282,7 +419,7 @@ template <class Cfg> struct TcSmem
 {
     union
     {
-        tc_t a[Cfg::ABUF][2][4 * IMG]; // left operands, hi and lo: 128 x 32 (8 KB each)
+        unsigned char a[Cfg::ABUF][Cfg::ABYTES]; // left operands: 128 x 32, every part
         struct
         {
             unsigned jbits[TC_NWCAP]; // the group's block columns jb (bitmap over NB)
@@ -294,8 +431,9 @@ template <class Cfg> struct TcSmem
     };
     union
     {
-        tc_t b[Cfg::BBUF][2][IMG];         // right operands, hi and lo: 32 x 32 (2 KB each)
+        unsigned char b[Cfg::BBUF][Cfg::BBYTES]; // right operands: 32 x 32, every part
         float stage[TC_GROUP][TB][TB + 1]; // epilogue transpose (the ring is idle then)
+        double dstage[TC_GROUP][TB][17];   // the same for the 8-bit mode's FP64 values, 16 columns at a time
     };
     uint64_t full_a[Cfg::ABUF], full_b[Cfg::BBUF]; // bulk copies landed
     uint64_t empty_b[Cfg::BBUF];                   // MMAs reading a B buffer (and all before) done
@@ -491,14 +629,23 @@ __device__ __forceinline__ unsigned rec_slot(const uint4 &r, int q)
 // flags: [0] row overflow, [1] widest kept row, [2] a group's tables outside
 // their sizes, [3] a tensor-core wait timed out, [4] next group to claim,
 // [8] max |x| of X (the split's scale)
-template <typename T, class Cfg>
+// I8: the 8-bit slice mode (kind::i8, four INT32 level accumulators per
+// tile, rowmax/colmax give the scales); otherwise the FP16 hi/lo mode.
+// img: 8 KB of operand images per block slot, left half then right half.
+template <typename T, class Cfg, bool I8>
 __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
-    tc_x2_kernel(TcView<T> X, TcOut<T> C, TcTab G, const tc_t *img, const tc_t *zimg, double thr,
-                 double *dA, double *dC, int *flags)
+    tc_x2_kernel(TcView<T> X, TcOut<T> C, TcTab G, const unsigned char *img, const unsigned char *zimg, double thr,
+                 const unsigned long long *rowmax, const unsigned long long *colmax, double *dA, double *dC,
+                 int *flags)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     constexpr int TC_TILES = Cfg::TILES, TC_ABUF = Cfg::ABUF, TC_BBUF = Cfg::BBUF;
-    static_assert(TC_TILES >= 8, "wave counters: NB / TILES <= 4 * TC_NWCAP");
+    constexpr int TUSED = TC_TILES * 32 * (I8 ? TC8_LEVELS : 1); // tensor memory columns used
+    constexpr int TCOLS = TUSED <= 32 ? 32 : TUSED <= 64 ? 64 : TUSED <= 128 ? 128 : TUSED <= 256 ? 256 : 512;
+    constexpr int BLK = I8 ? TC8_BLOCK_BYTES : TC16_BLOCK_BYTES; // image bytes per block slot
+    static_assert(TUSED <= 512, "tensor memory holds 512 columns per SM");
+    static_assert(Cfg::ABYTES >= TC_GROUP * BLK / 2 && Cfg::BBYTES >= BLK / 2, "operand buffers");
+    static_assert(!I8 || TC_TILES * TC8_LEVELS <= 32, "started bits: one per tile and level");
     TcSmem<Cfg> &S = *reinterpret_cast<TcSmem<Cfg> *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ngroups = (X.NB + TC_GROUP - 1) / TC_GROUP;
@@ -518,7 +665,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&S.tmem)),
-                     "r"(TC_TILES * 32)
+                     "r"(TCOLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -814,17 +961,25 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                             S.dead = 1;
                             break;
                         }
-                        mbar_expect(&S.full_a[a], 2 * 4 * IMG * 2);
+                        // 16 KB either way: FP16 hi and lo (2 parts of 2 KB
+                        // per block), or 4 slices of 1 KB per block; part p
+                        // of the four blocks stacks into the 128-row operand
+                        constexpr int NPART = I8 ? TC8_SLICES : 2;
+                        constexpr unsigned PBYTES = BLK / 2 / NPART;
+                        mbar_expect(&S.full_a[a], TC_GROUP * BLK / 2);
+                        unsigned char *abytes = S.a[a];
 #pragma unroll
                         for (int q = 0; q < TC_GROUP; ++q)
                         {
                             const unsigned jp = rec_slot(r, q);
 #pragma unroll
-                            for (int part = 0; part < 2; ++part)
+                            for (int part = 0; part < NPART; ++part)
                             {
-                                const tc_t *src =
-                                    jp != 0xFFFFu ? img + (((size_t) (ib0 + q) * X.MB + jp) * 4 + part) * IMG : zimg;
-                                bulk_copy(reinterpret_cast<unsigned char *>(S.a[a][part]) + q * 2048, src, IMG * 2,
+                                const unsigned char *src =
+                                    jp != 0xFFFFu
+                                        ? img + ((size_t) (ib0 + q) * X.MB + jp) * BLK + part * PBYTES
+                                        : zimg;
+                                bulk_copy(abytes + part * (TC_GROUP * PBYTES) + q * PBYTES, src, PBYTES,
                                           &S.full_a[a]);
                             }
                         }
@@ -836,10 +991,10 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         S.dead = 1;
                         break;
                     }
-                    mbar_expect(&S.full_b[b], 2 * IMG * 2);
-                    // the right hi and lo images are adjacent in both places:
-                    // one 4 KB copy
-                    bulk_copy(S.b[b][0], img + (size_t) r.y * 4 * IMG + 2 * IMG, 2 * IMG * 2, &S.full_b[b]);
+                    mbar_expect(&S.full_b[b], BLK / 2);
+                    // the right operand's parts are adjacent in both places:
+                    // one copy
+                    bulk_copy(S.b[b], img + (size_t) r.y * BLK + BLK / 2, BLK / 2, &S.full_b[b]);
                     ++gp;
                 }
             }
@@ -873,9 +1028,31 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         break;
                     }
                     tc_fence_after();
+                    if (I8)
+                    {
+                        // slices s, t (0-based) with s + t <= 3 into level
+                        // s + t's INT32 accumulator; K = 32 per instruction
+                        const unsigned a0 = su32(S.a[acur]), b0 = su32(S.b[b]);
+#pragma unroll
+                        for (int sa = 0; sa < TC8_SLICES; ++sa)
+#pragma unroll
+                            for (int sb = 0; sb + sa < TC8_LEVELS; ++sb)
+                            {
+                                const int lev = sa + sb;
+                                const unsigned bit = 1u << (tile * TC8_LEVELS + lev);
+                                const unsigned acc = (started & bit) ? 1u : 0u;
+                                started |= bit;
+                                umma_i8(tbase + (unsigned) (tile * 32 * TC8_LEVELS + lev * 32),
+                                        smem_desc(a0 + sa * (TC_GROUP * TC8_IMG), TC8_LBO, TC8_SBO),
+                                        smem_desc(b0 + sb * TC8_IMG, TC8_LBO, TC8_SBO), acc);
+                            }
+                        umma_commit(&S.empty_b[b]);
+                        ++gp;
+                        continue;
+                    }
                     const unsigned d = tbase + (unsigned) (tile * 32);
-                    const unsigned a0 = su32(S.a[acur][0]), a1 = su32(S.a[acur][1]);
-                    const unsigned b0 = su32(S.b[b][0]), b1 = su32(S.b[b][1]);
+                    const unsigned a0 = su32(S.a[acur]), a1 = a0 + TC_GROUP * 2 * IMG;
+                    const unsigned b0 = su32(S.b[b]), b1 = b0 + 2 * IMG;
                     unsigned acc = (started >> tile) & 1u;
                     started |= 1u << tile;
 #pragma unroll
@@ -916,7 +1093,73 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                 break;
             }
             // ---- epilogue: warp q reads block row ib0+q of every tile ----
-            for (int t = 0; t < nt; ++t)
+            if (I8)
+            {
+                const double srow = myrow < X.NB ? ldexp(1.0, tc8_exp(rowmax[(size_t) myrow * TB + lane]) - 12) : 0.0;
+                for (int t = 0; t < nt; ++t)
+                {
+                    // the four levels, highest first: v = ((D5 2^-7 + D4) 2^-7 + D3) 2^-7 + D2
+                    double v[32];
+                    for (int lev = TC8_LEVELS - 1; lev >= 0; --lev)
+                    {
+                        float w[32];
+                        tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32 * TC8_LEVELS + lev * 32),
+                                  w);
+#pragma unroll
+                        for (int c = 0; c < 32; ++c)
+                            v[c] = (lev == TC8_LEVELS - 1 ? 0.0 : v[c] * 0x1p-7) + (double) __float_as_int(w[c]);
+                    }
+                    const int kb = G.klist[t0 + t];
+                    if (myrow >= X.NB || !((G.ttouch[t0 + t] >> warp) & 1))
+                        continue;
+                    double mx = 0.0, diag = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c)
+                    {
+                        v[c] *= srow * ldexp(1.0, tc8_exp(colmax[(size_t) kb * TB + c]));
+                        mx = fmax(mx, fabs(v[c]));
+                        diag = c == lane ? v[c] : diag;
+                    }
+                    for (int o = 16; o; o >>= 1)
+                        mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
+                    const bool keep = kb == myrow || mx > thr;
+                    if (!keep)
+                        continue;
+                    if (kb == myrow)
+                    {
+                        double dd = diag;
+                        for (int o = 16; o; o >>= 1)
+                            dd += __shfl_xor_sync(FULL, dd, o);
+                        trc += dd;
+                    }
+                    if (kept < C.MB)
+                    {
+                        // lane = block row; through shared memory, 16
+                        // columns at a time, so that the warp writes the
+                        // row-major block in contiguous runs
+                        T *dst = C.pool + ((size_t) myrow * C.MB + kept) * C.slot;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                        {
+#pragma unroll
+                            for (int c = 0; c < 16; ++c)
+                                S.dstage[warp][lane][c] = v[h * 16 + c];
+                            __syncwarp();
+#pragma unroll 4
+                            for (int e = lane; e < 32 * 16; e += 32)
+                            {
+                                const int r = e >> 4, c = e & 15;
+                                dst[r * TB + h * 16 + c] = (T) S.dstage[warp][r][c];
+                            }
+                            __syncwarp();
+                        }
+                        if (lane == 0)
+                            C.indexb[(size_t) myrow * C.MB + kept] = kb;
+                    }
+                    ++kept;
+                }
+            }
+            for (int t = 0; t < (I8 ? 0 : nt); ++t)
             {
                 float v[32];
                 tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32), v);
@@ -1004,7 +1247,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TILES * 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TCOLS)
                      : "memory");
 }
 
@@ -1027,26 +1270,54 @@ template <typename T> TcView<T> tc_view(const bml_matrix_ellblock_t *X)
 }
 
 template <typename T>
-bool tc_launch(B200Context *c, const bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, const TcTab &tab,
-               const tc_t *img, const tc_t *zimg, double threshold, double *dA, double *dC, int *flags, int grid)
+bool tc8_split(B200Context *c, const bml_matrix_ellblock_t *X, int sgrid, unsigned long long *rowmax,
+               unsigned long long *colmax, signed char *img)
 {
-    const size_t smem = sizeof(TcSmem<TcShape>) + 1024;
-    auto k = tc_x2_kernel<T, TcShape>;
+    const T *pool = static_cast<const T *>(X->d_pool);
+    tc8_max_kernel<T><<<sgrid, 256, 0, c->stream>>>(pool, X->d_indexb, X->d_nnzb, X->NB, X->MB, X->slot_elems, rowmax,
+                                                   colmax);
+    if (!LAUNCH_OK("tc8_max_kernel"))
+        return false;
+    tc8_split_kernel<T><<<sgrid, 256, 0, c->stream>>>(pool, X->d_indexb, X->d_nnzb, X->NB, X->MB, X->slot_elems, rowmax,
+                                                     colmax, img);
+    return LAUNCH_OK("tc8_split_kernel");
+}
+
+// The 8-bit mode's shape: 3 tiles of five 32-column level accumulators
+// (480 of the 512 TMEM columns), one CTA per SM; buffers of five slices.
+using TcShape8 = TcCfg<3, 1, 3, 8, TC_GROUP * TC8_SLICES * TC8_IMG, TC8_SLICES * TC8_IMG>;
+
+template <typename T, class Cfg, bool I8>
+bool tc_launch(B200Context *c, const bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, const TcTab &tab,
+               const unsigned char *img, const unsigned char *zimg, double threshold, const unsigned long long *rowmax,
+               const unsigned long long *colmax, double *dA, double *dC, int *flags, int grid)
+{
+    // a one-CTA shape holds all of the SM's tensor memory: ask for enough
+    // shared memory that a second CTA cannot share the SM
+    const size_t smem = std::max(sizeof(TcSmem<Cfg>) + 1024, Cfg::CTAS == 1 ? size_t(120) << 10 : size_t(0));
+    auto k = tc_x2_kernel<T, Cfg, I8>;
     if (!CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
         return false;
     k<<<grid, TC_THREADS, smem, c->stream>>>(
         tc_view<T>(X), TcOut<T>{static_cast<T *>(X2->d_pool), X2->d_indexb, X2->d_nnzb, X2->MB, X2->slot_elems}, tab,
-        img, zimg, threshold, dA, dC, flags);
+        img, zimg, threshold, rowmax, colmax, dA, dC, flags);
     return LAUNCH_OK("tc_x2_kernel");
 }
+
+// The split of the tensor-core X^2: 0 FP16 hi/lo with FP32 accumulation, 1
+// 8-bit slices with exact INT32 accumulation.
+static int g_tc_split = 0;
 
 // Bytes of device memory the tables of one X^2 may take (all CTAs).
 constexpr size_t TC_TABLE_BUDGET = size_t(16) << 30;
 
-// X2 = X*X on the tensor cores (FP16 hi/lo split, FP32 accumulation); X and
-// X2 must have blocks of 32 throughout.  Returns false with a status set
+// X2 = X*X on the tensor cores, in the split g_tc_split selects (FP16 hi/lo
+// with FP32 accumulation, or 8-bit slices with INT32 accumulation); X and X2
+// must have blocks of 32 throughout.  Returns false with a status set
 // (UNSUPPORTED when the partition is outside this path, or the group tables
-// would exceed TC_TABLE_BUDGET).
+// would exceed TC_TABLE_BUDGET; in the 8-bit split also NB > 32768, or a
+// group with more than TC8_MAX_COLS block columns, whose level sums could
+// pass 2^31).
 bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, double threshold, double *trace)
 {
     if (!X || !X2 || X == X2 || X->NB != X2->NB || X->matrix_precision != X2->matrix_precision)
@@ -1099,12 +1370,21 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
         b200_set_error(BML_B200_ERR_INVALID, "multiply_x2_tc: a block column outside 0..NB-1");
         return false;
     }
-    const int grid = c->sm_count * TcShape::CTAS;
+    const bool i8 = g_tc_split == 1;
+    if (i8 && (NB > 4 * TC_NWCAP * TcShape8::TILES || hf[5] > TC8_MAX_COLS))
+    {
+        b200_set_error(BML_B200_ERR_UNSUPPORTED,
+                       "multiply_x2_tc: the 8-bit split takes NB <= %d and groups of <= %d block columns",
+                       4 * TC_NWCAP * TcShape8::TILES, TC8_MAX_COLS);
+        return false;
+    }
+    const int tiles = i8 ? TcShape8::TILES : TcShape::TILES;
+    const int grid = c->sm_count * (i8 ? TcShape8::CTAS : TcShape::CTAS);
     TcTab tab{};
     tab.jcap = std::max(hf[5], 1);
     tab.kcap = std::max(hf[6], 1);
     tab.pcap = std::max(hf[7], 1);
-    tab.wcap = (tab.kcap + TcShape::TILES - 1) / TcShape::TILES;
+    tab.wcap = (tab.kcap + tiles - 1) / tiles;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t J = tab.jcap, K = tab.kcap, P = tab.pcap, W = tab.wcap, g = grid;
     const size_t sz[9] = {g * J * 4, g * J * 8, g * J, g * (J + 1) * 4, g * K * 4, g * K * 4,
@@ -1118,17 +1398,23 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
                        tab_bytes);
         return false;
     }
-    const size_t n_img = (size_t) NB * MB * 4 * IMG;
-    const size_t off_tr = al(n_img * sizeof(tc_t));
+    // 8 KB of images per block slot (either split), the traces, a zero
+    // image, the 8-bit split's row and column maxima, the tables
+    const size_t n_img = (size_t) NB * MB * (i8 ? TC8_BLOCK_BYTES : TC16_BLOCK_BYTES);
+    const size_t off_tr = al(n_img);
     const size_t off_zero = al(off_tr + (size_t) 2 * NB * sizeof(double));
-    const size_t off_tab = al(off_zero + IMG * sizeof(tc_t));
+    const size_t off_max = al(off_zero + 2 * IMG);
+    const size_t n_scalar = (size_t) NB * TB;
+    const size_t off_tab = al(off_max + (i8 ? 2 * n_scalar * sizeof(unsigned long long) : 0));
     unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_tab + tab_bytes));
     if (!scr)
         return false;
-    tc_t *img = reinterpret_cast<tc_t *>(scr);
+    unsigned char *img = scr;
     double *dA = reinterpret_cast<double *>(scr + off_tr);
     double *dC = dA + NB;
-    tc_t *zimg = reinterpret_cast<tc_t *>(scr + off_zero);
+    unsigned char *zimg = scr + off_zero;
+    unsigned long long *rowmax = i8 ? reinterpret_cast<unsigned long long *>(scr + off_max) : nullptr;
+    unsigned long long *colmax = i8 ? rowmax + n_scalar : nullptr;
     {
         unsigned char *p = scr + off_tab;
         auto take = [&](int i) {
@@ -1147,15 +1433,33 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
         tab.wstart = reinterpret_cast<int *>(take(8));
     }
     if (!CUDA_OK(cudaMemsetAsync(flags, 0, 64, c->stream)) ||
-        !CUDA_OK(cudaMemsetAsync(zimg, 0, IMG * sizeof(tc_t), c->stream)) ||
-        !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)))
+        !CUDA_OK(cudaMemsetAsync(zimg, 0, 2 * IMG, c->stream)) ||
+        !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)) ||
+        (i8 && !CUDA_OK(cudaMemsetAsync(rowmax, 0, 2 * n_scalar * sizeof(unsigned long long), c->stream))))
         return false;
     const int sgrid = (int) std::min((long long) NB * MB, (long long) c->sm_count * 32);
-    bool ok = dbl ? tc_split<double>(c, X, sgrid, maxbits, img) : tc_split<float>(c, X, sgrid, maxbits, img);
-    if (!ok)
-        return false;
-    ok = dbl ? tc_launch<double>(c, X, X2, tab, img, zimg, threshold, dA, dC, flags, grid)
-             : tc_launch<float>(c, X, X2, tab, img, zimg, threshold, dA, dC, flags, grid);
+    bool ok;
+    if (i8)
+    {
+        signed char *img8 = reinterpret_cast<signed char *>(img);
+        ok = dbl ? tc8_split<double>(c, X, sgrid, rowmax, colmax, img8)
+                 : tc8_split<float>(c, X, sgrid, rowmax, colmax, img8);
+        if (ok)
+            ok = dbl ? tc_launch<double, TcShape8, true>(c, X, X2, tab, img, zimg, threshold, rowmax, colmax, dA, dC,
+                                                         flags, grid)
+                     : tc_launch<float, TcShape8, true>(c, X, X2, tab, img, zimg, threshold, rowmax, colmax, dA, dC,
+                                                        flags, grid);
+    }
+    else
+    {
+        tc_t *img16 = reinterpret_cast<tc_t *>(img);
+        ok = dbl ? tc_split<double>(c, X, sgrid, maxbits, img16) : tc_split<float>(c, X, sgrid, maxbits, img16);
+        if (ok)
+            ok = dbl ? tc_launch<double, TcShape, false>(c, X, X2, tab, img, zimg, threshold, nullptr, nullptr, dA,
+                                                          dC, flags, grid)
+                     : tc_launch<float, TcShape, false>(c, X, X2, tab, img, zimg, threshold, nullptr, nullptr, dA, dC,
+                                                         flags, grid);
+    }
     if (!ok)
         return false;
     double *out = reinterpret_cast<double *>(static_cast<unsigned char *>(c->d_small) + 4096 + 256);
@@ -1191,6 +1495,13 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+extern "C" int bml_b200_set_tc_split(int mode)
+{
+    const int old = g_tc_split;
+    g_tc_split = mode == 1 ? 1 : 0;
+    return old;
+}
+
 extern "C" int bml_b200_ellblock_multiply_x2_tc(bml_matrix_t *X, bml_matrix_t *X2, double threshold,
                                                 double *trace)
 {

@@ -444,6 +444,18 @@ BML_B200_API int bml_b200_sp2_mixed(bml_matrix_t *H, bml_matrix_t *D, double thr
 BML_B200_API int bml_b200_ellblock_multiply_x2_tc(bml_matrix_t *X, bml_matrix_t *X2, double threshold,
     double *trace);
 
+/* Chooses the split of bml_b200_ellblock_multiply_x2_tc (no reference
+ * counterpart) and returns the previous choice.  0 (the default): FP16 hi/lo
+ * halves, three products per block pair, FP32 accumulation in tensor memory
+ * (about 1e-5 of the product magnitudes per entry).  1: each entry as five
+ * signed 8-bit slices of its row's (left operand) or column's (right
+ * operand) power-of-two scale, the fifteen slice products of order <= 6 per
+ * block pair on kind::i8 with exact INT32 accumulation, recombined in FP64:
+ * within about 2^-33 of the row and column scales per product term, with no
+ * accumulation error.  Takes NB <= 24576 and groups of four block rows with
+ * at most 3276 block columns (else UNSUPPORTED). */
+BML_B200_API int bml_b200_set_tc_split(int mode);
+
 /* SP2 on ELLBLOCK matrices in mixed precision (no reference counterpart):
  * bulk iterations use bml_b200_ellblock_multiply_x2_tc, the last nclose
  * iterations the matrix-precision X^2 of bml_multiply_x2; adds, copies, the
