@@ -62,6 +62,8 @@ def parse():
                     help="run the small tensor-core ELLBLOCK case for an ncu capture (10^3 block lattice)")
     ap.add_argument("--profile-tc-wide", action="store_true",
                     help="the same for the SP2 iterate after one iteration (the second iteration's product)")
+    ap.add_argument("--tc-split", type=int, default=0, choices=[0, 1],
+                    help="split of the tensor-core X^2 in the profile cases: 0 FP16 hi/lo, 1 8-bit slices")
     ap.add_argument("--profile-eb-ops", action="store_true",
                     help="the one-pass ELLBLOCK operations, once each, for an ncu capture (7^3 block lattice)")
     ap.add_argument("--eb-ops-L", type=int, default=7, help="block lattice side for --profile-eb-ops")
@@ -730,12 +732,13 @@ def ellblock_case(L):
     return H, nb * 32
 
 
-def run_profile_tc(wide=False):
+def run_profile_tc(wide=False, split=0):
     """Three tensor-core X^2 calls on the 10^3 block lattice (N = 32000): of
     H, or (wide) of X1, the iterate after one exact SP2 iteration from H
     (the product of the second SP2 iteration); the three calls run inside the
     NVTX range "tc"."""
     import bml_b200 as B
+    B.lib.bml_b200_set_tc_split(split)
     H, n = ellblock_case(10)
     X = H
     if wide:
@@ -961,7 +964,7 @@ def main():
         run_profile_case()
         return
     if args.profile_tc or args.profile_tc_wide:
-        run_profile_tc(wide=args.profile_tc_wide)
+        run_profile_tc(wide=args.profile_tc_wide, split=args.tc_split)
         return
     if args.profile_ops:
         run_profile_ops()
