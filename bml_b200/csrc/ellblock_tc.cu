@@ -1,8 +1,12 @@
-// ELLBLOCK X^2 on the tcgen05 tensor cores, FP16 with a hi/lo split (mixed
+// ELLBLOCK X^2 on the tcgen05 tensor cores, in one of two splits (mixed
 // precision; no reference counterpart: the reference multiplies blocks in the
-// matrix precision, ellblock/bml_multiply_ellblock_typed.c:246-442).
+// matrix precision, ellblock/bml_multiply_ellblock_typed.c:246-442): FP16
+// hi/lo halves with FP32 accumulation (the default, below), or 8-bit slices
+// with exact INT32 accumulation (bml_b200_set_tc_split(1); described with
+// its kernels further down).  Both share the group tables, the rings and the
+// pipeline; they differ in the operand images, the MMA kind and the epilogue.
 //
-// X is scaled by a power of two 2^s (its largest entry near 2^14) and every
+// FP16 split.  X is scaled by a power of two 2^s (its largest entry near 2^14) and every
 // 32x32 block x is split as hi = fp16(2^s x), lo = fp16(2^s x - hi); X^2 =
 // sum_jb X[ib,jb] X[jb,kb] is formed as hi*hi + hi*lo + lo*hi with FP32
 // accumulation in tensor memory and scaled back by 2^-2s (lo*lo, about 2^-22
