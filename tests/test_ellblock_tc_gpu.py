@@ -403,3 +403,40 @@ def test_ellblock_sp2_mixed_8bit_meets_the_1e6_target():
     finally:
         B.lib.bml_b200_set_tc_split(old)
         B.lib.bml_b200_reset_block_sizes()
+
+
+@pytest.mark.parametrize("split", [0, 1], ids=["fp16", "8bit"])
+def test_tc_x2_empty_block_rows_and_ragged_groups(split):
+    """Block rows with no blocks at all (rows and columns 5, 6 and the last
+    of a 3^3 block lattice emptied) and NB = 27, not a multiple of the four
+    block rows a group takes: the empty rows come out empty, the others as
+    the FP64 dense product (FP16 split within 2e-5 of S; 8-bit split, whose
+    bound is relative to the row and column scales, within 1e-7 of S:
+    measured 1e-8 on these lattices)."""
+    import torch
+    thr = 1e-6
+    H = block_lattice(3, 1.8, seed=11)
+    nb, N = 27, H.shape[0]
+    for b in (5, 6, 26):
+        H[b * 32:(b + 1) * 32, :] = 0.0
+        H[:, b * 32:(b + 1) * 32] = 0.0
+    set_partition(nb, nb)
+    old = B.lib.bml_b200_set_tc_split(split)
+    try:
+        X = from_dense(H)
+        Xt = B.lib.bml_zero_matrix(ELLBLOCK, DOUBLE, N, N, 0)
+        B.check()
+        st = B.lib.bml_b200_ellblock_multiply_x2_tc(X, Xt, thr, None)
+        assert st == B.OK, B.lib.bml_b200_error_string(st)
+        want, S, keep = _fp64_block_x2(H, nb, thr)
+        got = torch.from_numpy(to_dense(Xt, N)).to(want.device)
+        for b in (5, 6, 26):
+            assert float(got[b * 32:(b + 1) * 32, :].abs().max()) == 0.0
+        eps = 2e-5 if split == 0 else 1e-7
+        err = (got - want).abs()
+        assert float((err / S.clamp_min(1e-300)).max()) <= eps
+        for h in (X, Xt):
+            free(h)
+    finally:
+        B.lib.bml_b200_set_tc_split(old)
+        B.lib.bml_b200_reset_block_sizes()
