@@ -30,16 +30,18 @@
 // the largest group: the kernel takes groups of any size.
 // Operands are staged into shared memory in the UMMA canonical K-major
 // no-swizzle layout (8-row x 16-byte core matrices).  A split kernel first
-// writes every block of X in that layout, as the left operand (rows x k) and
-// as the right operand (columns x k, the block transposed), one contiguous
-// 2 KB image each, so staging is one bulk copy (cp.async.bulk, completing on
-// an mbarrier) per block, issued by one producer thread into rings of left
-// and right operand buffers.  One thread issues the MMAs and releases each
-// buffer with tcgen05.commit on its "empty" mbarrier.  A sorted pair's record
-// holds everything either thread needs (the new-left-operand flag, the
-// positions of the left blocks, the right operand's slot, the tile), so their
-// loops hold only one record load, the waits, the copies and the MMAs.  Every
-// wait is bounded.
+// writes every block of X in that layout, as the left operand (rows x k, 2 KB
+// per part) and as the right operand (columns x k, the block transposed, its
+// parts interleaved by row group), so staging is one bulk copy
+// (cp.async.bulk, completing on an mbarrier) per block and part.  The pairs
+// of one wave and one block column jb form a step: one left operand (the
+// group's four blocks of column jb) and at most one right operand per tile.
+// A producer warp copies a step's left operand into a ring of buffers and its
+// right operands side by side, in tile order, into a ring of slots; an issuer
+// warp (one lane) then issues one MMA per run of consecutive tiles and part,
+// N = 32 x the run's tiles (up to 256), and releases the buffer and slots
+// with tcgen05.commit on their "empty" mbarriers.  Both warps read the sorted
+// pairs 32 records per load; every wait is bounded.
 #include "device_util.cuh"
 #include "ellblock.h"
 
@@ -64,15 +66,17 @@ constexpr int IMG = TB * TB;      // 16-bit elements per block image (2 KB)
 constexpr int TC_NWCAP = 2048;    // bitmap words: up to 65536 block columns
 // Shape of the kernel: TILES output tiles of 32 TMEM columns live per CTA (a
 // wave), CTAS CTAs per SM (two, so that one CTA's set-up and epilogue overlap
-// the other's MMAs), ABUF and BBUF buffers in the left and right operand
-// rings.  Measured on the 16^3 block lattice's X^2: 8 tiles x 2 CTAs 6.9 ms,
-// 16 tiles x 1 CTA 10.0 ms.
+// the other's MMAs), ABUF left-operand buffers and BBUF right-operand slots
+// (a step takes one slot per pair, side by side).  Measured on the 16^3 block
+// lattice's X^2: 8 tiles x 2 CTAs 6.9 ms, 16 tiles x 1 CTA 10.0 ms (with one
+// MMA per pair).
 template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int ABYTES_ = 16384, int BBYTES_ = 4096> struct TcCfg
 {
     static constexpr int TILES = TILES_, CTAS = CTAS_, ABUF = ABUF_, BBUF = BBUF_;
-    static constexpr int ABYTES = ABYTES_, BBYTES = BBYTES_; // one left / right operand buffer
+    static constexpr int ABYTES = ABYTES_, BBYTES = BBYTES_; // one left operand / right operand slot
     static_assert(CTAS * TILES * 32 <= 512, "tensor memory holds 512 columns per SM");
-    static_assert(TILES <= 16, "tile numbers take 4 bits of a pair");
+    static_assert(TILES <= 16, "a step's tiles take 16 bits of a record");
+    static_assert(BBUF >= TILES, "a step's right operands fit the slot ring");
 };
 #ifndef B200_TC_TILES
 #define B200_TC_TILES 8
@@ -80,7 +84,13 @@ template <int TILES_, int CTAS_, int ABUF_, int BBUF_, int ABYTES_ = 16384, int 
 #ifndef B200_TC_CTAS
 #define B200_TC_CTAS 2
 #endif
-using TcShape = TcCfg<B200_TC_TILES, B200_TC_CTAS, 3, 8>;
+#ifndef B200_TC_ABUF
+#define B200_TC_ABUF 3
+#endif
+#ifndef B200_TC_BBUF
+#define B200_TC_BBUF 14
+#endif
+using TcShape = TcCfg<B200_TC_TILES, B200_TC_CTAS, B200_TC_ABUF, B200_TC_BBUF>;
 
 // Operand type of the split: FP16 (11-bit significands: hi and lo carry
 // about 22 bits, the dropped lo*lo about 2^-22 of a product) with the whole
@@ -112,16 +122,28 @@ __device__ __forceinline__ int tc_scale_exp(unsigned maxbits)
 }
 
 // 16-bit image of a block in the K-major no-swizzle layout, as a left operand
-// (element (r, k) of the block) or a right operand (element (n, k) = block
-// (k, n)): 16-byte rows of 8 k, 8-row core matrices of 128 bytes; the four
-// k-chunks of an 8-row group sit next to each other (LBO = 128 B) and the
-// row groups follow at SBO = 512 B, so each 32 x 32 block is one contiguous
-// 2 KB image and four blocks stack into the 128-row left operand.
+// (element (r, k) of the block): 16-byte rows of 8 k, 8-row core matrices of
+// 128 bytes; the four k-chunks of an 8-row group sit next to each other
+// (LBO = 128 B) and the row groups follow at SBO = 512 B, so each 32 x 32
+// block is one contiguous 2 KB image and four blocks stack into the 128-row
+// left operand.
 constexpr unsigned TC_LBO = 128, TC_SBO = 512;
 
 __device__ __forceinline__ int img_off(int row, int k)
 {
     return (row >> 3) * 256 + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
+}
+
+// The right operand (element (n, k) = block (k, n)) keeps hi and lo of an
+// 8-row group together: row group g at g * 1 KB, hi at +0 and lo at +512 B,
+// each four k-chunks of 128 B.  A block is then one 4 KB image whose row
+// groups follow at a uniform SBO = 1 KB, so the images of consecutive output
+// tiles, placed side by side, form one operand of N = 32 x (tiles).
+constexpr unsigned TC_RSBO = 1024, TC_RLO = 512;
+
+__device__ __forceinline__ int rimg_off(int n, int k, int part)
+{
+    return (n >> 3) * 512 + part * 256 + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
 }
 
 // max |x| over the stored blocks of X, as float bits (non-negative floats
@@ -146,31 +168,64 @@ __global__ void tc_maxabs_kernel(const T *pool, const int *nnzb, int NB, int MB,
         atomicMax(maxbits, __float_as_uint(m));
 }
 
-// Split every stored block of X, scaled by 2^s, into four images: left hi,
-// left lo, right hi, right lo, at img + slot*4*IMG.
+// Split every stored block of X, scaled by 2^s, into its images at
+// img + slot*4*IMG: left hi, left lo (2 KB each), then the right operand's
+// hi and lo interleaved by row group (4 KB).  One warp per block: lane c
+// holds column c of every row; the right image (n = c) is written from
+// registers, the left one (row r) through a shared-memory transpose, both in
+// 16-byte stores.
+constexpr int TC_SPLIT_WARPS = 8;
+
 template <typename T>
-__global__ void tc_split_kernel(const T *pool, const int *nnzb, int NB, int MB, long long slot_elems,
-                                const unsigned *maxbits, tc_t *img)
+__global__ void __launch_bounds__(TC_SPLIT_WARPS * 32)
+    tc_split_kernel(const T *pool, const int *nnzb, int NB, int MB, long long slot_elems, const unsigned *maxbits,
+                    tc_t *img)
 {
+    __shared__ __align__(16) tc_t sh[TC_SPLIT_WARPS][2][TB][TB + 8]; // [part][row][k], rows of 80 B
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
     const double scale = ldexp(1.0, tc_scale_exp(*maxbits));
-    for (long long s = blockIdx.x; s < (long long) NB * MB; s += gridDim.x)
+    const long long warps = (long long) gridDim.x * TC_SPLIT_WARPS;
+    for (long long s = (long long) blockIdx.x * TC_SPLIT_WARPS + wq; s < (long long) NB * MB; s += warps)
     {
         const int ib = (int) (s / MB), jp = (int) (s % MB);
         if (jp >= nnzb[ib])
             continue;
         const T *x = pool + s * slot_elems;
         tc_t *o = img + s * 4 * IMG;
-        for (int e = threadIdx.x; e < IMG; e += blockDim.x)
+        tc_t hi[TB], lo[TB];
+#pragma unroll
+        for (int r = 0; r < TB; ++r)
         {
-            const int r = e >> 5, c = e & 31;
-            const double v = (double) x[e] * scale; // a power of two: exact
-            const tc_t hi = tc_from_double(v);
-            const tc_t lo = tc_from_double(v - tc_to_double(hi));
-            o[img_off(r, c)] = hi;           // left: row r, k = c
-            o[IMG + img_off(r, c)] = lo;
-            o[2 * IMG + img_off(c, r)] = hi; // right: n = c, k = r
-            o[3 * IMG + img_off(c, r)] = lo;
+            const double v = (double) x[r * TB + lane] * scale; // a power of two: exact
+            hi[r] = tc_from_double(v);
+            lo[r] = tc_from_double(v - tc_to_double(hi[r]));
+            sh[wq][0][r][lane] = hi[r];
+            sh[wq][1][r][lane] = lo[r];
         }
+        // right: n = lane, k = r; eight consecutive k per 16-byte store
+#pragma unroll
+        for (int kc = 0; kc < 4; ++kc)
+        {
+            uint4 vh, vl;
+            tc_t *ph = reinterpret_cast<tc_t *>(&vh), *pl = reinterpret_cast<tc_t *>(&vl);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+                ph[i] = hi[kc * 8 + i];
+                pl[i] = lo[kc * 8 + i];
+            }
+            *reinterpret_cast<uint4 *>(o + 2 * IMG + rimg_off(lane, kc * 8, 0)) = vh;
+            *reinterpret_cast<uint4 *>(o + 2 * IMG + rimg_off(lane, kc * 8, 1)) = vl;
+        }
+        __syncwarp();
+        // left: row r = lane, k = eight consecutive columns per store
+#pragma unroll
+        for (int part = 0; part < 2; ++part)
+#pragma unroll
+            for (int kc = 0; kc < 4; ++kc)
+                *reinterpret_cast<uint4 *>(o + part * IMG + img_off(lane, kc * 8)) =
+                    *reinterpret_cast<const uint4 *>(&sh[wq][part][lane][kc * 8]);
+        __syncwarp();
     }
 }
 
@@ -205,6 +260,16 @@ constexpr unsigned TC8_LBO = 128, TC8_SBO = 256;
 __device__ __forceinline__ int img8_off(int row, int k)
 {
     return (row >> 3) * 256 + (k >> 4) * 128 + (row & 7) * 16 + (k & 15);
+}
+
+// The right operand's five slices interleaved by row group: row group g at
+// g * 1280 B, slice s at +256 s; a block is one 5 KB image with a uniform
+// SBO = 1280 B, so consecutive tiles' images form one wider operand.
+constexpr unsigned TC8_RSBO = 1280;
+
+__device__ __forceinline__ int rimg8_off(int n, int k, int s)
+{
+    return (n >> 3) * 1280 + s * 256 + (k >> 4) * 128 + (n & 7) * 16 + (k & 15);
 }
 
 // Exponent e with 2^e > m >= 0 (m given by its bits; 0 for m = 0).
@@ -262,10 +327,11 @@ __device__ __forceinline__ void tc8_slices(double u, signed char (&a)[TC8_SLICES
     }
 }
 
-// Slice every stored block of X into its 8-bit images at img + slot * 8 KB:
-// left slices 1..4 (element (r, k) of the block, scaled by sigma of scalar
-// row r) at +0, +1 KB, +2 KB, +3 KB, right slices 1..4 (element (n, k) =
-// block (k, n), scaled by tau of scalar column n) at +4 KB ... +7 KB.
+// Slice every stored block of X into its 8-bit images at img + slot * 10 KB:
+// left slices 1..5 (element (r, k) of the block, scaled by sigma of scalar
+// row r) at +0, +1 KB, ..., +4 KB, then the right slices 1..5 (element
+// (n, k) = block (k, n), scaled by tau of scalar column n) interleaved by row
+// group in 5 KB.
 template <typename T>
 __global__ void tc8_split_kernel(const T *pool, const int *indexb, const int *nnzb, int NB, int MB,
                                  long long slot_elems, const unsigned long long *rowmax,
@@ -291,7 +357,7 @@ __global__ void tc8_split_kernel(const T *pool, const int *indexb, const int *nn
             tc8_slices(ldexp(v, -tc8_exp(colmax[(size_t) jb * TB + c])), a);
 #pragma unroll
             for (int q = 0; q < TC8_SLICES; ++q)
-                o[(TC8_SLICES + q) * TC8_IMG + img8_off(c, r)] = a[q];
+                o[TC8_SLICES * TC8_IMG + rimg8_off(c, r, q)] = a[q];
         }
     }
 }
@@ -308,31 +374,38 @@ __device__ __forceinline__ uint64_t smem_desc(unsigned addr, unsigned lbo, unsig
 }
 
 // kind::f16 instruction descriptor: D F32, A and B both FP16 (type 0) or
-// both BF16 (type 1), both K-major, N = 32, M = 128.
+// both BF16 (type 1), both K-major, M = 128; N (bits 17-22, N / 8) is added
+// per MMA: 32 per output tile of the run it covers.
 constexpr uint32_t TC_AB_TYPE = B200_TC_F16 ? 0u : 1u;
-constexpr uint32_t TC_IDESC =
-    (1u << 4) | (TC_AB_TYPE << 7) | (TC_AB_TYPE << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t TC_IDESC = (1u << 4) | (TC_AB_TYPE << 7) | (TC_AB_TYPE << 10) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ void umma_f16(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, unsigned accumulate)
+// N field of an instruction descriptor for a run of `tiles` output tiles
+// (N = 32 tiles: 32..256, a multiple of 16 as M = 128 requires; longer runs
+// are split by the caller).
+__device__ __forceinline__ uint32_t idesc_n(int tiles) { return (uint32_t) (tiles * 32 >> 3) << 17; }
+
+__device__ __forceinline__ void umma_f16(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         unsigned accumulate)
 {
     asm volatile("{\n\t.reg .pred p;\n\t"
                  "setp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                 ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u),
+                 ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u),
                    "r"(0u), "r"(0u)
                  : "memory");
 }
 
 // kind::i8 instruction descriptor: D S32 (2), A and B signed 8-bit (1),
-// both K-major, N = 32, M = 128.
-constexpr uint32_t TC8_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// both K-major, M = 128; N added per MMA as above.
+constexpr uint32_t TC8_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ void umma_i8(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, unsigned accumulate)
+__device__ __forceinline__ void umma_i8(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        unsigned accumulate)
 {
     asm volatile("{\n\t.reg .pred p;\n\t"
                  "setp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                 ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(TC8_IDESC), "r"(accumulate), "r"(0u), "r"(0u),
+                 ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u),
                    "r"(0u), "r"(0u)
                  : "memory");
 }
@@ -435,14 +508,15 @@ template <class Cfg> struct TcSmem
     };
     union
     {
-        unsigned char b[Cfg::BBUF][Cfg::BBYTES]; // right operands: 32 x 32, every part
+        unsigned char b[Cfg::BBUF][Cfg::BBYTES]; // right operand slots: 32 x 32, every part
         float stage[TC_GROUP][TB][TB + 1]; // epilogue transpose (the ring is idle then)
         double dstage[TC_GROUP][TB][17];   // the same for the 8-bit mode's FP64 values, 16 columns at a time
     };
-    uint64_t full_a[Cfg::ABUF], full_b[Cfg::BBUF]; // bulk copies landed
-    uint64_t empty_b[Cfg::BBUF];                   // MMAs reading a B buffer (and all before) done
+    uint64_t full_a[Cfg::ABUF], full_b[Cfg::BBUF]; // bulk copies landed (B: per step, a ring of BBUF)
+    uint64_t empty_b[Cfg::BBUF];                   // MMAs of a step (and all before) done
     uint64_t empty_a[Cfg::ABUF];                   // MMAs reading an A buffer's fill (and all before) done
     uint64_t done;                                 // all MMAs of a wave done
+    unsigned sstart[Cfg::BBUF];                    // producer: first slot (a running count) of each live step
     unsigned tmem;
     int nJ, nK, npairs, dead, grp;
     int scratch[TC_THREADS / 32];
@@ -467,8 +541,12 @@ template <typename T> struct TcOut
 // A group's tables, in global memory: one set per CTA, each sized for the
 // largest group (tc_count_kernel).  A pair (j, kp) is the product of the
 // group's left operand for J entry j with the right operand X[jb_j, kb],
-// kb the kp-th block column of row jb_j.  Records of the sorted pairs:
-//   x = tile within the wave (bits 0-3) | j << 4 | a new left operand << 31,
+// kb the kp-th block column of row jb_j.  The pairs of one wave and one J
+// entry (a step: at most one pair per tile) share one left operand and go to
+// the tensor cores together.  Records of the sorted pairs:
+//   x = tile within the wave (bits 0-3) | j << 4 (bits 4-19; while the
+//       tables are built) | 1 << 31 on a step's first pair, whose bits 4-19
+//       then hold the step's tiles as a mask,
 //   y = slot of the right operand, jb * MB + kp,
 //   z, w = position jp of X[ib0+q, jb] in row ib0+q for q = 0..3, 16 bits
 //          each (z: q = 0, 1; w: q = 2, 3), 0xFFFF where the row lacks jb.
@@ -649,7 +727,6 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     constexpr int BLK = I8 ? TC8_BLOCK_BYTES : TC16_BLOCK_BYTES; // image bytes per block slot
     static_assert(TUSED <= 512, "tensor memory holds 512 columns per SM");
     static_assert(Cfg::ABYTES >= TC_GROUP * BLK / 2 && Cfg::BBYTES >= BLK / 2, "operand buffers");
-    static_assert(!I8 || TC_TILES * TC8_LEVELS <= 32, "started bits: one per tile and level");
     TcSmem<Cfg> &S = *reinterpret_cast<TcSmem<Cfg> *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ngroups = (X.NB + TC_GROUP - 1) / TC_GROUP;
@@ -695,8 +772,10 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     const float unscale = ldexpf(1.0f, -2 * tc_scale_exp((unsigned) flags[8]));
     bool dead = false; // a wait timed out: stop issuing work
     // pipeline counters, kept alike by the producer (thread 0) and the MMA
-    // issuer (thread 32): pairs and left operands issued so far
-    unsigned gp = 0, ga = 0, nwaves = 0;
+    // issuer (thread 32): steps, right-operand slots (a running count) and
+    // left operands issued so far; go: the producer's oldest step not yet
+    // seen done
+    unsigned gs = 0, bh = 0, ga = 0, go = 0, nwaves = 0;
     unsigned copied_a = 0; // left operands whose copies thread 0 issued
 
     for (;;)
@@ -897,18 +976,42 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             }
         }
         __syncthreads();
-        // a new left operand where j changes within a wave, and at every
-        // wave's first pair
+        // a step starts (a new left operand) where j changes within a wave,
+        // and at every wave's first pair
         for (int p = tid; p < npairs; p += TC_THREADS)
         {
             const unsigned x = G.list[p].x;
-            if (p == 0 || ((x ^ G.list[p - 1].x) & 0x7FFFFFF0u))
+            if (p == 0 || ((x ^ G.list[p - 1].x) & 0x000FFFF0u))
                 G.list[p].x = x | 0x80000000u;
         }
         __syncthreads();
         for (int w = tid; w < nW; w += TC_THREADS)
             if (G.wstart[w] < npairs) // every wave has a pair: each tile is some pair's
                 G.list[G.wstart[w]].x |= 0x80000000u;
+        __syncthreads();
+        // every step's tiles, into its first record (ptile is free again: the
+        // sort above was its last reader); the pairs of a step have distinct
+        // tiles unless a row of X repeats a block column
+        int badstep = 0;
+        for (int p = tid; p < npairs; p += TC_THREADS)
+            if (G.list[p].x >> 31)
+            {
+                unsigned m = 1u << (G.list[p].x & 15u);
+                int n = 1;
+                for (int q = p + 1; q < npairs && !(G.list[q].x >> 31); ++q, ++n)
+                    m |= 1u << (G.list[q].x & 15u);
+                badstep |= __popc(m) != n;
+                G.ptile[p] = (int) m;
+            }
+        if (__syncthreads_or(badstep))
+        {
+            if (tid == 0)
+                atomicExch(&flags[2], 1);
+            continue;
+        }
+        for (int p = tid; p < npairs; p += TC_THREADS)
+            if (G.list[p].x >> 31)
+                G.list[p].x = (G.list[p].x & 0x8000000Fu) | (unsigned) G.ptile[p] << 4;
         int kept = 0;
         double trc = 0.0;
 
@@ -945,141 +1048,227 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             const int t0 = w * TC_TILES;
             const int nt = min(TC_TILES, nK - t0);
             const int p0 = G.wstart[w], p1 = G.wstart[w + 1];
-            if (tid == 0)
+            if (warp == 0)
             {
-                // producer (thread 0): for each pair, its right operand into
-                // the next B buffer and, on a new left operand, the group's
-                // four blocks of column jb into the next A buffer, each once
-                // the MMAs that read the buffer's previous fill are done
-                for (int p = p0; p < p1; ++p)
+                // producer (warp 0): 32 records per load; for each step wholly
+                // inside them, the group's four blocks of column jb into the
+                // next A buffer (a lane per block and part) and the step's
+                // right operands into a run of free slots (a lane per pair,
+                // slot = rank of its tile among the step's), each once the
+                // MMAs that read the buffer's or slots' previous fill are
+                // done.  Lane 0 waits and arms the barriers; the counters are
+                // alike in all lanes.
+                constexpr int NPART = I8 ? TC8_SLICES : 2;
+                constexpr unsigned PBYTES = BLK / 2 / NPART;
+                static_assert(TC_GROUP * NPART <= 32, "a lane per left block and part");
+                bool quit = false;
+                for (int p = p0; p < p1 && !quit;)
                 {
-                    if (((p - p0) & 7) == 0 && p + 16 < p1)
-                        prefetch_l1(G.list + p + 16);
-                    const uint4 r = G.list[p];
-                    const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
-                    if (r.x >> 31)
+                    const int n = min(32, p1 - p);
+                    const uint4 r = lane < n ? G.list[p + lane] : make_uint4(0u, 0u, 0u, 0u);
+                    unsigned todo = __ballot_sync(FULL, lane < n && (r.x >> 31));
+                    int used = 0;
+                    while (todo)
                     {
+                        const int s0 = __ffs(todo) - 1;
+                        todo &= todo - 1;
+                        const unsigned mask = (__shfl_sync(FULL, r.x, s0) >> 4) & 0xFFFFu;
+                        const int need = __popc(mask);
+                        if (s0 + need > n)
+                            break; // runs past the loaded records: the next load starts here
+                        const unsigned rz = __shfl_sync(FULL, r.z, s0), rw = __shfl_sync(FULL, r.w, s0);
                         const unsigned a = ga % TC_ABUF, fa = ga / TC_ABUF;
-                        if (fa >= 1 && !mbar_wait2s(&S.empty_a[a], (fa - 1) & 1))
+                        unsigned h = bh;
+                        if (h % TC_BBUF + need > TC_BBUF)
+                            h += TC_BBUF - h % TC_BBUF;
+                        const unsigned e = gs % TC_BBUF;
+                        int late = 0;
+                        if (lane == 0)
                         {
-                            S.dead = 1;
+                            if (fa >= 1 && !mbar_wait2s(&S.empty_a[a], (fa - 1) & 1))
+                                late = 1;
+                            // slots [h, h + need) of the ring (a running
+                            // count), not across its end: free once the older
+                            // steps holding them are done (and this step's
+                            // barriers once their previous use is)
+                            while (!late && (gs - go >= (unsigned) TC_BBUF ||
+                                             (go < gs && h + need - S.sstart[go % TC_BBUF] > (unsigned) TC_BBUF)))
+                            {
+                                if (!mbar_wait2s(&S.empty_b[go % TC_BBUF], (go / TC_BBUF) & 1))
+                                    late = 1;
+                                else
+                                    ++go;
+                            }
+                            if (late)
+                                S.dead = 1;
+                            else
+                            {
+                                S.sstart[e] = h;
+                                mbar_expect(&S.full_a[a], TC_GROUP * BLK / 2);
+                                mbar_expect(&S.full_b[e], need * (BLK / 2));
+                            }
+                        }
+                        go = __shfl_sync(FULL, go, 0);
+                        if (__shfl_sync(FULL, late, 0))
+                        {
+                            quit = true;
                             break;
                         }
-                        // 16 KB either way: FP16 hi and lo (2 parts of 2 KB
-                        // per block), or 4 slices of 1 KB per block; part p
-                        // of the four blocks stacks into the 128-row operand
-                        constexpr int NPART = I8 ? TC8_SLICES : 2;
-                        constexpr unsigned PBYTES = BLK / 2 / NPART;
-                        mbar_expect(&S.full_a[a], TC_GROUP * BLK / 2);
-                        unsigned char *abytes = S.a[a];
-#pragma unroll
-                        for (int q = 0; q < TC_GROUP; ++q)
+                        if (lane < TC_GROUP * NPART)
                         {
-                            const unsigned jp = rec_slot(r, q);
-#pragma unroll
-                            for (int part = 0; part < NPART; ++part)
-                            {
-                                const unsigned char *src =
-                                    jp != 0xFFFFu
-                                        ? img + ((size_t) (ib0 + q) * X.MB + jp) * BLK + part * PBYTES
-                                        : zimg;
-                                bulk_copy(abytes + part * (TC_GROUP * PBYTES) + q * PBYTES, src, PBYTES,
-                                          &S.full_a[a]);
-                            }
+                            // 16 KB (FP16: hi and lo, 2 parts of 2 KB per
+                            // block) or 20 KB (8-bit: 5 slices of 1 KB per
+                            // block); part p of the four blocks stacks into
+                            // the 128-row operand
+                            const int q = lane / NPART, part = lane % NPART;
+                            const unsigned jp = ((q < 2 ? rz : rw) >> ((q & 1) * 16)) & 0xFFFFu;
+                            const unsigned char *src =
+                                jp != 0xFFFFu ? img + ((size_t) (ib0 + q) * X.MB + jp) * BLK + part * PBYTES : zimg;
+                            bulk_copy(S.a[a] + part * (TC_GROUP * PBYTES) + q * PBYTES, src, PBYTES, &S.full_a[a]);
+                        }
+                        if (lane >= s0 && lane < s0 + need)
+                        {
+                            // the right operand's parts are adjacent in both
+                            // places: one copy
+                            const unsigned rank = __popc(mask & ((1u << (r.x & 15u)) - 1u));
+                            bulk_copy(S.b[h % TC_BBUF] + rank * Cfg::BBYTES, img + (size_t) r.y * BLK + BLK / 2,
+                                      BLK / 2, &S.full_b[e]);
                         }
                         ++ga;
                         copied_a = ga;
+                        bh = h + need;
+                        ++gs;
+                        used = s0 + need;
                     }
-                    if (f >= 1 && !mbar_wait2s(&S.empty_b[b], (f - 1) & 1))
+                    if (used == 0 && !quit)
                     {
-                        S.dead = 1;
-                        break;
+                        // a step longer than 32 records: tables out of shape
+                        if (lane == 0)
+                        {
+                            atomicExch(&flags[2], 1);
+                            S.dead = 1;
+                        }
+                        quit = true;
                     }
-                    mbar_expect(&S.full_b[b], BLK / 2);
-                    // the right operand's parts are adjacent in both places:
-                    // one copy
-                    bulk_copy(S.b[b], img + (size_t) r.y * BLK + BLK / 2, BLK / 2, &S.full_b[b]);
-                    ++gp;
+                    p += used;
                 }
             }
-            else if (tid == 32)
+            else if (warp == 1)
             {
-                // MMA issuer (thread 32): the same sequence, consuming the
-                // ring; the first MMA into a tile in this wave overwrites it
+                // MMA issuer (warp 1; lane 0 issues): the same steps, from 32
+                // records per load, consuming the rings.  A step's tiles fall
+                // into runs of consecutive tiles whose slots are adjacent: one
+                // MMA per run and part, N = 32 x the run's tiles.  The first
+                // MMA into a tile in this wave overwrites it, so a run also
+                // ends where that changes.
                 unsigned started = 0, acur = 0;
-                for (int p = p0; p < p1; ++p)
+                bool any = false, quit = false;
+                for (int p = p0; p < p1 && !quit;)
                 {
-                    if (((p - p0) & 7) == 0 && p + 16 < p1)
-                        prefetch_l1(G.list + p + 16);
-                    const unsigned rx = G.list[p].x;
-                    const int tile = (int) (rx & 15u);
-                    const unsigned b = gp % TC_BBUF, f = gp / TC_BBUF;
-                    if (rx >> 31)
+                    const int n = min(32, p1 - p);
+                    const unsigned rxl = lane < n ? G.list[p + lane].x : 0u;
+                    unsigned todo = __ballot_sync(FULL, lane < n && (rxl >> 31));
+                    int used = 0;
+                    while (todo)
                     {
-                        if (p > p0)
-                            umma_commit(&S.empty_a[acur]); // the previous left operand is done with
-                        acur = ga % TC_ABUF;
-                        if (!mbar_wait2s(&S.full_a[acur], (ga / TC_ABUF) & 1))
+                        const int s0 = __ffs(todo) - 1;
+                        todo &= todo - 1;
+                        const unsigned mask = (__shfl_sync(FULL, rxl, s0) >> 4) & 0xFFFFu;
+                        const int need = __popc(mask);
+                        if (s0 + need > n)
+                            break;
+                        unsigned h = bh;
+                        if (h % TC_BBUF + need > TC_BBUF)
+                            h += TC_BBUF - h % TC_BBUF;
+                        const unsigned e = gs % TC_BBUF;
+                        int late = 0;
+                        if (lane == 0)
                         {
-                            S.dead = 1;
+                            if (any)
+                                umma_commit(&S.empty_a[acur]); // the previous left operand is done with
+                            acur = ga % TC_ABUF;
+                            if (!mbar_wait2s(&S.full_a[acur], (ga / TC_ABUF) & 1) ||
+                                !mbar_wait2s(&S.full_b[e], (gs / TC_BBUF) & 1))
+                                late = 1;
+                        }
+                        if (__shfl_sync(FULL, late, 0))
+                        {
+                            if (lane == 0)
+                                S.dead = 1;
+                            quit = true;
                             break;
                         }
-                        ++ga;
-                    }
-                    if (!mbar_wait2s(&S.full_b[b], f & 1))
-                    {
-                        S.dead = 1;
-                        break;
-                    }
-                    tc_fence_after();
-                    if (I8)
-                    {
-                        // slices s, t (0-based) with s + t <= 3 into level
-                        // s + t's INT32 accumulator; K = 32 per instruction
-                        const unsigned a0 = su32(S.a[acur]), b0 = su32(S.b[b]);
-#pragma unroll
-                        for (int sa = 0; sa < TC8_SLICES; ++sa)
-#pragma unroll
-                            for (int sb = 0; sb + sa < TC8_LEVELS; ++sb)
+                        if (lane == 0)
+                        {
+                            tc_fence_after();
+                            const unsigned a0 = su32(S.a[acur]), sb0 = su32(S.b[h % TC_BBUF]);
+                            unsigned m = mask;
+                            while (m)
                             {
-                                const int lev = sa + sb;
-                                const unsigned bit = 1u << (tile * TC8_LEVELS + lev);
-                                const unsigned acc = (started & bit) ? 1u : 0u;
-                                started |= bit;
-                                umma_i8(tbase + (unsigned) (tile * 32 * TC8_LEVELS + lev * 32),
-                                        smem_desc(a0 + sa * (TC_GROUP * TC8_IMG), TC8_LBO, TC8_SBO),
-                                        smem_desc(b0 + sb * TC8_IMG, TC8_LBO, TC8_SBO), acc);
-                            }
-                        umma_commit(&S.empty_b[b]);
-                        ++gp;
-                        continue;
-                    }
-                    const unsigned d = tbase + (unsigned) (tile * 32);
-                    const unsigned a0 = su32(S.a[acur]), a1 = a0 + TC_GROUP * 2 * IMG;
-                    const unsigned b0 = su32(S.b[b]), b1 = b0 + 2 * IMG;
-                    unsigned acc = (started >> tile) & 1u;
-                    started |= 1u << tile;
+                                const int ta = __ffs(m) - 1;
+                                const unsigned st = (started >> ta) & 1u;
+                                const unsigned x = (m >> ta) & ((st ? started : ~started) >> ta);
+                                // x's trailing ones (at least 1), at most 8
+                                // tiles: an MMA takes N <= 256
+                                const int len = min(__ffs(~x) - 1, 8);
+                                m &= ~(((1u << len) - 1u) << ta);
+                                const unsigned b0 = sb0 + (unsigned) __popc(mask & ((1u << ta) - 1u)) * Cfg::BBYTES;
+                                if (I8)
+                                {
+                                    // slices s, t (0-based) with s + t <= 4 into
+                                    // level s + t's INT32 accumulators,
+                                    // [level][tile]; K = 32 per instruction
+                                    const uint32_t id = TC8_IDESC | idesc_n(len);
 #pragma unroll
-                    for (int ks = 0; ks < 2; ++ks)
-                    {
-                        // K = 16: two 8-wide k-chunks per step
-                        const uint64_t ah = smem_desc(a0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
-                        const uint64_t al = smem_desc(a1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
-                        const uint64_t bh = smem_desc(b0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
-                        const uint64_t bl = smem_desc(b1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
-                        umma_f16(d, ah, bh, acc);
-                        umma_f16(d, ah, bl, 1u);
-                        umma_f16(d, al, bh, 1u);
-                        acc = 1u;
+                                    for (int sa = 0; sa < TC8_SLICES; ++sa)
+#pragma unroll
+                                        for (int sb = 0; sb + sa < TC8_LEVELS; ++sb)
+                                            umma_i8(tbase + (unsigned) ((sa + sb) * TC_TILES * 32 + ta * 32),
+                                                    smem_desc(a0 + sa * (TC_GROUP * TC8_IMG), TC8_LBO, TC8_SBO),
+                                                    smem_desc(b0 + sb * 256, TC8_LBO, TC8_RSBO), id,
+                                                    sa == 0 ? st : 1u);
+                                    continue;
+                                }
+                                const unsigned d = tbase + (unsigned) (ta * 32);
+                                const unsigned a1 = a0 + TC_GROUP * 2 * IMG;
+                                const uint32_t id = TC_IDESC | idesc_n(len);
+                                unsigned acc = st;
+#pragma unroll
+                                for (int ks = 0; ks < 2; ++ks)
+                                {
+                                    // K = 16: two 8-wide k-chunks per step
+                                    const uint64_t ah = smem_desc(a0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
+                                    const uint64_t al = smem_desc(a1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
+                                    const uint64_t bh = smem_desc(b0 + ks * 2 * TC_LBO, TC_LBO, TC_RSBO);
+                                    const uint64_t bl = smem_desc(b0 + TC_RLO + ks * 2 * TC_LBO, TC_LBO, TC_RSBO);
+                                    umma_f16(d, ah, bh, id, acc);
+                                    umma_f16(d, ah, bl, id, 1u);
+                                    umma_f16(d, al, bh, id, 1u);
+                                    acc = 1u;
+                                }
+                            }
+                            umma_commit(&S.empty_b[e]);
+                        }
+                        __syncwarp();
+                        any = true;
+                        started |= mask;
+                        ++ga;
+                        bh = h + need;
+                        ++gs;
+                        used = s0 + need;
                     }
-                    umma_commit(&S.empty_b[b]);
-                    ++gp;
+                    if (used == 0)
+                        quit = true; // the producer flagged it
+                    p += used;
                 }
                 // the wave's last left operand, then every MMA of the wave
                 // (and before) done -> done barrier
-                if (p1 > p0)
-                    umma_commit(&S.empty_a[acur]);
-                umma_commit(&S.done);
+                if (lane == 0)
+                {
+                    if (any)
+                        umma_commit(&S.empty_a[acur]);
+                    umma_commit(&S.done);
+                }
             }
             // the other lanes of warps 0 and 1 wait here, not in a polling
             // loop beside their working lane
@@ -1107,7 +1296,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                     for (int lev = TC8_LEVELS - 1; lev >= 0; --lev)
                     {
                         float w[32];
-                        tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32 * TC8_LEVELS + lev * 32),
+                        tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (lev * TC_TILES * 32 + t * 32),
                                   w);
 #pragma unroll
                         for (int c = 0; c < 32; ++c)
@@ -1238,11 +1427,8 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     {
         // bulk copies still in flight land before the CTA leaves: the last
         // fill of every buffer (bounded waits)
-        for (unsigned b = 0; b < TC_BBUF && b < gp; ++b)
-        {
-            const unsigned last = (gp - 1 - b) / TC_BBUF; // fill index of buffer (gp-1-b) % TC_BBUF
-            mbar_wait2s(&S.full_b[(gp - 1 - b) % TC_BBUF], last & 1);
-        }
+        for (unsigned b = 0; b < TC_BBUF && b < gs; ++b)
+            mbar_wait2s(&S.full_b[(gs - 1 - b) % TC_BBUF], ((gs - 1 - b) / TC_BBUF) & 1);
         for (unsigned a = 0; a < TC_ABUF && a < copied_a; ++a)
             mbar_wait2s(&S.full_a[(copied_a - 1 - a) % TC_ABUF], ((copied_a - 1 - a) / TC_ABUF) & 1);
     }
@@ -1264,7 +1450,8 @@ bool tc_split(B200Context *c, const bml_matrix_ellblock_t *X, int sgrid, unsigne
     tc_maxabs_kernel<T><<<sgrid, 256, 0, c->stream>>>(pool, X->d_nnzb, X->NB, X->MB, X->slot_elems, maxbits);
     if (!LAUNCH_OK("tc_maxabs_kernel"))
         return false;
-    tc_split_kernel<T><<<sgrid, 256, 0, c->stream>>>(pool, X->d_nnzb, X->NB, X->MB, X->slot_elems, maxbits, img);
+    tc_split_kernel<T><<<sgrid, TC_SPLIT_WARPS * 32, 0, c->stream>>>(pool, X->d_nnzb, X->NB, X->MB, X->slot_elems,
+                                                                      maxbits, img);
     return LAUNCH_OK("tc_split_kernel");
 }
 
@@ -1288,8 +1475,9 @@ bool tc8_split(B200Context *c, const bml_matrix_ellblock_t *X, int sgrid, unsign
 }
 
 // The 8-bit mode's shape: 3 tiles of five 32-column level accumulators
-// (480 of the 512 TMEM columns), one CTA per SM; buffers of five slices.
-using TcShape8 = TcCfg<3, 1, 3, 8, TC_GROUP * TC8_SLICES * TC8_IMG, TC8_SLICES * TC8_IMG>;
+// (480 of the 512 TMEM columns), one CTA per SM, so the rings take most of
+// the SM's shared memory: 5 left buffers and 18 right slots of five slices.
+using TcShape8 = TcCfg<3, 1, 5, 18, TC_GROUP * TC8_SLICES * TC8_IMG, TC8_SLICES * TC8_IMG>;
 
 template <typename T, class Cfg, bool I8>
 bool tc_launch(B200Context *c, const bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, const TcTab &tab,
