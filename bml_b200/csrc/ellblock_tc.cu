@@ -331,13 +331,20 @@ __device__ __forceinline__ void tc8_slices(double u, signed char (&a)[TC8_SLICES
 // left slices 1..5 (element (r, k) of the block, scaled by sigma of scalar
 // row r) at +0, +1 KB, ..., +4 KB, then the right slices 1..5 (element
 // (n, k) = block (k, n), scaled by tau of scalar column n) interleaved by row
-// group in 5 KB.
+// group in 5 KB.  One warp per block, lane c on column c: the right slices
+// are packed in registers, the left ones go through a shared-memory
+// transpose; both are written in 16-byte stores.
+constexpr int TC8_SPLIT_WARPS = 4; // 30 KB of static shared memory
+
 template <typename T>
-__global__ void tc8_split_kernel(const T *pool, const int *indexb, const int *nnzb, int NB, int MB,
-                                 long long slot_elems, const unsigned long long *rowmax,
-                                 const unsigned long long *colmax, signed char *img)
+__global__ void __launch_bounds__(TC8_SPLIT_WARPS * 32)
+    tc8_split_kernel(const T *pool, const int *indexb, const int *nnzb, int NB, int MB, long long slot_elems,
+                     const unsigned long long *rowmax, const unsigned long long *colmax, signed char *img)
 {
-    for (long long s = blockIdx.x; s < (long long) NB * MB; s += gridDim.x)
+    __shared__ __align__(16) signed char sh[TC8_SPLIT_WARPS][TC8_SLICES][TB][TB + 16]; // rows of 48 B
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const long long warps = (long long) gridDim.x * TC8_SPLIT_WARPS;
+    for (long long s = (long long) blockIdx.x * TC8_SPLIT_WARPS + wq; s < (long long) NB * MB; s += warps)
     {
         const int ib = (int) (s / MB), jp = (int) (s % MB);
         if (jp >= nnzb[ib])
@@ -345,20 +352,46 @@ __global__ void tc8_split_kernel(const T *pool, const int *indexb, const int *nn
         const int jb = indexb[s];
         const T *x = pool + s * slot_elems;
         signed char *o = img + s * TC8_BLOCK_BYTES;
-        for (int e = threadIdx.x; e < IMG; e += blockDim.x)
+        const int ec = -tc8_exp(colmax[(size_t) jb * TB + lane]);
+        unsigned rp[TC8_SLICES][2][4]; // right slices: [slice][k-chunk][4 bytes per word]
+#pragma unroll
+        for (int q = 0; q < TC8_SLICES; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    rp[q][h][i] = 0u;
+#pragma unroll
+        for (int r = 0; r < TB; ++r)
         {
-            const int r = e >> 5, c = e & 31;
-            const double v = (double) x[e];
+            const double v = (double) x[r * TB + lane];
             signed char a[TC8_SLICES];
             tc8_slices(ldexp(v, -tc8_exp(rowmax[(size_t) ib * TB + r])), a);
 #pragma unroll
             for (int q = 0; q < TC8_SLICES; ++q)
-                o[q * TC8_IMG + img8_off(r, c)] = a[q];
-            tc8_slices(ldexp(v, -tc8_exp(colmax[(size_t) jb * TB + c])), a);
+                sh[wq][q][r][lane] = a[q];
+            tc8_slices(ldexp(v, ec), a);
+            // byte r & 15 of k-chunk r >> 4: word (r & 15) >> 2, shift 8 (r & 3)
 #pragma unroll
             for (int q = 0; q < TC8_SLICES; ++q)
-                o[TC8_SLICES * TC8_IMG + rimg8_off(c, r, q)] = a[q];
+                rp[q][r >> 4][(r & 15) >> 2] |= (unsigned) (unsigned char) a[q] << (8 * (r & 3));
         }
+        // right: n = lane, sixteen consecutive k per store
+#pragma unroll
+        for (int q = 0; q < TC8_SLICES; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                *reinterpret_cast<uint4 *>(o + TC8_SLICES * TC8_IMG + rimg8_off(lane, h * 16, q)) =
+                    make_uint4(rp[q][h][0], rp[q][h][1], rp[q][h][2], rp[q][h][3]);
+        __syncwarp();
+        // left: row r = lane, sixteen consecutive columns per store
+#pragma unroll
+        for (int q = 0; q < TC8_SLICES; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                *reinterpret_cast<uint4 *>(o + q * TC8_IMG + img8_off(lane, h * 16)) =
+                    *reinterpret_cast<const uint4 *>(&sh[wq][q][lane][h * 16]);
+        __syncwarp();
     }
 }
 
@@ -845,17 +878,24 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             G.jmask[j] = m;
         }
         // ---- output block columns K: a bitmap over NB, tiles by rank ----
+        // (each warp takes 32 J entries at a time, their rows' lengths loaded
+        // at once, then walks the rows one by one)
         int badk = 0;
-        for (int j = warp; j < nJ; j += TC_THREADS / 32)
+        for (int j0 = warp * 32; j0 < nJ; j0 += TC_THREADS)
         {
-            const int jb = G.jb[j];
-            for (int kp = lane; kp < X.nnzb[jb]; kp += 32)
+            const int jl = j0 + lane;
+            const int jbl = jl < nJ ? G.jb[jl] : 0, nl = jl < nJ ? X.nnzb[jbl] : 0;
+            for (int i = 0; i < min(32, nJ - j0); ++i)
             {
-                const int kb = X.indexb[(size_t) jb * X.MB + kp];
-                if (kb < 0 || kb >= X.NB)
-                    badk = 1;
-                else
-                    atomicOr(&S.su.kbits[kb >> 5], 1u << (kb & 31));
+                const int jb = __shfl_sync(FULL, jbl, i), n = __shfl_sync(FULL, nl, i);
+                for (int kp = lane; kp < n; kp += 32)
+                {
+                    const int kb = X.indexb[(size_t) jb * X.MB + kp];
+                    if (kb < 0 || kb >= X.NB)
+                        badk = 1;
+                    else
+                        atomicOr(&S.su.kbits[kb >> 5], 1u << (kb & 31));
+                }
             }
         }
         if (__syncthreads_or(badk))
@@ -903,25 +943,53 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             G.ttouch[t] = 0;
         __syncthreads();
         // the output tile of every pair (j, kp), and the rows each tile touches
-        for (int j = warp; j < nJ; j += TC_THREADS / 32)
+        for (int j0 = warp * 32; j0 < nJ; j0 += TC_THREADS)
         {
-            const int jb = G.jb[j], ps = G.jstart[j];
-            const int m = G.jmask[j];
-            for (int kp = lane; kp < X.nnzb[jb]; kp += 32)
+            const int jl = j0 + lane;
+            int jbl = 0, psl = 0, nl = 0, ml = 0;
+            if (jl < nJ)
             {
-                const int kb = X.indexb[(size_t) jb * X.MB + kp];
-                const int t = S.su.kpre[kb >> 5] + __popc(S.su.kbits[kb >> 5] & ((1u << (kb & 31)) - 1u));
-                G.ptile[ps + kp] = t;
-                atomicOr(&G.ttouch[t], m);
+                jbl = G.jb[jl];
+                psl = G.jstart[jl];
+                nl = G.jstart[jl + 1] - psl;
+                ml = G.jmask[jl];
+            }
+            for (int i = 0; i < min(32, nJ - j0); ++i)
+            {
+                const int jb = __shfl_sync(FULL, jbl, i), ps = __shfl_sync(FULL, psl, i);
+                const int n = __shfl_sync(FULL, nl, i), m = __shfl_sync(FULL, ml, i);
+                for (int kp = lane; kp < n; kp += 32)
+                {
+                    const int kb = X.indexb[(size_t) jb * X.MB + kp];
+                    const int t = S.su.kpre[kb >> 5] + __popc(S.su.kbits[kb >> 5] & ((1u << (kb & 31)) - 1u));
+                    G.ptile[ps + kp] = t;
+                    atomicOr(&G.ttouch[t], m);
+                }
             }
         }
         __syncthreads();
         // ---- the pairs sorted by wave (a stable counting sort) ----
-        for (int w = tid; w < nW; w += TC_THREADS)
-            S.wpos[w] = 0;
+        // The J entries are cut into nq ranges of consecutive entries, one
+        // per warp (nq = 4 when four rows of wave counters fit, else 1); warp
+        // q places its range's pairs, in (j, kp) order, after those of the
+        // earlier ranges in every wave: stable.
+        const int nq = nW <= TC_NWCAP ? TC_THREADS / 32 : 1;
+        int *cnt = S.wpos; // [nq][nW]: pairs per range and wave, then the next free place
+        for (int w = tid; w < nq * nW; w += TC_THREADS)
+            cnt[w] = 0;
         __syncthreads();
-        for (int p = tid; p < npairs; p += TC_THREADS)
-            atomicAdd(&S.wpos[G.ptile[p] / TC_TILES], 1);
+        const int jlo = (int) ((long long) nJ * warp / nq), jhi = (int) ((long long) nJ * (warp + 1) / nq);
+        if (nq == 1)
+        {
+            for (int p = tid; p < npairs; p += TC_THREADS)
+                atomicAdd(&cnt[G.ptile[p] / TC_TILES], 1);
+        }
+        else
+        {
+            const int pl = G.jstart[jlo], ph = G.jstart[jhi];
+            for (int p = pl + lane; p < ph; p += 32)
+                atomicAdd(&cnt[warp * nW + G.ptile[p] / TC_TILES], 1);
+        }
         __syncthreads();
         if (warp == 0)
         {
@@ -929,7 +997,10 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             for (int w0 = 0; w0 < nW; w0 += 32)
             {
                 const int w = w0 + lane;
-                const int n = w < nW ? S.wpos[w] : 0;
+                int n = 0;
+                if (w < nW)
+                    for (int q = 0; q < nq; ++q)
+                        n += cnt[q * nW + w];
                 int incl = n;
                 for (int o = 1; o < 32; o <<= 1)
                 {
@@ -939,38 +1010,62 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                 }
                 if (w < nW)
                 {
-                    S.wpos[w] = run + incl - n;
-                    G.wstart[w] = run + incl - n;
+                    int base = run + incl - n;
+                    G.wstart[w] = base;
+                    for (int q = 0; q < nq; ++q)
+                    {
+                        const int c = cnt[q * nW + w];
+                        cnt[q * nW + w] = base;
+                        base += c;
+                    }
                 }
                 run += __shfl_sync(FULL, incl, 31);
             }
             if (lane == 0)
                 G.wstart[nW] = run;
-            __syncwarp();
-            // one warp places the pairs in (j, kp) order: stable
-            for (int j = 0; j < nJ; ++j)
+        }
+        __syncthreads();
+        if (warp < nq)
+        {
+            int *wpos = cnt + warp * nW;
+            for (int j0 = jlo; j0 < jhi; j0 += 32)
             {
-                const int jb = G.jb[j], ps = G.jstart[j], n = G.jstart[j + 1] - ps;
-                const uint2 sl = G.jslot[j];
-                for (int k0 = 0; k0 < n; k0 += 32)
+                const int jl = j0 + lane;
+                int jbl = 0, psl = 0, nl = 0;
+                uint2 sll = make_uint2(0u, 0u);
+                if (jl < jhi)
                 {
-                    const int kp = k0 + lane;
-                    const int t = kp < n ? G.ptile[ps + kp] : -1;
-                    const int w = t >= 0 ? t / TC_TILES : -1 - lane;
-                    const unsigned peers = __match_any_sync(FULL, w);
-                    const int leader = __ffs(peers) - 1;
-                    int base = 0;
-                    if (lane == leader && t >= 0)
+                    jbl = G.jb[jl];
+                    psl = G.jstart[jl];
+                    nl = G.jstart[jl + 1] - psl;
+                    sll = G.jslot[jl];
+                }
+                for (int i = 0; i < min(32, jhi - j0); ++i)
+                {
+                    const int j = j0 + i;
+                    const int jb = __shfl_sync(FULL, jbl, i), ps = __shfl_sync(FULL, psl, i);
+                    const int n = __shfl_sync(FULL, nl, i);
+                    const unsigned slx = __shfl_sync(FULL, sll.x, i), sly = __shfl_sync(FULL, sll.y, i);
+                    for (int k0 = 0; k0 < n; k0 += 32)
                     {
-                        base = S.wpos[w];
-                        S.wpos[w] = base + __popc(peers);
-                    }
-                    base = __shfl_sync(FULL, base, leader);
-                    if (t >= 0)
-                    {
-                        const int pos = base + __popc(peers & lanemask_lt());
-                        G.list[pos] = make_uint4((unsigned) (t - w * TC_TILES) | ((unsigned) j << 4),
-                                                 (unsigned) jb * (unsigned) X.MB + (unsigned) kp, sl.x, sl.y);
+                        const int kp = k0 + lane;
+                        const int t = kp < n ? G.ptile[ps + kp] : -1;
+                        const int w = t >= 0 ? t / TC_TILES : -1 - lane;
+                        const unsigned peers = __match_any_sync(FULL, w);
+                        const int leader = __ffs(peers) - 1;
+                        int base = 0;
+                        if (lane == leader && t >= 0)
+                        {
+                            base = wpos[w];
+                            wpos[w] = base + __popc(peers);
+                        }
+                        base = __shfl_sync(FULL, base, leader);
+                        if (t >= 0)
+                        {
+                            const int pos = base + __popc(peers & lanemask_lt());
+                            G.list[pos] = make_uint4((unsigned) (t - w * TC_TILES) | ((unsigned) j << 4),
+                                                     (unsigned) jb * (unsigned) X.MB + (unsigned) kp, slx, sly);
+                        }
                     }
                 }
             }
@@ -1469,8 +1564,8 @@ bool tc8_split(B200Context *c, const bml_matrix_ellblock_t *X, int sgrid, unsign
                                                    colmax);
     if (!LAUNCH_OK("tc8_max_kernel"))
         return false;
-    tc8_split_kernel<T><<<sgrid, 256, 0, c->stream>>>(pool, X->d_indexb, X->d_nnzb, X->NB, X->MB, X->slot_elems, rowmax,
-                                                     colmax, img);
+    tc8_split_kernel<T><<<sgrid, TC8_SPLIT_WARPS * 32, 0, c->stream>>>(pool, X->d_indexb, X->d_nnzb, X->NB, X->MB,
+                                                                        X->slot_elems, rowmax, colmax, img);
     return LAUNCH_OK("tc8_split_kernel");
 }
 
