@@ -1400,11 +1400,13 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                     const int kb = G.klist[t0 + t];
                     if (myrow >= X.NB || !((G.ttouch[t0 + t] >> warp) & 1))
                         continue;
+                    // the power of two of scalar column c, from lane c
+                    const double cs = ldexp(1.0, tc8_exp(colmax[(size_t) kb * TB + lane]));
                     double mx = 0.0, diag = 0.0;
 #pragma unroll
                     for (int c = 0; c < 32; ++c)
                     {
-                        v[c] *= srow * ldexp(1.0, tc8_exp(colmax[(size_t) kb * TB + c]));
+                        v[c] *= srow * __shfl_sync(FULL, cs, c);
                         mx = fmax(mx, fabs(v[c]));
                         diag = c == lane ? v[c] : diag;
                     }
