@@ -1386,7 +1386,12 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                 const double srow = myrow < X.NB ? ldexp(1.0, tc8_exp(rowmax[(size_t) myrow * TB + lane]) - 12) : 0.0;
                 for (int t = 0; t < nt; ++t)
                 {
-                    // the four levels, highest first: v = ((D5 2^-7 + D4) 2^-7 + D3) 2^-7 + D2
+                    // a row without products in the tile skips it (the warp
+                    // reads only its own row's lanes of tensor memory)
+                    const int kb = G.klist[t0 + t];
+                    if (myrow >= X.NB || !((G.ttouch[t0 + t] >> warp) & 1))
+                        continue;
+                    // the five levels, highest first: v = (((D6 2^-7 + D5) 2^-7 + D4) 2^-7 + D3) 2^-7 + D2
                     double v[32];
                     for (int lev = TC8_LEVELS - 1; lev >= 0; --lev)
                     {
@@ -1397,9 +1402,6 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                         for (int c = 0; c < 32; ++c)
                             v[c] = (lev == TC8_LEVELS - 1 ? 0.0 : v[c] * 0x1p-7) + (double) __float_as_int(w[c]);
                     }
-                    const int kb = G.klist[t0 + t];
-                    if (myrow >= X.NB || !((G.ttouch[t0 + t] >> warp) & 1))
-                        continue;
                     // the power of two of scalar column c, from lane c
                     const double cs = ldexp(1.0, tc8_exp(colmax[(size_t) kb * TB + lane]));
                     double mx = 0.0, diag = 0.0;
@@ -1451,14 +1453,14 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
             }
             for (int t = 0; t < (I8 ? 0 : nt); ++t)
             {
+                const int kb = G.klist[t0 + t];
+                if (myrow >= X.NB || !((G.ttouch[t0 + t] >> warp) & 1))
+                    continue;
                 float v[32];
                 tmem_ld32(tbase + ((unsigned) (warp * 32) << 16) + (unsigned) (t * 32), v);
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
                     v[c] *= unscale; // undo the split's 2^s on both factors
-                const int kb = G.klist[t0 + t];
-                if (myrow >= X.NB || !((G.ttouch[t0 + t] >> warp) & 1))
-                    continue;
                 float mx = 0.f, diag = 0.f;
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
