@@ -30,10 +30,10 @@
 // the largest group: the kernel takes groups of any size.
 // Operands are staged into shared memory in the UMMA canonical K-major
 // no-swizzle layout (8-row x 16-byte core matrices).  A split kernel first
-// writes every block of X in that layout, as the left operand (rows x k, 2 KB
-// per part) and as the right operand (columns x k, the block transposed, its
-// parts interleaved by row group), so staging is one bulk copy
-// (cp.async.bulk, completing on an mbarrier) per block and part.  The pairs
+// writes every block of X in that layout, as the left operand (rows x k) and
+// as the right operand (columns x k, the block transposed), the parts of each
+// interleaved by row group, so staging is one bulk copy (cp.async.bulk,
+// completing on an mbarrier) per block.  The pairs
 // of one wave and one block column jb form a step: one left operand (the
 // group's four blocks of column jb) and at most one right operand per tile.
 // A producer warp copies a step's left operand into a ring of buffers and its
@@ -121,25 +121,16 @@ __device__ __forceinline__ int tc_scale_exp(unsigned maxbits)
     return min(max(14 - e, -100), 100);
 }
 
-// 16-bit image of a block in the K-major no-swizzle layout, as a left operand
-// (element (r, k) of the block): 16-byte rows of 8 k, 8-row core matrices of
-// 128 bytes; the four k-chunks of an 8-row group sit next to each other
-// (LBO = 128 B) and the row groups follow at SBO = 512 B, so each 32 x 32
-// block is one contiguous 2 KB image and four blocks stack into the 128-row
-// left operand.
-constexpr unsigned TC_LBO = 128, TC_SBO = 512;
-
-__device__ __forceinline__ int img_off(int row, int k)
-{
-    return (row >> 3) * 256 + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
-}
-
-// The right operand (element (n, k) = block (k, n)) keeps hi and lo of an
-// 8-row group together: row group g at g * 1 KB, hi at +0 and lo at +512 B,
-// each four k-chunks of 128 B.  A block is then one 4 KB image whose row
-// groups follow at a uniform SBO = 1 KB, so the images of consecutive output
-// tiles, placed side by side, form one operand of N = 32 x (tiles).
-constexpr unsigned TC_RSBO = 1024, TC_RLO = 512;
+// 16-bit images of a block in the K-major no-swizzle layout, as a left
+// operand (element (row, k) = block (r, k)) or a right operand (element
+// (row, k) = block (k, n), row = n): 16-byte rows of 8 k, 8-row core
+// matrices of 128 bytes, the four k-chunks of an 8-row group side by side
+// (LBO = 128 B); hi and lo of a row group together, row group g at g * 1 KB,
+// hi at +0 and lo at +512 B.  A block is then one 4 KB image whose row
+// groups follow at a uniform SBO = 1 KB, so four blocks placed one after the
+// other form the 128-row left operand, and the images of consecutive output
+// tiles side by side one right operand of N = 32 x (tiles).
+constexpr unsigned TC_LBO = 128, TC_RSBO = 1024, TC_RLO = 512;
 
 __device__ __forceinline__ int rimg_off(int n, int k, int part)
 {
@@ -169,8 +160,8 @@ __global__ void tc_maxabs_kernel(const T *pool, const int *nnzb, int NB, int MB,
 }
 
 // Split every stored block of X, scaled by 2^s, into its images at
-// img + slot*4*IMG: left hi, left lo (2 KB each), then the right operand's
-// hi and lo interleaved by row group (4 KB).  One warp per block: lane c
+// img + slot*4*IMG: the left operand's hi and lo interleaved by row group
+// (4 KB), then the right operand's (4 KB).  One warp per block: lane c
 // holds column c of every row; the right image (n = c) is written from
 // registers, the left one (row r) through a shared-memory transpose, both in
 // 16-byte stores.
@@ -223,7 +214,7 @@ __global__ void __launch_bounds__(TC_SPLIT_WARPS * 32)
         for (int part = 0; part < 2; ++part)
 #pragma unroll
             for (int kc = 0; kc < 4; ++kc)
-                *reinterpret_cast<uint4 *>(o + part * IMG + img_off(lane, kc * 8)) =
+                *reinterpret_cast<uint4 *>(o + rimg_off(lane, kc * 8, part)) =
                     *reinterpret_cast<const uint4 *>(&sh[wq][part][lane][kc * 8]);
         __syncwarp();
     }
@@ -251,20 +242,17 @@ constexpr int TC8_LEVELS = TC8_SLICES;  // s + t = 2..6
 constexpr int TC8_IMG = TB * TB;        // bytes per 8-bit slice image of a block (1 KB)
 constexpr int TC8_BLOCK_BYTES = 2 * TC8_SLICES * TC8_IMG; // left slices | right slices
 constexpr int TC16_BLOCK_BYTES = 8 * IMG;                 // left hi, lo | right hi, lo
+constexpr int TC_ZERO_BYTES = TC8_BLOCK_BYTES / 2;        // a zero left image, either split
 constexpr int TC8_MAX_COLS = 3276;      // block columns per group the level sums hold
-constexpr unsigned TC8_LBO = 128, TC8_SBO = 256;
+constexpr unsigned TC8_LBO = 128;
 
-// Byte offset of element (row, k) in an 8-bit K-major no-swizzle image:
+// Byte offset of element (row, k) in an 8-bit image, left or right operand:
 // 16-byte rows of 16 k, 8-row core matrices of 128 bytes, the two k-chunks
-// of an 8-row group side by side (LBO = 128 B), row groups at SBO = 256 B.
-__device__ __forceinline__ int img8_off(int row, int k)
-{
-    return (row >> 3) * 256 + (k >> 4) * 128 + (row & 7) * 16 + (k & 15);
-}
-
-// The right operand's five slices interleaved by row group: row group g at
-// g * 1280 B, slice s at +256 s; a block is one 5 KB image with a uniform
-// SBO = 1280 B, so consecutive tiles' images form one wider operand.
+// of an 8-row group side by side (LBO = 128 B), the five slices of a row
+// group together, row group g at g * 1280 B and slice s at +256 s.  A block
+// is one 5 KB image with a uniform SBO = 1280 B, so four blocks stack into
+// the 128-row left operand and consecutive tiles' images form one wider
+// right operand.
 constexpr unsigned TC8_RSBO = 1280;
 
 __device__ __forceinline__ int rimg8_off(int n, int k, int s)
@@ -328,10 +316,10 @@ __device__ __forceinline__ void tc8_slices(double u, signed char (&a)[TC8_SLICES
 }
 
 // Slice every stored block of X into its 8-bit images at img + slot * 10 KB:
-// left slices 1..5 (element (r, k) of the block, scaled by sigma of scalar
-// row r) at +0, +1 KB, ..., +4 KB, then the right slices 1..5 (element
-// (n, k) = block (k, n), scaled by tau of scalar column n) interleaved by row
-// group in 5 KB.  One warp per block, lane c on column c: the right slices
+// the left slices 1..5 (element (r, k) of the block, scaled by sigma of
+// scalar row r), then the right slices 1..5 (element (n, k) = block (k, n),
+// scaled by tau of scalar column n), each operand interleaved by row group in
+// 5 KB.  One warp per block, lane c on column c: the right slices
 // are packed in registers, the left ones go through a shared-memory
 // transpose; both are written in 16-byte stores.
 constexpr int TC8_SPLIT_WARPS = 4; // 30 KB of static shared memory
@@ -389,7 +377,7 @@ __global__ void __launch_bounds__(TC8_SPLIT_WARPS * 32)
         for (int q = 0; q < TC8_SLICES; ++q)
 #pragma unroll
             for (int h = 0; h < 2; ++h)
-                *reinterpret_cast<uint4 *>(o + q * TC8_IMG + img8_off(lane, h * 16)) =
+                *reinterpret_cast<uint4 *>(o + rimg8_off(lane, h * 16, q)) =
                     *reinterpret_cast<const uint4 *>(&sh[wq][q][lane][h * 16]);
         __syncwarp();
     }
@@ -731,8 +719,6 @@ __global__ void __launch_bounds__(TC_THREADS) tc_count_kernel(TcView<T> X, int *
         __syncthreads();
     }
 }
-
-__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 // Position of X[ib0+q, jb] in row ib0+q from a record's z, w (0xFFFF: none).
 __device__ __forceinline__ unsigned rec_slot(const uint4 &r, int q)
@@ -1153,9 +1139,7 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                 // MMAs that read the buffer's or slots' previous fill are
                 // done.  Lane 0 waits and arms the barriers; the counters are
                 // alike in all lanes.
-                constexpr int NPART = I8 ? TC8_SLICES : 2;
-                constexpr unsigned PBYTES = BLK / 2 / NPART;
-                static_assert(TC_GROUP * NPART <= 32, "a lane per left block and part");
+
                 bool quit = false;
                 for (int p = p0; p < p1 && !quit;)
                 {
@@ -1209,17 +1193,16 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
                             quit = true;
                             break;
                         }
-                        if (lane < TC_GROUP * NPART)
+                        if (lane < TC_GROUP)
                         {
-                            // 16 KB (FP16: hi and lo, 2 parts of 2 KB per
-                            // block) or 20 KB (8-bit: 5 slices of 1 KB per
-                            // block); part p of the four blocks stacks into
-                            // the 128-row operand
-                            const int q = lane / NPART, part = lane % NPART;
+                            // block q's left image (4 KB: hi and lo; or 5 KB:
+                            // five slices), one copy; the four stack into the
+                            // 128-row operand
+                            const int q = lane;
                             const unsigned jp = ((q < 2 ? rz : rw) >> ((q & 1) * 16)) & 0xFFFFu;
                             const unsigned char *src =
-                                jp != 0xFFFFu ? img + ((size_t) (ib0 + q) * X.MB + jp) * BLK + part * PBYTES : zimg;
-                            bulk_copy(S.a[a] + part * (TC_GROUP * PBYTES) + q * PBYTES, src, PBYTES, &S.full_a[a]);
+                                jp != 0xFFFFu ? img + ((size_t) (ib0 + q) * X.MB + jp) * BLK : zimg;
+                            bulk_copy(S.a[a] + q * (BLK / 2), src, BLK / 2, &S.full_a[a]);
                         }
                         if (lane >= s0 && lane < s0 + need)
                         {
@@ -1319,21 +1302,21 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
 #pragma unroll
                                         for (int sb = 0; sb + sa < TC8_LEVELS; ++sb)
                                             umma_i8(tbase + (unsigned) ((sa + sb) * TC_TILES * 32 + ta * 32),
-                                                    smem_desc(a0 + sa * (TC_GROUP * TC8_IMG), TC8_LBO, TC8_SBO),
+                                                    smem_desc(a0 + sa * 256, TC8_LBO, TC8_RSBO),
                                                     smem_desc(b0 + sb * 256, TC8_LBO, TC8_RSBO), id,
                                                     sa == 0 ? st : 1u);
                                     continue;
                                 }
                                 const unsigned d = tbase + (unsigned) (ta * 32);
-                                const unsigned a1 = a0 + TC_GROUP * 2 * IMG;
+                                const unsigned a1 = a0 + TC_RLO;
                                 const uint32_t id = TC_IDESC | idesc_n(len);
                                 unsigned acc = st;
 #pragma unroll
                                 for (int ks = 0; ks < 2; ++ks)
                                 {
                                     // K = 16: two 8-wide k-chunks per step
-                                    const uint64_t ah = smem_desc(a0 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
-                                    const uint64_t al = smem_desc(a1 + ks * 2 * TC_LBO, TC_LBO, TC_SBO);
+                                    const uint64_t ah = smem_desc(a0 + ks * 2 * TC_LBO, TC_LBO, TC_RSBO);
+                                    const uint64_t al = smem_desc(a1 + ks * 2 * TC_LBO, TC_LBO, TC_RSBO);
                                     const uint64_t bh = smem_desc(b0 + ks * 2 * TC_LBO, TC_LBO, TC_RSBO);
                                     const uint64_t bl = smem_desc(b0 + TC_RLO + ks * 2 * TC_LBO, TC_LBO, TC_RSBO);
                                     umma_f16(d, ah, bh, id, acc);
@@ -1694,7 +1677,7 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
     const size_t n_img = (size_t) NB * MB * (i8 ? TC8_BLOCK_BYTES : TC16_BLOCK_BYTES);
     const size_t off_tr = al(n_img);
     const size_t off_zero = al(off_tr + (size_t) 2 * NB * sizeof(double));
-    const size_t off_max = al(off_zero + 2 * IMG);
+    const size_t off_max = al(off_zero + TC_ZERO_BYTES);
     const size_t n_scalar = (size_t) NB * TB;
     const size_t off_tab = al(off_max + (i8 ? 2 * n_scalar * sizeof(unsigned long long) : 0));
     unsigned char *scr = static_cast<unsigned char *>(b200_scratch(off_tab + tab_bytes));
@@ -1724,7 +1707,7 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
         tab.wstart = reinterpret_cast<int *>(take(8));
     }
     if (!CUDA_OK(cudaMemsetAsync(flags, 0, 64, c->stream)) ||
-        !CUDA_OK(cudaMemsetAsync(zimg, 0, 2 * IMG, c->stream)) ||
+        !CUDA_OK(cudaMemsetAsync(zimg, 0, TC_ZERO_BYTES, c->stream)) ||
         !CUDA_OK(cudaMemsetAsync(dA, 0, (size_t) 2 * NB * sizeof(double), c->stream)) ||
         (i8 && !CUDA_OK(cudaMemsetAsync(rowmax, 0, 2 * n_scalar * sizeof(unsigned long long), c->stream))))
         return false;
