@@ -841,8 +841,10 @@ def ellblock_sp2_leg(iters=5, nclose=2):
     `iters` iterations from X0, every X^2 in FP64 against bulk X^2 on the
     tensor cores and the last `nclose` in FP64, with their errors, for both
     splits of the tensor-core X^2 (FP16 hi/lo with FP32 accumulation, and
-    8-bit slices with exact INT32 accumulation).  Device time by CUDA events
-    on the library stream."""
+    8-bit slices with exact INT32 accumulation); the 8-bit split also with a
+    single closing FP64 iteration, which its exact accumulation allows at
+    the same error target.  Device time by CUDA events on the library
+    stream."""
     import bml_b200 as B
     H, n = ellblock_case(16)
     # warm-up: the exact and tensor-core X^2 size their device scratch once
@@ -854,7 +856,8 @@ def ellblock_sp2_leg(iters=5, nclose=2):
     B.lib.bml_deallocate(C.byref(hh))
     out = {}
     old_split = B.lib.bml_b200_set_tc_split(0)
-    for name, nc, split in (("fp64", iters, 0), ("mixed", nclose, 0), ("mixed_8bit", nclose, 1)):
+    for name, nc, split in (("fp64", iters, 0), ("mixed", nclose, 0), ("mixed_8bit", nclose, 1),
+                            ("mixed_8bit_close1", 1, 1)):
         D = B.lib.bml_zero_matrix(3, 2, n, n, 0)
         B.check()
         info = (C.c_double * 8)()
@@ -878,17 +881,18 @@ def ellblock_sp2_leg(iters=5, nclose=2):
     hh = C.c_void_p(H)
     B.lib.bml_deallocate(C.byref(hh))
     B.lib.bml_b200_reset_block_sizes()
-    e, m, m8 = out["fp64"], out["mixed"], out["mixed_8bit"]
+    e, m, m8, m81 = out["fp64"], out["mixed"], out["mixed_8bit"], out["mixed_8bit_close1"]
     rel = lambda a, b: abs(a - b) / abs(b)
-    m8.update({"speedup": e["s"] / m8["s"], "trace_rel_err": rel(m8["trace"], e["trace"]),
-               "energy_rel_err": rel(m8["energy_trDH"], e["energy_trDH"]),
-               "split": "8-bit slices (5 per entry), exact INT32 accumulation, FP64 recombination"})
+    for x, nc in ((m8, nclose), (m81, 1)):
+        x.update({"speedup": e["s"] / x["s"], "trace_rel_err": rel(x["trace"], e["trace"]),
+                  "energy_rel_err": rel(x["energy_trDH"], e["energy_trDH"]), "closing_fp64": nc,
+                  "split": "8-bit slices (5 per entry), exact INT32 accumulation, FP64 recombination"})
     return {"workload": "SP2 on the 16^3 block lattice Hamiltonian (4096 block rows of 32x32, N=131072, radius 2, "
                         "thr 1e-6, occ N/2), first %d iterations from X0" % iters,
             "iterations": iters, "closing_fp64": nclose, "fp64": e, "mixed": m, "speedup": e["s"] / m["s"],
             "trace_rel_err": rel(m["trace"], e["trace"]),
             "energy_rel_err": rel(m["energy_trDH"], e["energy_trDH"]),
-            "mixed_8bit": m8,
+            "mixed_8bit": m8, "mixed_8bit_close1": m81,
             "note": "bulk X^2 on the tensor cores (mixed: FP16 hi/lo split, FP32 accumulation; mixed_8bit: "
                     "8-bit slices, exact INT32 accumulation), the closing iterations on the FP64 block product"}
 

@@ -790,12 +790,12 @@ __global__ void __launch_bounds__(TC_THREADS, Cfg::CTAS)
     const unsigned tbase = S.tmem;
     const float unscale = ldexpf(1.0f, -2 * tc_scale_exp((unsigned) flags[8]));
     bool dead = false; // a wait timed out: stop issuing work
-    // pipeline counters, kept alike by the producer (thread 0) and the MMA
-    // issuer (thread 32): steps, right-operand slots (a running count) and
+    // pipeline counters, kept alike by the producer (warp 0) and the MMA
+    // issuer (warp 1): steps, right-operand slots (a running count) and
     // left operands issued so far; go: the producer's oldest step not yet
     // seen done
     unsigned gs = 0, bh = 0, ga = 0, go = 0, nwaves = 0;
-    unsigned copied_a = 0; // left operands whose copies thread 0 issued
+    unsigned copied_a = 0; // left operands whose copies warp 0 issued
 
     for (;;)
     {
@@ -1672,7 +1672,7 @@ bool eb_multiply_x2_tc(bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, doub
                        tab_bytes);
         return false;
     }
-    // 8 KB of images per block slot (either split), the traces, a zero
+    // 8 KB (FP16) or 10 KB (8-bit) of images per block slot, the traces, a zero
     // image, the 8-bit split's row and column maxima, the tables
     const size_t n_img = (size_t) NB * MB * (i8 ? TC8_BLOCK_BYTES : TC16_BLOCK_BYTES);
     const size_t off_tr = al(n_img);
