@@ -1559,7 +1559,13 @@ bool tc8_split(B200Context *c, const bml_matrix_ellblock_t *X, int sgrid, unsign
 // The 8-bit mode's shape: 3 tiles of five 32-column level accumulators
 // (480 of the 512 TMEM columns), one CTA per SM, so the rings take most of
 // the SM's shared memory: 5 left buffers and 18 right slots of five slices.
-using TcShape8 = TcCfg<3, 1, 5, 18, TC_GROUP * TC8_SLICES * TC8_IMG, TC8_SLICES * TC8_IMG>;
+#ifndef B200_TC8_ABUF
+#define B200_TC8_ABUF 5
+#endif
+#ifndef B200_TC8_BBUF
+#define B200_TC8_BBUF 18
+#endif
+using TcShape8 = TcCfg<3, 1, B200_TC8_ABUF, B200_TC8_BBUF, TC_GROUP * TC8_SLICES * TC8_IMG, TC8_SLICES * TC8_IMG>;
 
 template <typename T, class Cfg, bool I8>
 bool tc_launch(B200Context *c, const bml_matrix_ellblock_t *X, bml_matrix_ellblock_t *X2, const TcTab &tab,
