@@ -64,6 +64,9 @@ def parse():
                     help="the same for the SP2 iterate after one iteration (the second iteration's product)")
     ap.add_argument("--tc-split", type=int, default=0, choices=[0, 1],
                     help="split of the tensor-core X^2 in the profile cases: 0 FP16 hi/lo, 1 8-bit slices")
+    ap.add_argument("--profile-eb-sp2", action="store_true",
+                    help="one mixed ELLBLOCK SP2 run (16^3, 5 iterations, 8-bit split, 1 closing FP64 iteration) "
+                         "inside the NVTX range sp2, for an ncu launch list")
     ap.add_argument("--profile-eb-ops", action="store_true",
                     help="the one-pass ELLBLOCK operations, once each, for an ncu capture (7^3 block lattice)")
     ap.add_argument("--eb-ops-L", type=int, default=7, help="block lattice side for --profile-eb-ops")
@@ -760,6 +763,38 @@ def run_profile_tc(wide=False, split=0):
                       "blocks_x2": int(B.lib.bml_b200_nnz(X2)) // 1024}))
 
 
+def run_profile_eb_sp2(iters=5, nclose=1):
+    """The mixed ELLBLOCK SP2 of the ellblock_sp2 leg's mixed_8bit_close1
+    entry (16^3 block lattice, the 8-bit split for the bulk iterations, one
+    closing FP64 iteration), once to size the device memory, then once
+    inside the NVTX range "sp2"; prints its device time, the trace and the
+    number of tensor-core iterations."""
+    import bml_b200 as B
+    H, n = ellblock_case(16)
+    old = B.lib.bml_b200_set_tc_split(1)
+    nvtx = _nvtx()
+    for timed in (False, True):
+        D = B.lib.bml_zero_matrix(3, 2, n, n, 0)
+        B.check()
+        info = (C.c_double * 8)()
+        B.check(B.lib.bml_b200_synchronize())
+        if timed:
+            nvtx.range_push("sp2")
+        B.check(B.lib.bml_b200_event_record(6))
+        B.check(B.lib.bml_b200_ellblock_sp2_mixed(H, D, 1e-6, n / 2.0, iters, -1.0, 0, nclose, info))
+        B.check(B.lib.bml_b200_event_record(7))
+        B.check(B.lib.bml_b200_synchronize())
+        if timed:
+            nvtx.range_pop()
+            print(json.dumps({"profile_case": "mixed ELLBLOCK SP2, 16^3 block lattice, %d iterations, 8-bit split, "
+                                              "%d closing FP64" % (iters, nclose),
+                              "s": B.event_ms(6, 7) / 1e3, "trace": B.lib.bml_trace(D),
+                              "tc_iterations": int(info[6])}))
+        hh = C.c_void_p(D)
+        B.lib.bml_deallocate(C.byref(hh))
+    B.lib.bml_b200_set_tc_split(old)
+
+
 def block_lattice_products(L, radius):
     """Block products of X^2 on the L^3 block lattice: the (ib, jb, kb)
     triples, sum over ib and its neighbours jb of jb's neighbour count."""
@@ -966,6 +1001,9 @@ def main():
     rank, world, local = dist_env()
     if args.profile:
         run_profile_case()
+        return
+    if args.profile_eb_sp2:
+        run_profile_eb_sp2()
         return
     if args.profile_tc or args.profile_tc_wide:
         run_profile_tc(wide=args.profile_tc_wide, split=args.tc_split)
